@@ -1,0 +1,377 @@
+"""gem_b200 — Python view of libgem, a B200-native edge-centric subgraph matcher.
+
+Everything here is a thin ctypes layer over the C-ABI declared in
+include/gem.h; the work happens in libgem.so (C++ host code and sm_100a CUDA
+kernels).  There is no CPU fallback: if libgem.so is missing or no CUDA device
+is present, device calls raise.
+
+Typical use::
+
+    import gem_b200 as gem
+    g = gem.HostGraph.rmat(scale=16, edge_factor=8, seed=1).set_labels(8)
+    qs = gem.gen_queries(g, k=4, density=gem.SPARSE, count=10, seed=7)
+    ctx = gem.Context()
+    ctx.load_graph(g)
+    res = ctx.run(qs[0])            # exact embedding count (u64)
+
+The reference's driver surface is `GEM -q <query> -d <data> -t 0`
+(in-core/src/main.cu:23-275); `gem_b200/bin/gem` is the drop-in CLI and this
+module mirrors its phases (filter, hash index, edge tables, join) for tests
+and tools.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libgem.so")
+
+ANY, SPARSE, DENSE = 0, 1, 2
+MODE_COUNT, MODE_HASH, MODE_ENUMERATE = 0, 1, 2
+IDX_AUTO, IDX_RANK, IDX_CUCKOO = 0, 1, 2
+MAX_QV, MAX_QE = 32, 496
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_LIMIT", 4: "ERR_TIMEOUT", 5: "ERR_CUDA",
+          6: "ERR_IO", 7: "ERR_STATE", 8: "ERR_OVERFLOW", 9: "ERR_INTERNAL"}
+PHASES = ("filter", "index", "tables", "join", "total", "h2d", "d2h", "host")
+
+# C-ABI symbols declared in include/gem.h (checked by the CPU test suite).
+EXPORTS = (
+    "gem_strerror", "gem_hgraph_create", "gem_hgraph_read_text", "gem_hgraph_write_text",
+    "gem_hgraph_rmat", "gem_hgraph_set_labels", "gem_hgraph_info", "gem_hgraph_view",
+    "gem_hgraph_destroy", "gem_query_read_text", "gem_query_write_text", "gem_gen_queries",
+    "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
+    "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
+    "gem_submit", "gem_poll",
+)
+
+
+class GemError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+
+
+class _Query(C.Structure):
+    _fields_ = [("nv", C.c_uint32), ("ne", C.c_uint32), ("labels", C.POINTER(C.c_uint32)),
+                ("edges", C.POINTER(C.c_uint32))]
+
+
+class _Opts(C.Structure):
+    _fields_ = [("device", C.c_int), ("device_budget_bytes", C.c_uint64), ("pinned_budget_bytes", C.c_uint64),
+                ("ooc", C.c_int), ("time_cap_ms", C.c_uint32), ("index_kind", C.c_uint32),
+                ("reserved", C.c_uint32 * 6)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("emb_hash", C.c_uint64), ("n_written", C.c_uint64),
+                ("status", C.c_uint32), ("n_tables", C.c_uint32), ("cand_total", C.c_uint64),
+                ("table_total", C.c_uint64), ("nodes", C.c_uint64), ("bytes_alg", C.c_uint64 * 4),
+                ("ms", C.c_float * 8)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libgem.so (built in-tree by gem_b200.build / __graft_entry__.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libgem.so not built at {LIB_PATH}; run `python -m gem_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        u32p, u64p = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)
+        vp = C.c_void_p
+        L.gem_strerror.restype = C.c_char_p
+        L.gem_last_error.restype = C.c_char_p
+        L.gem_last_error.argtypes = [vp]
+        L.gem_hgraph_create.argtypes = [C.c_uint32, u64p, u32p, u32p, C.POINTER(vp)]
+        L.gem_hgraph_read_text.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.gem_hgraph_write_text.argtypes = [vp, C.c_char_p]
+        L.gem_hgraph_rmat.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                      C.POINTER(vp)]
+        L.gem_hgraph_set_labels.argtypes = [vp, C.c_uint32, C.c_double, C.c_uint64]
+        L.gem_hgraph_info.argtypes = [vp, u32p, u64p, u32p, u32p]
+        L.gem_hgraph_view.argtypes = [vp, C.POINTER(u64p), C.POINTER(u32p), C.POINTER(u32p)]
+        L.gem_hgraph_destroy.argtypes = [vp]
+        L.gem_hgraph_destroy.restype = None
+        L.gem_query_read_text.argtypes = [C.c_char_p, u32p, u32p, u32p, u32p]
+        L.gem_query_write_text.argtypes = [C.POINTER(_Query), C.c_char_p]
+        L.gem_gen_queries.argtypes = [vp, C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, u32p, u32p, u32p]
+        L.gem_ctx_create.argtypes = [C.POINTER(_Opts), C.POINTER(vp)]
+        L.gem_ctx_destroy.argtypes = [vp]
+        L.gem_ctx_destroy.restype = None
+        L.gem_ctx_load_graph.argtypes = [vp, vp]
+        L.gem_query_run.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, u32p, C.c_uint64,
+                                    C.POINTER(_Result)]
+        L.gem_batch_run.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, C.POINTER(_Result)]
+        L.gem_embedding_hash.argtypes = [u32p, C.c_uint32]
+        L.gem_embedding_hash.restype = C.c_uint64
+        L.gem_filter.argtypes = [vp, C.POINTER(_Query), C.c_uint32, u32p, u32p, C.c_uint64]
+        L.gem_edge_table.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_uint32, u64p, C.c_uint64, u32p,
+                                     C.c_uint64, u64p, u64p]
+        L.gem_index_probe.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_uint32, u32p, C.c_uint32, u32p]
+        L.gem_submit.argtypes = [vp, C.POINTER(_Query), C.c_int, u64p]
+        L.gem_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Result), C.POINTER(C.c_int)]
+        _lib = L
+    return _lib
+
+
+def _p32(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _p64(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint64))
+
+
+def _check(st, ctx=None, what=""):
+    if st != 0:
+        msg = what
+        if ctx is not None:
+            m = lib().gem_last_error(ctx)
+            if m:
+                msg += ": " + m.decode()
+        raise GemError(st, msg)
+
+
+class Query:
+    """A query graph: labels (nv,) and undirected edges (ne, 2), vertices 0..nv-1."""
+
+    def __init__(self, labels, edges):
+        self.labels = np.ascontiguousarray(np.asarray(labels, dtype=np.uint32).reshape(-1))
+        e = np.asarray(edges, dtype=np.uint32).reshape(-1, 2) if len(edges) else np.zeros((0, 2), np.uint32)
+        self.edges = np.ascontiguousarray(e)
+
+    @property
+    def nv(self):
+        return int(self.labels.shape[0])
+
+    @property
+    def ne(self):
+        return int(self.edges.shape[0])
+
+    def _c(self):
+        q = _Query(self.nv, self.ne, _p32(self.labels), _p32(self.edges.reshape(-1)))
+        q._keep = (self.labels, self.edges)
+        return q
+
+    @staticmethod
+    def read_text(path):
+        nv, ne = C.c_uint32(), C.c_uint32()
+        lab = np.zeros(MAX_QV, np.uint32)
+        edg = np.zeros(2 * MAX_QE, np.uint32)
+        _check(lib().gem_query_read_text(path.encode(), C.byref(nv), C.byref(ne), _p32(lab), _p32(edg)),
+               what=f"read {path}")
+        return Query(lab[:nv.value].copy(), edg[:2 * ne.value].reshape(-1, 2).copy())
+
+    def write_text(self, path):
+        q = self._c()
+        _check(lib().gem_query_write_text(C.byref(q), path.encode()), what=f"write {path}")
+
+    def __repr__(self):
+        return f"Query(nv={self.nv}, ne={self.ne})"
+
+
+class HostGraph:
+    """Host CSR data graph with sorted adjacency (owned by libgem)."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.gem_hgraph_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    @staticmethod
+    def rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=None):
+        h = C.c_void_p()
+        seed = (0x47454D00 + scale) if seed is None else seed
+        _check(lib().gem_hgraph_rmat(scale, edge_factor, a, b, c, seed, C.byref(h)), what="rmat")
+        return HostGraph(h)
+
+    @staticmethod
+    def from_csr(offsets, nbrs, labels):
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        nb = np.ascontiguousarray(nbrs, dtype=np.uint32)
+        lb = np.ascontiguousarray(labels, dtype=np.uint32)
+        if nb.size == 0:
+            nb = np.zeros(1, np.uint32)
+        h = C.c_void_p()
+        _check(lib().gem_hgraph_create(len(lb), _p64(off), _p32(nb), _p32(lb), C.byref(h)), what="hgraph_create")
+        return HostGraph(h)
+
+    @staticmethod
+    def from_edges(nv, edges, labels):
+        """Undirected edge list -> CSR with sorted adjacency."""
+        e = np.asarray(edges, dtype=np.int64).reshape(-1, 2)
+        e = e[e[:, 0] != e[:, 1]]
+        lo, hi = np.minimum(e[:, 0], e[:, 1]), np.maximum(e[:, 0], e[:, 1])
+        key = np.unique(lo * (nv + 1) + hi)
+        lo, hi = key // (nv + 1), key % (nv + 1)
+        src = np.concatenate([lo, hi])
+        dst = np.concatenate([hi, lo])
+        order = np.lexsort((dst, src))
+        src, dst = src[order], dst[order]
+        off = np.zeros(nv + 1, np.uint64)
+        np.add.at(off, src + 1, 1)
+        off = np.cumsum(off).astype(np.uint64)
+        return HostGraph.from_csr(off, dst.astype(np.uint32), labels)
+
+    @staticmethod
+    def read_text(path):
+        h = C.c_void_p()
+        _check(lib().gem_hgraph_read_text(path.encode(), C.byref(h)), what=f"read {path}")
+        return HostGraph(h)
+
+    def write_text(self, path):
+        _check(lib().gem_hgraph_write_text(self._h, path.encode()), what=f"write {path}")
+
+    def set_labels(self, nlabels, zipf_s=0.0, seed=None):
+        if seed is None:
+            seed = 0x47454D4C
+        _check(lib().gem_hgraph_set_labels(self._h, nlabels, zipf_s, seed), what="set_labels")
+        return self
+
+    def info(self):
+        nv, na, ml, md = C.c_uint32(), C.c_uint64(), C.c_uint32(), C.c_uint32()
+        _check(lib().gem_hgraph_info(self._h, C.byref(nv), C.byref(na), C.byref(ml), C.byref(md)))
+        return {"nv": nv.value, "n_arcs": na.value, "n_labels": ml.value, "max_degree": md.value}
+
+    @property
+    def nv(self):
+        return self.info()["nv"]
+
+    def arrays(self):
+        """(offsets u64[nv+1], nbrs u32[arcs], labels u32[nv]) as read-only numpy views."""
+        inf = self.info()
+        po, pn, pl = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+        _check(lib().gem_hgraph_view(self._h, C.byref(po), C.byref(pn), C.byref(pl)))
+        off = np.ctypeslib.as_array(po, shape=(inf["nv"] + 1,))
+        nbr = np.ctypeslib.as_array(pn, shape=(max(inf["n_arcs"], 1),))[:inf["n_arcs"]]
+        lab = np.ctypeslib.as_array(pl, shape=(max(inf["nv"], 1),))[:inf["nv"]]
+        for a in (off, nbr, lab):
+            a.flags.writeable = False
+        return off, nbr, lab
+
+
+def gen_queries(graph, k, density=ANY, count=1, seed=0x51000, max_e=MAX_QE):
+    """Random-walk queries (see gem_gen_queries in include/gem.h)."""
+    ne = np.zeros(count, np.uint32)
+    lab = np.zeros(count * k, np.uint32)
+    edg = np.zeros(count * 2 * max_e, np.uint32)
+    _check(lib().gem_gen_queries(graph._h, k, density, count, seed, max_e, _p32(ne), _p32(lab), _p32(edg)),
+           what="gen_queries")
+    out = []
+    for i in range(count):
+        e = edg[i * 2 * max_e: i * 2 * max_e + 2 * int(ne[i])].reshape(-1, 2).copy()
+        out.append(Query(lab[i * k:(i + 1) * k].copy(), e))
+    return out
+
+
+def embedding_hash(f):
+    f = np.ascontiguousarray(f, dtype=np.uint32)
+    return int(lib().gem_embedding_hash(_p32(f), len(f)))
+
+
+class Result(dict):
+    """Per-query result: count, emb_hash, status, timings (ms) and byte counters."""
+
+    @staticmethod
+    def _from(r):
+        d = Result(count=int(r.count), emb_hash=int(r.emb_hash), n_written=int(r.n_written),
+                   status=STATUS.get(r.status, r.status), status_code=int(r.status), n_tables=int(r.n_tables),
+                   cand_total=int(r.cand_total), table_total=int(r.table_total), nodes=int(r.nodes),
+                   bytes_alg=[int(x) for x in r.bytes_alg], ms={p: float(r.ms[i]) for i, p in enumerate(PHASES)})
+        return d
+
+
+class Context:
+    """One GPU with a resident data graph (gem_ctx)."""
+
+    def __init__(self, device=0, budget_bytes=0, time_cap_ms=0, index_kind=IDX_AUTO, ooc=False, pinned_bytes=0):
+        o = _Opts()
+        o.device = device
+        o.device_budget_bytes = budget_bytes
+        o.pinned_budget_bytes = pinned_bytes
+        o.ooc = 1 if ooc else 0
+        o.time_cap_ms = time_cap_ms
+        o.index_kind = index_kind
+        h = C.c_void_p()
+        _check(lib().gem_ctx_create(C.byref(o), C.byref(h)), what="ctx_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().gem_ctx_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def load_graph(self, g):
+        _check(lib().gem_ctx_load_graph(self._h, g._h), self._h, "load_graph")
+
+    def run(self, q, mode=MODE_COUNT, threshold=0, emb_cap=0, raise_on_error=True):
+        qc = q._c()
+        r = _Result()
+        buf = np.zeros(max(emb_cap, 1) * q.nv, np.uint32) if mode == MODE_ENUMERATE else None
+        st = lib().gem_query_run(self._h, C.byref(qc), threshold, mode, _p32(buf) if buf is not None else None,
+                                 emb_cap, C.byref(r))
+        res = Result._from(r)
+        if mode == MODE_ENUMERATE:
+            res["embeddings"] = buf[: res["n_written"] * q.nv].reshape(-1, q.nv)
+        if st != 0 and raise_on_error and st != 8:
+            _check(st, self._h, "query_run")
+        return res
+
+    def batch(self, qs, mode=MODE_COUNT):
+        arr = (_Query * len(qs))()
+        keep = []
+        for i, q in enumerate(qs):
+            arr[i] = q._c()
+            keep.append(q)
+        rs = (_Result * len(qs))()
+        st = lib().gem_batch_run(self._h, arr, len(qs), mode, rs)
+        out = [Result._from(r) for r in rs]
+        return st, out
+
+    def filter(self, q, threshold=0):
+        counts = np.zeros(q.nv, np.uint32)
+        cap = 1 << 26
+        cand = np.zeros(cap, np.uint32)
+        qc = q._c()
+        _check(lib().gem_filter(self._h, C.byref(qc), threshold, _p32(counts), _p32(cand), cap), self._h, "filter")
+        lists, at = [], 0
+        for u in range(q.nv):
+            lists.append(cand[at:at + int(counts[u])].copy())
+            at += int(counts[u])
+        return lists
+
+    def edge_table(self, q, u, w, values_cap=1 << 26):
+        nk, nvals = C.c_uint64(), C.c_uint64()
+        off = np.zeros(1 << 24, np.uint64)
+        vals = np.zeros(values_cap, np.uint32)
+        qc = q._c()
+        _check(lib().gem_edge_table(self._h, C.byref(qc), u, w, _p64(off), off.size, _p32(vals), values_cap,
+                                    C.byref(nk), C.byref(nvals)), self._h, "edge_table")
+        return off[:nk.value + 1].copy(), vals[:nvals.value].copy()
+
+    def index_probe(self, q, u, keys, kind=IDX_RANK):
+        keys = np.ascontiguousarray(keys, dtype=np.uint32)
+        out = np.zeros(max(len(keys), 1), np.uint32)
+        qc = q._c()
+        _check(lib().gem_index_probe(self._h, C.byref(qc), u, kind, _p32(keys), len(keys), _p32(out)), self._h,
+               "index_probe")
+        return out[:len(keys)]

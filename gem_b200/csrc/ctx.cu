@@ -1,0 +1,902 @@
+// libgem host orchestration: the device context, the resident data graph, a
+// chunked device arena, the matching-order planner, and the wave pipeline
+//   filter -> compaction -> plan -> edge tables -> index -> join
+// that serves gem_query_run (a wave of one query) and gem_batch_run (waves of
+// many queries in one persistent join launch).
+//
+// Reference counterparts: main()'s phase chain (in-core/src/main.cu:140-236),
+// the process globals of in-core/lib/utils/src/globals.cu, the per-phase
+// allocate/scan/sync sequences of in-core/lib/structure/src/unifiedTrie.cu and
+// in-core/lib/join/src/join_trie.cu.  Everything here hangs off a gem_ctx; no
+// call exits the process.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ctx.h"
+#include "kernels.h"
+
+using namespace gem;
+
+// ---------------------------------------------------------------------------
+// Error helpers
+// ---------------------------------------------------------------------------
+#define CU(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                 \
+      return e_ == cudaErrorMemoryAllocation ? GEM_ERR_OOM : GEM_ERR_CUDA;           \
+    }                                                                                \
+  } while (0)
+#define ST(call)                      \
+  do {                                \
+    gem_status s_ = (call);           \
+    if (s_ != GEM_OK) return s_;      \
+  } while (0)
+
+extern "C" const char *gem_strerror(gem_status s) {
+  switch (s) {
+    case GEM_OK: return "ok";
+    case GEM_ERR_ARG: return "invalid argument";
+    case GEM_ERR_OOM: return "out of device or pinned memory budget";
+    case GEM_ERR_LIMIT: return "outside the supported envelope";
+    case GEM_ERR_TIMEOUT: return "time cap or bounded wait expired";
+    case GEM_ERR_CUDA: return "CUDA runtime error";
+    case GEM_ERR_IO: return "file missing or malformed";
+    case GEM_ERR_STATE: return "call out of order";
+    case GEM_ERR_OVERFLOW: return "result exceeds buffer or counter";
+    case GEM_ERR_INTERNAL: return "internal consistency check failed";
+  }
+  return "unknown status";
+}
+
+// ---------------------------------------------------------------------------
+// Arena: chunks from cudaMalloc, bump allocation, reset per wave.
+// ---------------------------------------------------------------------------
+gem_status Arena::alloc(gem_ctx *ctx, uint64_t bytes, void **out) {
+  bytes = (bytes + 255) & ~255ull;
+  if (bytes == 0) bytes = 256;
+  for (; cur < chunks.size(); ++cur) {
+    Chunk &c = chunks[cur];
+    if (c.used + bytes <= c.size) {
+      *out = c.base + c.used;
+      c.used += bytes;
+      in_use += bytes;
+      peak = std::max(peak, in_use);
+      return GEM_OK;
+    }
+  }
+  uint64_t sz = std::max<uint64_t>(bytes, 512ull << 20);
+  if (ctx->device_bytes + sz > ctx->budget) {
+    sz = bytes;
+    if (ctx->device_bytes + sz > ctx->budget) {
+      ctx->err = "device budget exceeded: need " + std::to_string(bytes) + " more bytes";
+      return GEM_ERR_OOM;
+    }
+  }
+  char *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, sz);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return GEM_ERR_OOM;
+  }
+  ctx->device_bytes += sz;
+  chunks.push_back({p, sz, bytes});
+  cur = chunks.size() - 1;
+  *out = p;
+  in_use += bytes;
+  peak = std::max(peak, in_use);
+  return GEM_OK;
+}
+void Arena::reset() {
+  for (auto &c : chunks) c.used = 0;
+  cur = 0;
+  in_use = 0;
+}
+void Arena::release(gem_ctx *ctx) {
+  for (auto &c : chunks) {
+    cudaFree(c.base);
+    ctx->device_bytes -= c.size;
+  }
+  chunks.clear();
+  cur = 0;
+  in_use = 0;
+}
+
+template <class T>
+static gem_status aalloc(gem_ctx *ctx, uint64_t n, T **out) {
+  void *p = nullptr;
+  gem_status s = ctx->arena.alloc(ctx, n * sizeof(T), &p);
+  *out = (T *)p;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Context and graph
+// ---------------------------------------------------------------------------
+extern "C" gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out) {
+  if (!out) return GEM_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<gem_ctx> c(new gem_ctx());
+  if (opts) c->opts = *opts;
+  gem_ctx *ctx = c.get();
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return GEM_ERR_CUDA;
+  }
+  if (ctx->opts.device < 0 || ctx->opts.device >= ndev) return GEM_ERR_ARG;
+  CU(cudaSetDevice(ctx->opts.device));
+  CU(cudaStreamCreateWithFlags(&ctx->s, cudaStreamNonBlocking));
+  for (auto &ev : ctx->ev) CU(cudaEventCreate(&ev));
+  size_t fr = 0, tot = 0;
+  CU(cudaMemGetInfo(&fr, &tot));
+  ctx->budget = ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : (uint64_t)(fr * 0.9);
+  if (ctx->budget > fr) ctx->budget = fr;
+  CU(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->opts.device));
+  for (uint32_t m = 0; m < 3; ++m) ctx->join_bps[m] = join_blocks_per_sm(m);
+  // persistent small buffers
+  CU(cudaMalloc(&ctx->d_ctl, sizeof(JControl)));
+  CU(cudaMalloc(&ctx->d_queue, sizeof(JTask) * TASK_CAP));
+  CU(cudaMalloc(&ctx->d_err, sizeof(uint32_t) * 4));
+  CU(cudaHostAlloc(&ctx->h_small, 1 << 20, cudaHostAllocDefault));
+  ctx->device_bytes += sizeof(JControl) + sizeof(JTask) * TASK_CAP + 16;
+  *out = c.release();
+  return GEM_OK;
+}
+
+static void free_graph(gem_ctx *ctx) {
+  if (ctx->graph_mem) {
+    cudaFree(ctx->graph_mem);
+    ctx->device_bytes -= ctx->graph_bytes;
+  }
+  ctx->graph_mem = nullptr;
+  ctx->graph_bytes = 0;
+  ctx->g = DevGraph();
+  ctx->loaded = false;
+}
+
+extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->opts.device);
+  cudaStreamSynchronize(ctx->s);
+  ctx->arena.release(ctx);
+  free_graph(ctx);
+  if (ctx->d_ctl) cudaFree(ctx->d_ctl);
+  if (ctx->d_queue) cudaFree(ctx->d_queue);
+  if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->h_small) cudaFreeHost(ctx->h_small);
+  for (auto &ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->s) cudaStreamDestroy(ctx->s);
+  delete ctx;
+}
+
+extern "C" const char *gem_last_error(const gem_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
+  if (!ctx || !hg) return GEM_ERR_ARG;
+  CU(cudaSetDevice(ctx->opts.device));
+  CU(cudaStreamSynchronize(ctx->s));
+  ctx->arena.reset();
+  free_graph(ctx);
+  const uint32_t nv = hg->nv;
+  const uint64_t na = hg->n_arcs();
+  const uint32_t L = hg->max_label_plus1;
+  const uint32_t stride = (L > 0 && L <= NLC_MAX_LABELS) ? ((L + 15) / 16) * 16 : 0;
+  auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
+  const uint64_t b_off = al(8ull * (nv + 1)), b_nbr = al(4ull * na), b_lab = al(4ull * nv), b_deg = al(4ull * nv),
+                 b_nlc = al((uint64_t)stride * nv);
+  const uint64_t total = b_off + b_nbr + b_lab + b_deg + b_nlc;
+  if (ctx->device_bytes + total > ctx->budget) {
+    ctx->err = "graph does not fit the device budget";
+    return GEM_ERR_OOM;
+  }
+  char *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, total);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->err = std::string("cudaMalloc graph: ") + cudaGetErrorString(e);
+    return GEM_ERR_OOM;
+  }
+  ctx->graph_mem = p;
+  ctx->graph_bytes = total;
+  ctx->device_bytes += total;
+  uint64_t *d_off = (uint64_t *)p;
+  uint32_t *d_nbr = (uint32_t *)(p + b_off);
+  uint32_t *d_lab = (uint32_t *)(p + b_off + b_nbr);
+  uint32_t *d_deg = (uint32_t *)(p + b_off + b_nbr + b_lab);
+  uint8_t *d_nlc = stride ? (uint8_t *)(p + b_off + b_nbr + b_lab + b_deg) : nullptr;
+  CU(cudaMemcpyAsync(d_off, hg->off.data(), 8ull * (nv + 1), cudaMemcpyHostToDevice, ctx->s));
+  if (na) CU(cudaMemcpyAsync(d_nbr, hg->nbr.data(), 4ull * na, cudaMemcpyHostToDevice, ctx->s));
+  if (nv) CU(cudaMemcpyAsync(d_lab, hg->lab.data(), 4ull * nv, cudaMemcpyHostToDevice, ctx->s));
+  DevGraph g;
+  g.nv = nv;
+  g.narcs = na;
+  g.nlabels = L;
+  g.nlc_stride = stride;
+  g.off = d_off;
+  g.nbr = d_nbr;
+  g.lab = d_lab;
+  g.deg = d_deg;
+  g.nlc = d_nlc;
+  launch_degrees(g, d_deg, ctx->s);
+  if (stride) launch_nlc(g, d_nlc, stride, ctx->s);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(ctx->s));
+  ctx->g = g;
+  ctx->loaded = true;
+  ctx->label_freq.assign(L, 0);
+  for (uint32_t v = 0; v < nv; ++v) ctx->label_freq[hg->lab[v]]++;
+  return GEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Planner: matching order for the DFS join.
+// ---------------------------------------------------------------------------
+void make_plan(const HostQuery &q, const uint32_t *cnt, Plan &p) {
+  const uint32_t n = q.nv;
+  p.n = n;
+  uint32_t used = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    int best = -1;
+    uint64_t bkey[5] = {0, 0, 0, 0, 0};
+    for (uint32_t u = 0; u < n; ++u) {
+      if (used & (1u << u)) continue;
+      const uint32_t back = __builtin_popcount(q.adj[u] & used);
+      if (k > 0 && back == 0) continue;
+      const uint32_t d = q.deg(u);
+      // Root: fewest candidates per incident edge.  Later: most backward
+      // neighbours, non-leaves before leaves, fewest candidates, most edges.
+      uint64_t key[5];
+      if (k == 0) {
+        key[0] = (uint64_t)((double)cnt[u] / (double)(d + 1) * 1024.0);
+        key[1] = ~(uint64_t)d;
+        key[2] = u;
+        key[3] = key[4] = 0;
+      } else {
+        key[0] = ~(uint64_t)back;
+        key[1] = d <= 1 ? 1 : 0;
+        key[2] = cnt[u];
+        key[3] = ~(uint64_t)d;
+        key[4] = u;
+      }
+      if (best < 0 || std::lexicographical_compare(key, key + 5, bkey, bkey + 5)) {
+        best = (int)u;
+        std::memcpy(bkey, key, sizeof key);
+      }
+    }
+    const uint32_t u = (uint32_t)best;
+    p.order[k] = u;
+    p.level_of[u] = k;
+    used |= 1u << u;
+  }
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t u = p.order[k];
+    p.back[k].clear();
+    p.dup_mask[k] = 0;
+    for (uint32_t j = 0; j < k; ++j) {
+      if (q.adj[u] & (1u << p.order[j])) p.back[k].push_back(j);
+      if (q.lab[p.order[j]] == q.lab[u]) p.dup_mask[k] |= 1u << j;
+    }
+    p.need_idx[k] = 0;
+  }
+  for (uint32_t k = 0; k < n; ++k)
+    for (uint32_t j : p.back[k]) p.need_idx[j] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Wave pipeline
+// ---------------------------------------------------------------------------
+struct EvPair {
+  cudaEvent_t a, b;
+};
+
+static void fill_filter_desc(const HostQuery &q, uint32_t threshold, uint32_t row_base, FilterDesc &d) {
+  std::memset(&d, 0, sizeof d);
+  d.nq = q.nv;
+  d.threshold = threshold;
+  d.row_base = row_base;
+  for (uint32_t u = 0; u < q.nv; ++u) {
+    d.lab[u] = q.lab[u];
+    d.deg[u] = q.deg(u);
+    uint32_t k = 0;
+    while (k < d.nql && d.ql[k] != q.lab[u]) ++k;
+    if (k == d.nql) d.ql[d.nql++] = q.lab[u];
+  }
+  for (uint32_t u = 0; u < q.nv; ++u)
+    for (uint32_t w = 0; w < q.nv; ++w)
+      if (q.adj[u] & (1u << w)) {
+        uint32_t k = 0;
+        while (d.ql[k] != q.lab[w]) ++k;
+        d.nlc[u][k]++;
+      }
+}
+
+static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return ms;
+}
+
+// Runs the filter for every query of the wave; fills w.rows / counts / lists.
+static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
+  const uint32_t nwords = (ctx->g.nv + 31) / 32;
+  w.nwords = nwords;
+  uint32_t rows = 0;
+  std::vector<FilterDesc> fd(w.q.size());
+  for (size_t i = 0; i < w.q.size(); ++i) {
+    w.row_base[i] = rows;
+    fill_filter_desc(w.q[i], threshold, rows, fd[i]);
+    rows += w.q[i].nv;
+  }
+  w.nrows = rows;
+  FilterDesc *d_fd;
+  ST(aalloc(ctx, fd.size(), &d_fd));
+  CU(cudaMemcpyAsync(d_fd, fd.data(), fd.size() * sizeof(FilterDesc), cudaMemcpyHostToDevice, ctx->s));
+  const uint64_t nbits = (uint64_t)rows * nwords;
+  ST(aalloc(ctx, nbits, &w.d_rb));
+  uint64_t *d_ex, *d_tmp, *d_rows;
+  ST(aalloc(ctx, nbits + 1, &d_ex));
+  ST(aalloc(ctx, scan_tmp_words(nbits), &d_tmp));
+  ST(aalloc(ctx, rows + 1, &d_rows));
+  launch_filter(ctx->g, d_fd, (uint32_t)fd.size(), w.d_rb, nwords, ctx->s);
+  launch_scan(w.d_rb, SCAN_POPC_U64LO, nbits, d_ex, d_tmp, ctx->s);
+  launch_gather_strided(d_ex, nwords, rows + 1, d_rows, ctx->s);
+  std::vector<uint64_t> rs(rows + 1);
+  CU(cudaMemcpyAsync(rs.data(), d_rows, 8ull * (rows + 1), cudaMemcpyDeviceToHost, ctx->s));
+  CU(cudaStreamSynchronize(ctx->s));
+  CU(cudaGetLastError());
+  w.cnt.resize(rows);
+  w.c_base.resize(rows + 1);
+  for (uint32_t r = 0; r < rows; ++r) w.cnt[r] = (uint32_t)(rs[r + 1] - rs[r]);
+  for (uint32_t r = 0; r <= rows; ++r) w.c_base[r] = rs[r] - rs[0];
+  const uint64_t total = w.c_base[rows];
+  uint64_t *d_cbase;
+  ST(aalloc(ctx, rows + 1, &d_cbase));
+  CU(cudaMemcpyAsync(d_cbase, w.c_base.data(), 8ull * (rows + 1), cudaMemcpyHostToDevice, ctx->s));
+  ST(aalloc(ctx, total ? total : 1, &w.d_cand));
+  launch_compact(w.d_rb, d_ex, rows, nwords, d_cbase, w.d_cand, ctx->s);
+  CU(cudaGetLastError());
+  w.cand_total = total;
+  // algorithmic bytes: labels + degrees of every vertex, the label-count rows
+  // of vertices whose label occurs in the query, the bit rows (write, scan,
+  // rank rewrite) and the candidate lists.
+  uint64_t b = 0;
+  for (size_t i = 0; i < w.q.size(); ++i) {
+    uint64_t lb = 8ull * ctx->g.nv;
+    for (uint32_t k = 0; k < fd[i].nql; ++k)
+      if (fd[i].ql[k] < ctx->label_freq.size()) lb += (uint64_t)ctx->g.nlc_stride * ctx->label_freq[fd[i].ql[k]];
+    lb += 8ull * nwords * w.q[i].nv * 4;
+    b += lb;
+  }
+  w.bytes_filter = b + 4 * total;
+  return GEM_OK;
+}
+
+static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
+  // sources and edges of every active query
+  std::vector<TabSource> src;
+  std::vector<TabEdge> edge;
+  std::vector<uint32_t> src_row;
+  std::vector<int> row_src(w.nrows, -1);
+  uint64_t nkeys = 0;
+  for (size_t qi = 0; qi < w.q.size(); ++qi) {
+    if (!w.active[qi]) continue;
+    const Plan &p = w.plan[qi];
+    for (uint32_t k = 1; k < p.n; ++k)
+      for (uint32_t j : p.back[k]) {
+        const uint32_t r = w.row_base[qi] + p.order[j];
+        if (row_src[r] < 0) {
+          row_src[r] = (int)src.size();
+          TabSource s;
+          s.keys = w.d_cand + w.c_base[r];
+          s.nkeys = w.cnt[r];
+          s.pad = 0;
+          s.key_base = nkeys;
+          nkeys += w.cnt[r];
+          src.push_back(s);
+          src_row.push_back(r);
+        }
+      }
+  }
+  w.nsrc = (uint32_t)src.size();
+  if (src.empty()) return GEM_OK;
+  TabSource *d_src;
+  ST(aalloc(ctx, src.size(), &d_src));
+  CU(cudaMemcpyAsync(d_src, src.data(), src.size() * sizeof(TabSource), cudaMemcpyHostToDevice, ctx->s));
+  uint32_t *d_tiles;
+  uint64_t *d_tp, *d_tmp, *d_stb;
+  ST(aalloc(ctx, nkeys ? nkeys : 1, &d_tiles));
+  ST(aalloc(ctx, nkeys + 1, &d_tp));
+  ST(aalloc(ctx, scan_tmp_words(nkeys), &d_tmp));
+  ST(aalloc(ctx, src.size() + 1, &d_stb));
+  launch_key_tiles(ctx->g, d_src, (uint32_t)src.size(), nkeys, d_tiles, ctx->s);
+  launch_scan(d_tiles, SCAN_U32, nkeys, d_tp, d_tmp, ctx->s);
+  launch_source_tile_bases(d_src, (uint32_t)src.size(), nkeys, d_tp, d_stb, ctx->s);
+  std::vector<uint64_t> stb(src.size() + 1);
+  CU(cudaMemcpyAsync(stb.data(), d_stb, 8 * stb.size(), cudaMemcpyDeviceToHost, ctx->s));
+  CU(cudaStreamSynchronize(ctx->s));
+  CU(cudaGetLastError());
+  // edges
+  uint64_t tiles = 0, offs = 0;
+  w.edge_of.assign(w.q.size(), {});
+  for (size_t qi = 0; qi < w.q.size(); ++qi) {
+    if (!w.active[qi]) continue;
+    const Plan &p = w.plan[qi];
+    w.edge_of[qi].assign(QV * QV, UINT32_MAX);
+    for (uint32_t k = 1; k < p.n; ++k)
+      for (uint32_t j : p.back[k]) {
+        const uint32_t r = w.row_base[qi] + p.order[j];
+        const uint32_t s = (uint32_t)row_src[r];
+        TabEdge e;
+        e.src = s;
+        e.pad = 0;
+        e.rb_w = w.d_rb + (uint64_t)(w.row_base[qi] + p.order[k]) * w.nwords;
+        e.tile_base = tiles;
+        e.ntiles = stb[s + 1] - stb[s];
+        e.off_base = offs;
+        e.offsets = nullptr;
+        tiles += e.ntiles;
+        offs += (uint64_t)src[s].nkeys + 1;
+        w.edge_of[qi][j * QV + k] = (uint32_t)edge.size();
+        edge.push_back(e);
+      }
+  }
+  uint64_t *d_offs;
+  ST(aalloc(ctx, offs, &d_offs));
+  for (auto &e : edge) e.offsets = d_offs + e.off_base;
+  TabEdge *d_edge;
+  ST(aalloc(ctx, edge.size(), &d_edge));
+  CU(cudaMemcpyAsync(d_edge, edge.data(), edge.size() * sizeof(TabEdge), cudaMemcpyHostToDevice, ctx->s));
+  uint32_t *d_mask;
+  uint64_t *d_vp, *d_tmp2;
+  ST(aalloc(ctx, tiles ? tiles : 1, &d_mask));
+  ST(aalloc(ctx, tiles + 1, &d_vp));
+  ST(aalloc(ctx, scan_tmp_words(tiles), &d_tmp2));
+  launch_table_count(ctx->g, d_src, d_edge, (uint32_t)edge.size(), d_tp, tiles, d_mask, ctx->s);
+  launch_scan(d_mask, SCAN_POPC_U32, tiles, d_vp, d_tmp2, ctx->s);
+  uint64_t nvals = 0;
+  CU(cudaMemcpyAsync(&nvals, d_vp + tiles, 8, cudaMemcpyDeviceToHost, ctx->s));
+  CU(cudaStreamSynchronize(ctx->s));
+  CU(cudaGetLastError());
+  ST(aalloc(ctx, nvals ? nvals : 1, &w.d_values));
+  launch_table_offsets(d_src, d_edge, (uint32_t)edge.size(), d_tp, d_vp, offs, ctx->s);
+  launch_table_write(ctx->g, d_src, d_edge, (uint32_t)edge.size(), d_tp, tiles, d_mask, d_vp, w.d_values, ctx->s);
+  CU(cudaGetLastError());
+  w.edges = edge;
+  w.table_values = nvals;
+  w.table_tiles = tiles;
+  // algorithmic bytes: per tile the 32 neighbour ids (count pass) plus the
+  // membership words, the mask word written and read, the position word,
+  // values written with their ids re-read, and the offsets.
+  w.bytes_tables = tiles * (32ull * 4 + 32ull * 8 + 4 + 4 + 8) + nvals * (4 + 4) + offs * 8 + nkeys * (4 + 8 + 4);
+  return GEM_OK;
+}
+
+static gem_status wave_index(gem_ctx *ctx, Wave &w) {
+  std::vector<CuckooTable> tabs;
+  std::vector<std::pair<uint32_t, uint32_t>> who;  // (query, level)
+  uint64_t slots = 0, kb = 0;
+  for (size_t qi = 0; qi < w.q.size(); ++qi) {
+    if (!w.active[qi]) continue;
+    const Plan &p = w.plan[qi];
+    for (uint32_t k = 0; k < p.n; ++k) {
+      w.idx_kind[qi][k] = IDX_NONE;
+      if (k == 0 || !p.need_idx[k]) continue;
+      const uint32_t r = w.row_base[qi] + p.order[k];
+      uint32_t kind = ctx->opts.index_kind;
+      if (kind == 0) kind = IDX_RANK;
+      w.idx_kind[qi][k] = kind;
+      if (kind != IDX_CUCKOO) continue;
+      CuckooTable t;
+      std::memset(&t, 0, sizeof t);
+      t.keys = w.d_cand + w.c_base[r];
+      t.nkeys = w.cnt[r];
+      t.key_base = kb;
+      kb += t.nkeys;
+      uint64_t ns = cuckoo_slots_for(t.nkeys, &t.nb0, &t.nb1);
+      t.pad = (uint32_t)(slots >> 32);  // unused
+      uint64_t seed = mix64(0x43554B4Full ^ ((uint64_t)qi << 32) ^ k ^ ((uint64_t)w.cuckoo_round << 48));
+      t.a0 = mix64(seed) | 1ull;
+      t.c0 = mix64(seed + 1);
+      t.a1 = mix64(seed + 2) | 1ull;
+      t.c1 = mix64(seed + 3);
+      slots += ns;
+      tabs.push_back(t);
+      who.push_back({(uint32_t)qi, k});
+    }
+  }
+  w.ck_tabs = nullptr;
+  if (tabs.empty()) return GEM_OK;
+  uint64_t *d_slots;
+  uint32_t *d_sn;
+  ST(aalloc(ctx, slots, &d_slots));
+  ST(aalloc(ctx, tabs.size(), &d_sn));
+  CU(cudaMemsetAsync(d_slots, 0xFF, slots * 8, ctx->s));
+  CU(cudaMemsetAsync(d_sn, 0, tabs.size() * 4, ctx->s));
+  uint64_t at = 0;
+  for (size_t i = 0; i < tabs.size(); ++i) {
+    CuckooTable &t = tabs[i];
+    t.t0 = d_slots + at;
+    t.t1 = t.t0 + (uint64_t)t.nb0 * CK_SLOTS;
+    t.stash = t.t1 + (uint64_t)t.nb1 * CK_SLOTS;
+    t.stash_n = d_sn + i;
+    at += (uint64_t)(t.nb0 + t.nb1) * CK_SLOTS + CK_STASH;
+  }
+  // descriptors followed by room for the build's table lists
+  void *dv;
+  ST(ctx->arena.alloc(ctx, tabs.size() * sizeof(CuckooTable) + tabs.size() * 4 + 16, &dv));
+  CuckooTable *d_tabs = (CuckooTable *)dv;
+  CU(cudaMemcpyAsync(d_tabs, tabs.data(), tabs.size() * sizeof(CuckooTable), cudaMemcpyHostToDevice, ctx->s));
+  CU(cudaMemsetAsync(ctx->d_err, 0, 4, ctx->s));
+  launch_cuckoo_build(d_tabs, tabs.data(), (uint32_t)tabs.size(), ctx->d_err, ctx->s);
+  CU(cudaGetLastError());
+  uint32_t herr = 0;
+  CU(cudaMemcpyAsync(&herr, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->s));
+  CU(cudaStreamSynchronize(ctx->s));
+  if (herr) {
+    ctx->err = "cuckoo stash overflow";
+    return GEM_ERR_OVERFLOW;
+  }
+  for (size_t i = 0; i < tabs.size(); ++i) w.ck_of[who[i].first][who[i].second] = d_tabs + i;
+  w.ck_tabs = d_tabs;
+  w.bytes_index = kb * (4 + 8 + 8) + slots * 8 / 4;
+  return GEM_OK;
+}
+
+static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, uint64_t emb_cap) {
+  std::vector<JQuery> jq;
+  std::vector<JBack> jb;
+  std::vector<uint64_t> rp;
+  w.jq_index.assign(w.q.size(), UINT32_MAX);
+  uint64_t roots = 0;
+  for (size_t qi = 0; qi < w.q.size(); ++qi) {
+    if (!w.active[qi]) continue;
+    const Plan &p = w.plan[qi];
+    JQuery J;
+    std::memset(&J, 0, sizeof J);
+    J.n = p.n;
+    J.root_u = p.order[0];
+    const uint32_t r0 = w.row_base[qi] + p.order[0];
+    J.root_cand = w.d_cand + w.c_base[r0];
+    J.n_root = w.cnt[r0];
+    J.root_base = roots;
+    for (uint32_t k = 0; k < p.n; ++k) {
+      JLevel &L = J.lv[k];
+      L.u = p.order[k];
+      L.nback = (uint32_t)p.back[k].size();
+      L.back_base = (uint32_t)jb.size();
+      L.dup_mask = p.dup_mask[k];
+      L.idx_kind = k == 0 ? IDX_NONE : w.idx_kind[qi][k];
+      L.rb = w.d_rb + (uint64_t)(w.row_base[qi] + p.order[k]) * w.nwords;
+      L.ck = w.ck_of[qi][k];
+      for (uint32_t j : p.back[k]) {
+        JBack b;
+        b.lvl = j;
+        b.pad = 0;
+        b.off = w.edges[w.edge_of[qi][j * QV + k]].offsets;
+        jb.push_back(b);
+      }
+    }
+    w.jq_index[qi] = (uint32_t)jq.size();
+    rp.push_back(roots);
+    roots += J.n_root;
+    jq.push_back(J);
+  }
+  rp.push_back(roots);
+  w.out.assign(w.q.size(), JOut());
+  if (jq.empty()) return GEM_OK;
+  JQuery *d_jq;
+  JBack *d_jb;
+  uint64_t *d_rp;
+  JOut *d_out;
+  ST(aalloc(ctx, jq.size(), &d_jq));
+  ST(aalloc(ctx, jb.size() ? jb.size() : 1, &d_jb));
+  ST(aalloc(ctx, rp.size(), &d_rp));
+  ST(aalloc(ctx, jq.size(), &d_out));
+  CU(cudaMemcpyAsync(d_jq, jq.data(), jq.size() * sizeof(JQuery), cudaMemcpyHostToDevice, ctx->s));
+  if (!jb.empty()) CU(cudaMemcpyAsync(d_jb, jb.data(), jb.size() * sizeof(JBack), cudaMemcpyHostToDevice, ctx->s));
+  CU(cudaMemcpyAsync(d_rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, ctx->s));
+  CU(cudaMemsetAsync(d_out, 0, jq.size() * sizeof(JOut), ctx->s));
+  CU(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(JControl), ctx->s));
+  join_queue_init(ctx->d_queue, ctx->s);
+  const uint64_t cap_ms = ctx->opts.time_cap_ms ? ctx->opts.time_cap_ms : 600000u;
+  launch_set_deadline(&ctx->d_ctl->deadline_ns, cap_ms * 1000000ull, ctx->s);
+  JoinArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.queries = d_jq;
+  a.nquery = (uint32_t)jq.size();
+  a.mode = (uint32_t)mode;
+  a.backs = d_jb;
+  a.values = w.d_values;
+  a.root_prefix = d_rp;
+  a.n_roots = roots;
+  a.out = d_out;
+  a.ctl = ctx->d_ctl;
+  a.queue = ctx->d_queue;
+  a.emb = emb_dev;
+  a.emb_cap = emb_cap;
+  a.donate_max_level = ctx->donate_max_level;
+  CU(cudaEventRecord(ctx->ev[6], ctx->s));
+  launch_join(a, ctx->join_bps[mode], ctx->s);
+  CU(cudaEventRecord(ctx->ev[7], ctx->s));
+  CU(cudaGetLastError());
+  std::vector<JOut> out(jq.size());
+  CU(cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(JOut), cudaMemcpyDeviceToHost, ctx->s));
+  JControl hc;
+  CU(cudaMemcpyAsync(&hc, ctx->d_ctl, sizeof hc, cudaMemcpyDeviceToHost, ctx->s));
+  CU(cudaStreamSynchronize(ctx->s));
+  w.join_ms = ev_ms(ctx->ev[6], ctx->ev[7]);
+  for (size_t qi = 0; qi < w.q.size(); ++qi)
+    if (w.jq_index[qi] != UINT32_MAX) w.out[qi] = out[w.jq_index[qi]];
+  w.join_nodes = out[0].nodes;
+  w.join_scanned = out[0].scanned;
+  w.join_probes = out[0].probes;
+  w.emb_written = hc.emb_next;
+  w.join_err = hc.err;
+  // algorithmic bytes: per extended partial embedding its index word and the
+  // offsets pair of each table it keys; per evaluated candidate its id; per
+  // binary search a 16-byte sector beyond the cached upper levels.
+  uint64_t back_total = 0;
+  for (auto &J : jq) back_total += 0;  // per-level entries are counted through nodes
+  w.bytes_join = w.join_nodes * (8 + 16) + w.join_scanned * 4 + w.join_probes * 16 + back_total;
+  return GEM_OK;
+}
+
+gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_t *emb_dev, uint64_t emb_cap) {
+  if (!ctx->loaded) {
+    ctx->err = "no data graph loaded";
+    return GEM_ERR_STATE;
+  }
+  CU(cudaSetDevice(ctx->opts.device));
+  const size_t nq = w.q.size();
+  w.row_base.assign(nq, 0);
+  w.active.assign(nq, 1);
+  w.plan.assign(nq, Plan());
+  w.idx_kind.assign(nq, std::vector<uint32_t>(QV, 0));
+  w.ck_of.assign(nq, std::vector<const CuckooTable *>(QV, nullptr));
+  CU(cudaEventRecord(ctx->ev[0], ctx->s));
+  ST(wave_filter(ctx, w, threshold));
+  CU(cudaEventRecord(ctx->ev[1], ctx->s));
+  auto h0 = std::chrono::steady_clock::now();
+  for (size_t qi = 0; qi < nq; ++qi) {
+    const HostQuery &q = w.q[qi];
+    bool empty = false;
+    for (uint32_t u = 0; u < q.nv; ++u)
+      if (w.cnt[w.row_base[qi] + u] == 0) empty = true;
+    if (empty) {
+      w.active[qi] = 0;
+      continue;
+    }
+    make_plan(q, &w.cnt[w.row_base[qi]], w.plan[qi]);
+  }
+  w.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+  ST(wave_tables(ctx, w));
+  CU(cudaEventRecord(ctx->ev[2], ctx->s));
+  ST(wave_index(ctx, w));
+  CU(cudaEventRecord(ctx->ev[3], ctx->s));
+  ST(wave_join(ctx, w, mode, emb_dev, emb_cap));
+  CU(cudaEventRecord(ctx->ev[4], ctx->s));
+  CU(cudaStreamSynchronize(ctx->s));
+  w.filter_ms = ev_ms(ctx->ev[0], ctx->ev[1]);
+  w.tables_ms = ev_ms(ctx->ev[1], ctx->ev[2]);
+  w.index_ms = ev_ms(ctx->ev[2], ctx->ev[3]);
+  w.total_ms = ev_ms(ctx->ev[0], ctx->ev[4]);
+  return GEM_OK;
+}
+
+void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r) {
+  std::memset(r, 0, sizeof *r);
+  r->status = GEM_OK;
+  const JOut &o = w.out[qi];
+  r->count = o.count;
+  r->emb_hash = o.hash;
+  if (w.join_err == 1) r->status = GEM_ERR_TIMEOUT;
+  else if (w.join_err) r->status = GEM_ERR_INTERNAL;
+  uint64_t ct = 0;
+  for (uint32_t u = 0; u < w.q[qi].nv; ++u) ct += w.cnt[w.row_base[qi] + u];
+  r->cand_total = ct;
+  r->n_tables = w.active[qi] ? 0 : 0;
+  if (w.active[qi]) {
+    const Plan &p = w.plan[qi];
+    for (uint32_t k = 1; k < p.n; ++k) r->n_tables += (uint32_t)p.back[k].size();
+  }
+  r->table_total = w.table_values;
+  r->nodes = w.join_nodes;
+  r->bytes_alg[0] = w.bytes_filter;
+  r->bytes_alg[1] = w.bytes_index;
+  r->bytes_alg[2] = w.bytes_tables;
+  r->bytes_alg[3] = w.bytes_join;
+  r->ms[GEM_PH_FILTER] = w.filter_ms;
+  r->ms[GEM_PH_INDEX] = w.index_ms;
+  r->ms[GEM_PH_TABLES] = w.tables_ms;
+  r->ms[GEM_PH_JOIN] = w.join_ms;
+  r->ms[GEM_PH_TOTAL] = w.total_ms;
+  r->ms[GEM_PH_HOST] = (float)w.plan_ms;
+  (void)ctx;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI: queries
+// ---------------------------------------------------------------------------
+extern "C" gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold, int mode,
+                                    uint32_t *emb_out, uint64_t emb_cap, gem_result *res) {
+  if (!ctx || !q || !res) return GEM_ERR_ARG;
+  if (mode < GEM_MODE_COUNT || mode > GEM_MODE_ENUMERATE) return GEM_ERR_ARG;
+  if (mode == GEM_MODE_ENUMERATE && emb_cap && !emb_out) return GEM_ERR_ARG;
+  std::memset(res, 0, sizeof *res);
+  if (threshold != 0) {
+    ctx->err = "relaxed matching (threshold > 0) is not supported";
+    res->status = GEM_ERR_LIMIT;
+    return GEM_ERR_LIMIT;
+  }
+  Wave w;
+  w.q.resize(1);
+  ST(make_host_query(q, w.q[0], ctx->err));
+  auto t0 = std::chrono::steady_clock::now();
+  ctx->arena.reset();
+  uint32_t *d_emb = nullptr;
+  if (mode == GEM_MODE_ENUMERATE && emb_cap) ST(aalloc(ctx, emb_cap * q->nv, &d_emb));
+  ST(run_wave(ctx, w, 0, mode, d_emb, emb_cap));
+  wave_result(ctx, w, 0, res);
+  if (mode == GEM_MODE_ENUMERATE) {
+    uint64_t nw = std::min<uint64_t>(w.emb_written, emb_cap);
+    res->n_written = nw;
+    if (nw) CU(cudaMemcpy(emb_out, d_emb, nw * q->nv * 4, cudaMemcpyDeviceToHost));
+    if (w.emb_written > emb_cap && res->status == GEM_OK) res->status = GEM_ERR_OVERFLOW;
+  }
+  res->ms[GEM_PH_HOST] = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return (gem_status)res->status;
+}
+
+extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode, gem_result *res) {
+  if (!ctx || (n && (!qs || !res))) return GEM_ERR_ARG;
+  if (mode != GEM_MODE_COUNT && mode != GEM_MODE_HASH) return GEM_ERR_ARG;
+  std::vector<HostQuery> all(n);
+  std::vector<gem_status> vs(n, GEM_OK);
+  for (uint32_t i = 0; i < n; ++i) {
+    std::memset(&res[i], 0, sizeof res[i]);
+    std::string e;
+    vs[i] = make_host_query(&qs[i], all[i], e);
+    res[i].status = vs[i];
+  }
+  // waves: as many queries as the per-wave row limit allows
+  const uint32_t max_rows = ctx->wave_max_rows;
+  uint32_t i = 0;
+  gem_status first_err = GEM_OK;
+  while (i < n) {
+    Wave w;
+    std::vector<uint32_t> ids;
+    uint32_t rows = 0;
+    while (i < n && (ids.empty() || rows + all[i].nv <= max_rows)) {
+      if (vs[i] == GEM_OK) {
+        ids.push_back(i);
+        rows += all[i].nv;
+        w.q.push_back(all[i]);
+      }
+      ++i;
+    }
+    if (ids.empty()) continue;
+    ctx->arena.reset();
+    gem_status st = run_wave(ctx, w, 0, mode, nullptr, 0);
+    if (st != GEM_OK) {
+      for (uint32_t id : ids) res[id].status = st;
+      if (first_err == GEM_OK) first_err = st;
+      continue;
+    }
+    for (size_t k = 0; k < ids.size(); ++k) wave_result(ctx, w, k, &res[ids[k]]);
+  }
+  for (uint32_t k = 0; k < n; ++k)
+    if (res[k].status != GEM_OK && first_err == GEM_OK) first_err = (gem_status)res[k].status;
+  return first_err;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI: phase entry points
+// ---------------------------------------------------------------------------
+extern "C" gem_status gem_filter(gem_ctx *ctx, const gem_query *q, uint32_t threshold, uint32_t *counts,
+                                 uint32_t *cand_out, uint64_t cand_cap) {
+  if (!ctx || !q || !counts) return GEM_ERR_ARG;
+  if (!ctx->loaded) return GEM_ERR_STATE;
+  Wave w;
+  w.q.resize(1);
+  ST(make_host_query(q, w.q[0], ctx->err));
+  ctx->arena.reset();
+  w.row_base.assign(1, 0);
+  ST(wave_filter(ctx, w, threshold));
+  CU(cudaStreamSynchronize(ctx->s));
+  for (uint32_t u = 0; u < q->nv; ++u) counts[u] = w.cnt[u];
+  if (w.cand_total > cand_cap) return GEM_ERR_OVERFLOW;
+  if (w.cand_total && cand_out)
+    CU(cudaMemcpy(cand_out, w.d_cand, w.cand_total * 4, cudaMemcpyDeviceToHost));
+  return GEM_OK;
+}
+
+extern "C" gem_status gem_edge_table(gem_ctx *ctx, const gem_query *q, uint32_t u, uint32_t wv,
+                                     uint64_t *offsets_out, uint64_t offsets_cap, uint32_t *values_out,
+                                     uint64_t values_cap, uint64_t *n_keys, uint64_t *n_values) {
+  if (!ctx || !q || !n_keys || !n_values) return GEM_ERR_ARG;
+  if (!ctx->loaded) return GEM_ERR_STATE;
+  Wave w;
+  w.q.resize(1);
+  ST(make_host_query(q, w.q[0], ctx->err));
+  const HostQuery &hq = w.q[0];
+  if (u >= hq.nv || wv >= hq.nv || !(hq.adj[u] & (1u << wv))) return GEM_ERR_ARG;
+  ctx->arena.reset();
+  w.row_base.assign(1, 0);
+  w.active.assign(1, 1);
+  ST(wave_filter(ctx, w, 0));
+  // a two-level plan: u then w
+  Plan p;
+  p.n = 2;
+  p.order[0] = u;
+  p.order[1] = wv;
+  p.back[1] = {0};
+  w.plan.assign(1, p);
+  ST(wave_tables(ctx, w));
+  CU(cudaStreamSynchronize(ctx->s));
+  const TabEdge &e = w.edges[0];
+  const uint64_t nk = w.cnt[u];
+  *n_keys = nk;
+  std::vector<uint64_t> off(nk + 1);
+  CU(cudaMemcpy(off.data(), e.offsets, 8 * (nk + 1), cudaMemcpyDeviceToHost));
+  const uint64_t base = off[0];
+  *n_values = off[nk] - base;
+  if (offsets_cap < nk + 1 || values_cap < off[nk] - base) return GEM_ERR_OVERFLOW;
+  for (uint64_t i = 0; i <= nk; ++i) offsets_out[i] = off[i] - base;
+  if (off[nk] > base) CU(cudaMemcpy(values_out, w.d_values + base, 4 * (off[nk] - base), cudaMemcpyDeviceToHost));
+  return GEM_OK;
+}
+
+extern "C" gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t u, uint32_t index_kind,
+                                      const uint32_t *keys, uint32_t n_keys, uint32_t *pos_out) {
+  if (!ctx || !q || (n_keys && (!keys || !pos_out))) return GEM_ERR_ARG;
+  if (index_kind != IDX_RANK && index_kind != IDX_CUCKOO) return GEM_ERR_ARG;
+  if (!ctx->loaded) return GEM_ERR_STATE;
+  Wave w;
+  w.q.resize(1);
+  ST(make_host_query(q, w.q[0], ctx->err));
+  if (u >= w.q[0].nv) return GEM_ERR_ARG;
+  ctx->arena.reset();
+  w.row_base.assign(1, 0);
+  w.active.assign(1, 1);
+  w.idx_kind.assign(1, std::vector<uint32_t>(QV, 0));
+  w.ck_of.assign(1, std::vector<const CuckooTable *>(QV, nullptr));
+  ST(wave_filter(ctx, w, 0));
+  uint32_t *d_keys, *d_out;
+  ST(aalloc(ctx, n_keys ? n_keys : 1, &d_keys));
+  ST(aalloc(ctx, n_keys ? n_keys : 1, &d_out));
+  if (n_keys) CU(cudaMemcpyAsync(d_keys, keys, 4ull * n_keys, cudaMemcpyHostToDevice, ctx->s));
+  if (index_kind == IDX_RANK) {
+    launch_rank_probe(w.d_rb + (uint64_t)u * w.nwords, d_keys, n_keys, d_out, ctx->s);
+  } else {
+    Plan p;
+    p.n = 2;
+    p.order[0] = u == 0 ? 1 % w.q[0].nv : 0;
+    p.order[1] = u;
+    p.need_idx[1] = 1;
+    w.plan.assign(1, p);
+    const uint32_t saved = ctx->opts.index_kind;
+    ctx->opts.index_kind = IDX_CUCKOO;
+    gem_status s = wave_index(ctx, w);
+    ctx->opts.index_kind = saved;
+    if (s != GEM_OK) return s;
+    launch_cuckoo_probe(w.ck_of[0][1], d_keys, n_keys, d_out, ctx->s);
+  }
+  CU(cudaGetLastError());
+  if (n_keys) CU(cudaMemcpyAsync(pos_out, d_out, 4ull * n_keys, cudaMemcpyDeviceToHost, ctx->s));
+  CU(cudaStreamSynchronize(ctx->s));
+  return GEM_OK;
+}

@@ -1,0 +1,97 @@
+// Host-side state of a libgem context (not part of the C-ABI).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gem_internal.h"
+#include "kernels.h"
+
+struct gem_ctx;
+
+// Device memory in chunks obtained from cudaMalloc; bump-allocated, reset
+// between waves so steady-state queries never call cudaMalloc.
+struct Arena {
+  struct Chunk {
+    char *base;
+    uint64_t size;
+    uint64_t used;
+  };
+  std::vector<Chunk> chunks;
+  size_t cur = 0;
+  uint64_t in_use = 0, peak = 0;
+  gem_status alloc(gem_ctx *ctx, uint64_t bytes, void **out);
+  void reset();
+  void release(gem_ctx *ctx);
+};
+
+// Matching order of one query.
+struct Plan {
+  uint32_t n = 0;
+  uint32_t order[gem::QV] = {};     // level -> query vertex
+  uint32_t level_of[gem::QV] = {};  // query vertex -> level
+  std::vector<uint32_t> back[gem::QV];  // backward neighbour levels
+  uint32_t dup_mask[gem::QV] = {};  // earlier levels with the same label
+  uint32_t need_idx[gem::QV] = {};  // level's vertex keys a later table
+};
+void make_plan(const gem::HostQuery &q, const uint32_t *cnt, Plan &p);
+
+// One wave: a set of queries processed by shared launches.
+struct Wave {
+  std::vector<gem::HostQuery> q;
+  std::vector<uint32_t> row_base;   // first filter row of each query
+  std::vector<uint8_t> active;      // 0 = some C(u) empty (count 0)
+  std::vector<Plan> plan;
+  std::vector<std::vector<uint32_t>> idx_kind;  // per query, per level
+  std::vector<std::vector<const gem::CuckooTable *>> ck_of;
+  std::vector<std::vector<uint32_t>> edge_of;   // per query: [j*QV+k] -> edge index
+  uint32_t nrows = 0, nwords = 0, nsrc = 0;
+  uint64_t *d_rb = nullptr;       // rank bitmaps, nrows x nwords
+  uint32_t *d_cand = nullptr;     // candidate lists back to back
+  std::vector<uint32_t> cnt;      // |C| per row
+  std::vector<uint64_t> c_base;   // list start per row
+  uint64_t cand_total = 0;
+  std::vector<gem::TabEdge> edges;
+  uint32_t *d_values = nullptr;
+  uint64_t table_values = 0, table_tiles = 0;
+  const gem::CuckooTable *ck_tabs = nullptr;
+  uint32_t cuckoo_round = 0;
+  std::vector<uint32_t> jq_index;
+  std::vector<gem::JOut> out;
+  uint64_t join_nodes = 0, join_scanned = 0, join_probes = 0, emb_written = 0;
+  uint32_t join_err = 0;
+  float filter_ms = 0, tables_ms = 0, index_ms = 0, join_ms = 0, total_ms = 0;
+  double plan_ms = 0;
+  uint64_t bytes_filter = 0, bytes_tables = 0, bytes_index = 0, bytes_join = 0;
+};
+
+struct gem_ctx {
+  gem_opts opts{};
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev[8] = {};
+  int sms = 148;
+  int join_bps[3] = {1, 1, 1};
+  uint64_t budget = 0, device_bytes = 0;
+  std::string err;
+  // graph
+  bool loaded = false;
+  gem::DevGraph g;
+  char *graph_mem = nullptr;
+  uint64_t graph_bytes = 0;
+  std::vector<uint64_t> label_freq;
+  // scratch
+  Arena arena;
+  gem::JControl *d_ctl = nullptr;
+  gem::JTask *d_queue = nullptr;
+  uint32_t *d_err = nullptr;
+  void *h_small = nullptr;
+  // tunables
+  uint32_t donate_max_level = 30;
+  uint32_t wave_max_rows = 4096;
+};
+
+gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_t *emb_dev, uint64_t emb_cap);
+void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r);

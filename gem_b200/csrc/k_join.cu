@@ -1,0 +1,585 @@
+// Edge join: depth-first extension of partial embeddings, one warp per task.
+//
+// Replaces the reference's level-at-a-time join (in-core/lib/join/src/
+// join_trie.cu:1087-1277: direct_join 397-718, refer_join 720-1023,
+// host_select 116-395 and the kernels of join_trie_kernel.cu:85-1099), which
+// materialises every intermediate level as {vertex, parent} columns, runs a
+// count kernel, a CUB scan, a host sync and an allocation per step, and only
+// skips materialising the last level.  Same result (the number of injective,
+// label-preserving, edge-preserving maps), different execution:
+//
+//  * the matching order is a chain of levels; level k's candidates are the
+//    edge-table lists T(u_j -> u_k)[pos of f(u_j) in C(u_j)] of all its
+//    backward neighbours u_j (tree edge and non-tree edges alike): the
+//    shortest list is scanned 32 candidates at a time (one per lane) and the
+//    others are probed by binary search, which covers the reference's
+//    "select" step for non-tree edges;
+//  * injectivity compares a candidate with the earlier levels of the same
+//    label only (the reference's dup_check_type, join_trie.cu:450-462);
+//  * the state of level L lives in lane L's registers (levels <= 32), so a
+//    warp's whole DFS stack costs a few registers per lane and no memory;
+//  * the last level is never materialised; in count mode a last level with a
+//    single backward neighbour is counted in O(#same-label earlier levels)
+//    binary searches instead of scanning its list;
+//  * one persistent grid serves every query of a wave: warps take root
+//    candidates from a global counter and, once roots run out, receive work
+//    donated by busy warps (half of the unread candidates of a shallow
+//    level) through a bounded lock-free queue.  Every wait is bounded by the
+//    device deadline; an expired deadline sets a TIMEOUT status.
+#include "device_common.cuh"
+#include "index_device.cuh"
+#include "kernels.h"
+
+namespace gem {
+
+using namespace dev;
+
+struct LaneState {   // lane L holds the state of level L
+  uint32_t f;        // matched data vertex
+  uint32_t idx;      // position of f in C(u_L)
+  uint64_t hs;       // hash prefix over levels 0..L
+  uint64_t pos;      // next unread position of the level's source range
+  uint64_t end;      // end of the level's source range
+  uint64_t cbase;    // first position of the current chunk
+  uint32_t mask;     // candidates of the current chunk not yet descended
+  uint32_t src;      // back entry scanned at this level
+};
+
+struct Stats {
+  uint64_t nodes = 0, scanned = 0, probes = 0;
+};
+
+// Per back entry i (lane i < nback): the list T(u_j -> u_lvl)[idx_j] as the
+// absolute range [lo, hi) of the values array.  Returns the shortest entry
+// (lowest index on ties) and its range, identical in every lane.
+__device__ __forceinline__ void level_lists(const JLevel *__restrict__ L, const JBack *__restrict__ backs,
+                                            const LaneState &c, uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi,
+                                            uint32_t &src, uint64_t &s_lo, uint64_t &s_hi) {
+  const uint32_t lane = lane_id();
+  nback = L->nback;
+  uint32_t klvl = 0;
+  const uint64_t *off = nullptr;
+  if (lane < nback) {
+    const JBack *b = backs + L->back_base + lane;
+    klvl = b->lvl;
+    off = b->off;
+  }
+  const uint32_t kidx = __shfl_sync(FULL, c.idx, klvl);
+  my_lo = 0;
+  my_hi = 0;
+  if (lane < nback) {
+    my_lo = __ldg(off + kidx);
+    my_hi = __ldg(off + kidx + 1);
+  }
+  uint64_t best = lane < nback ? my_hi - my_lo : ~0ull;
+  uint32_t bl = lane;
+#pragma unroll
+  for (int d = 16; d; d >>= 1) {
+    uint64_t ob = __shfl_xor_sync(FULL, best, d);
+    uint32_t ol = __shfl_xor_sync(FULL, bl, d);
+    if (ob < best || (ob == best && ol < bl)) {
+      best = ob;
+      bl = ol;
+    }
+  }
+  src = bl;
+  s_lo = __shfl_sync(FULL, my_lo, src);
+  s_hi = __shfl_sync(FULL, my_hi, src);
+}
+
+// Ranges of every back entry (lane i holds entry i), for a level whose
+// source entry is already known.
+__device__ __forceinline__ void level_ranges(const JLevel *__restrict__ L, const JBack *__restrict__ backs,
+                                             const LaneState &c, uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi) {
+  const uint32_t lane = lane_id();
+  nback = L->nback;
+  uint32_t klvl = 0;
+  const uint64_t *off = nullptr;
+  if (lane < nback) {
+    const JBack *b = backs + L->back_base + lane;
+    klvl = b->lvl;
+    off = b->off;
+  }
+  const uint32_t kidx = __shfl_sync(FULL, c.idx, klvl);
+  my_lo = 0;
+  my_hi = 0;
+  if (lane < nback) {
+    my_lo = __ldg(off + kidx);
+    my_hi = __ldg(off + kidx + 1);
+  }
+}
+
+// Evaluates the chunk [cpos, min(cpos + 32, end)) of the source list: a lane's
+// candidate survives if every other backward list contains it and no earlier
+// same-label level holds it.  Returns the ballot; *w receives the lane's value.
+__device__ __forceinline__ uint32_t eval_chunk(const uint32_t *__restrict__ values, uint64_t cpos, uint64_t end,
+                                               uint32_t nback, uint32_t src, uint64_t my_lo, uint64_t my_hi,
+                                               uint32_t dup_mask, const LaneState &c, uint32_t *w_out, Stats &st) {
+  const uint32_t lane = lane_id();
+  const uint64_t e = cpos + lane;
+  bool ok = e < end;
+  uint32_t w = ok ? __ldg(values + e) : 0u;
+  for (uint32_t i = 0; i < nback; ++i) {
+    const uint64_t lo = __shfl_sync(FULL, my_lo, i), hi = __shfl_sync(FULL, my_hi, i);
+    if (i == src) continue;
+    if (ok) ok = contains_u32(values, lo, hi, w);
+  }
+  uint32_t dm = dup_mask;
+  while (dm) {
+    const uint32_t j = __ffs(dm) - 1;
+    dm &= dm - 1;
+    const uint32_t fj = __shfl_sync(FULL, c.f, j);
+    if (w == fj) ok = false;
+  }
+  if (lane == 0) {
+    st.scanned += (end - cpos) < 32 ? (end - cpos) : 32;
+    st.probes += (uint64_t)(nback - 1) * ((end - cpos) < 32 ? (end - cpos) : 32);
+  }
+  *w_out = w;
+  return __ballot_sync(FULL, ok);
+}
+
+// Count-mode last level: number of valid candidates of level lvl.
+__device__ __forceinline__ uint64_t count_last(const JLevel *__restrict__ L, const JBack *__restrict__ backs,
+                                               const uint32_t *__restrict__ values, const LaneState &c, Stats &st) {
+  uint32_t nback, src;
+  uint64_t my_lo, my_hi, s_lo, s_hi;
+  level_lists(L, backs, c, nback, my_lo, my_hi, src, s_lo, s_hi);
+  const uint32_t dup_mask = L->dup_mask;
+  const uint32_t lane = lane_id();
+  if (nback == 1) {
+    bool hit = false;
+    if ((dup_mask >> lane) & 1u) hit = contains_u32(values, s_lo, s_hi, c.f);
+    if (lane == 0) st.probes += __popc(dup_mask);
+    return (s_hi - s_lo) - (uint64_t)__popc(__ballot_sync(FULL, hit));
+  }
+  uint64_t cnt = 0;
+  for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
+    uint32_t w;
+    cnt += __popc(eval_chunk(values, cp, s_hi, nback, src, my_lo, my_hi, dup_mask, c, &w, st));
+  }
+  return cnt;
+}
+
+__device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
+  return *reinterpret_cast<const volatile unsigned long long *>(p);
+}
+__device__ __forceinline__ unsigned int ld_vol(const unsigned int *p) {
+  return *reinterpret_cast<const volatile unsigned int *>(p);
+}
+
+// Bounded MPMC queue (sequence-numbered cells).  Called by a whole warp;
+// lane 0 reserves, every lane writes its share, lane 0 publishes.
+__device__ bool queue_push(JControl *ctl, JTask *cells, uint32_t q, uint32_t lvl, uint32_t src, uint64_t begin,
+                           uint64_t end, uint64_t hs, const LaneState &c) {
+  const uint32_t lane = lane_id();
+  unsigned long long slot = 0;
+  int ok = 0;
+  if (lane == 0) {
+    unsigned long long pos = ld_vol(&ctl->tail);
+    for (int tries = 0; tries < 32; ++tries) {
+      JTask *cell = cells + (pos & (TASK_CAP - 1));
+      const unsigned long long seq = ld_vol(&cell->seq);
+      const long long dif = (long long)seq - (long long)pos;
+      if (dif == 0) {
+        if (atomicCAS(&ctl->tail, pos, pos + 1) == pos) {
+          ok = 1;
+          slot = pos;
+          break;
+        }
+        pos = ld_vol(&ctl->tail);
+      } else if (dif < 0) {
+        break;  // full
+      } else {
+        pos = ld_vol(&ctl->tail);
+      }
+    }
+  }
+  ok = __shfl_sync(FULL, ok, 0);
+  slot = __shfl_sync(FULL, slot, 0);
+  if (!ok) return false;
+  JTask *cell = cells + (slot & (TASK_CAP - 1));
+  if (lane < lvl) {
+    cell->f[lane] = c.f;
+    cell->idx[lane] = c.idx;
+  }
+  if (lane == 0) {
+    cell->q = q;
+    cell->lvl = lvl;
+    cell->src = src;
+    cell->begin = begin;
+    cell->end = end;
+    cell->hs = hs;
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) *reinterpret_cast<volatile unsigned long long *>(&cell->seq) = slot + 1;
+  return true;
+}
+
+struct PoppedTask {
+  uint32_t q, lvl, src;
+  uint64_t begin, end, hs;
+};
+
+__device__ bool queue_pop(JControl *ctl, JTask *cells, PoppedTask &t, LaneState &c) {
+  const uint32_t lane = lane_id();
+  unsigned long long slot = 0;
+  int ok = 0;
+  if (lane == 0) {
+    unsigned long long pos = ld_vol(&ctl->head);
+    for (int tries = 0; tries < 32; ++tries) {
+      JTask *cell = cells + (pos & (TASK_CAP - 1));
+      const unsigned long long seq = ld_vol(&cell->seq);
+      const long long dif = (long long)seq - (long long)(pos + 1);
+      if (dif == 0) {
+        if (atomicCAS(&ctl->head, pos, pos + 1) == pos) {
+          ok = 1;
+          slot = pos;
+          break;
+        }
+        pos = ld_vol(&ctl->head);
+      } else if (dif < 0) {
+        break;  // empty
+      } else {
+        pos = ld_vol(&ctl->head);
+      }
+    }
+  }
+  ok = __shfl_sync(FULL, ok, 0);
+  slot = __shfl_sync(FULL, slot, 0);
+  if (!ok) return false;
+  __threadfence();
+  JTask *cell = cells + (slot & (TASK_CAP - 1));
+  t.q = __ldcg(&cell->q);
+  t.lvl = __ldcg(&cell->lvl);
+  t.src = __ldcg(&cell->src);
+  t.begin = __ldcg(reinterpret_cast<const unsigned long long *>(&cell->begin));
+  t.end = __ldcg(reinterpret_cast<const unsigned long long *>(&cell->end));
+  t.hs = __ldcg(reinterpret_cast<const unsigned long long *>(&cell->hs));
+  if (lane < t.lvl) {
+    c.f = __ldcg(&cell->f[lane]);
+    c.idx = __ldcg(&cell->idx[lane]);
+  }
+  __syncwarp();
+  __threadfence();
+  if (lane == 0) *reinterpret_cast<volatile unsigned long long *>(&cell->seq) = slot + TASK_CAP;
+  return true;
+}
+
+__device__ __forceinline__ uint32_t find_query(const uint64_t *__restrict__ rp, uint32_t nq, uint64_t r) {
+  uint32_t lo = 0, hi = nq;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(rp + mid) <= r) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t index_of(const JLevel *__restrict__ L, uint32_t w) {
+  const uint32_t kind = L->idx_kind;
+  if (kind == IDX_RANK) return rank_lookup(L->rb, w);
+  if (kind == IDX_CUCKOO) return ck_lookup(L->ck, w);
+  return 0u;
+}
+
+template <uint32_t MODE>
+__device__ __forceinline__ void emit_last(const JoinArgs &a, const JQuery *__restrict__ Q, uint32_t lvl, uint32_t m,
+                                          uint32_t w, const LaneState &c, uint64_t &lane_cnt, uint64_t &lane_hash) {
+  const uint32_t lane = lane_id();
+  const bool ok = (m >> lane) & 1u;
+  const uint64_t hsp = __shfl_sync(FULL, c.hs, lvl - 1);
+  if (ok) {
+    lane_cnt += 1;
+    lane_hash += mix64(hsp + emb_term(Q->lv[lvl].u, w));
+  }
+  if (MODE == MODE_ENUM) {
+    unsigned long long base = 0;
+    if (lane == 0 && m) base = atomicAdd(&a.ctl->emb_next, (unsigned long long)__popc(m));
+    base = __shfl_sync(FULL, base, 0);
+    const uint64_t slot = base + __popc(m & ((1u << lane) - 1u));
+    const bool wr = ok && slot < a.emb_cap;
+    const uint32_t n = Q->n;
+    for (uint32_t j = 0; j < lvl; ++j) {
+      const uint32_t fj = __shfl_sync(FULL, c.f, j);
+      if (wr) a.emb[slot * n + Q->lv[j].u] = fj;
+    }
+    if (wr) a.emb[slot * n + Q->lv[lvl].u] = w;
+  }
+}
+
+template <uint32_t MODE>
+__global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
+  const uint32_t lane = lane_id();
+  JControl *ctl = a.ctl;
+  const uint32_t *__restrict__ values = a.values;
+  const JBack *__restrict__ backs = a.backs;
+  const uint64_t deadline = ctl->deadline_ns;
+  LaneState c;
+  c.f = 0; c.idx = 0; c.hs = 0; c.pos = 0; c.end = 0; c.cbase = 0; c.mask = 0; c.src = 0;
+  Stats st;
+  bool idle_registered = false;
+
+  for (;;) {
+    // ------------------------------------------------------------ acquire
+    uint32_t q = 0, base_lvl = 0, lvl = 0;
+    bool have = false, from_root = false;
+    uint64_t r = 0;
+    if (!idle_registered) {
+      unsigned long long rr = 0;
+      if (lane == 0) {
+        atomicAdd(&ctl->busy, 1u);
+        __threadfence();
+        rr = atomicAdd(&ctl->root_next, 1ull);
+        if (rr >= a.n_roots) atomicSub(&ctl->busy, 1u);
+      }
+      r = __shfl_sync(FULL, rr, 0);
+      if (r < a.n_roots) {
+        have = true;
+        from_root = true;
+      } else {
+        idle_registered = true;
+        if (lane == 0) atomicAdd(&ctl->idle, 1u);
+      }
+    }
+    if (!have) {
+      uint32_t backoff = 64;
+      for (;;) {
+        if (lane == 0) {
+          atomicAdd(&ctl->busy, 1u);
+          __threadfence();
+        }
+        PoppedTask t;
+        if (queue_pop(ctl, a.queue, t, c)) {
+          if (lane == 0) atomicSub(&ctl->idle, 1u);
+          idle_registered = false;  // a finished donated task re-registers as idle below
+          q = t.q;
+          lvl = base_lvl = t.lvl;
+          const uint64_t hsp = __shfl_sync(FULL, t.hs, 0);
+          if (lane == lvl - 1) c.hs = hsp;
+          if (lane == lvl) {
+            c.src = t.src;
+            c.pos = t.begin;
+            c.end = t.end;
+            c.mask = 0;
+          }
+          have = true;
+          break;
+        }
+        int leave = 0;
+        if (lane == 0) {
+          atomicSub(&ctl->busy, 1u);
+          __threadfence();
+          const unsigned int b = ld_vol(&ctl->busy);
+          __threadfence();
+          const bool empty = ld_vol(&ctl->head) >= ld_vol(&ctl->tail);
+          if (b == 0 && empty) leave = 1;
+          if (ld_vol(&ctl->err) != DERR_NONE) leave = 1;
+          if (globaltimer_ns() > deadline) {
+            set_error(&ctl->err, DERR_TIMEOUT);
+            leave = 1;
+          }
+        }
+        if (__shfl_sync(FULL, leave, 0)) break;
+        __nanosleep(backoff);
+        backoff = backoff < 4096 ? backoff * 2 : 4096;
+      }
+      if (!have) {
+        if (lane == 0) atomicSub(&ctl->idle, 1u);
+        break;
+      }
+    }
+
+    // ------------------------------------------------------------ set up
+    uint64_t lane_cnt = 0, lane_hash = 0;
+    const JQuery *__restrict__ Q;
+    if (from_root) {
+      q = find_query(a.root_prefix, a.nquery, r);
+      Q = a.queries + q;
+      const uint32_t rl = (uint32_t)(r - Q->root_base);
+      const uint32_t w0 = __ldg(Q->root_cand + rl);
+      const uint64_t h0 = MODE == MODE_COUNT ? 0ull : emb_term(Q->root_u, w0);
+      if (lane == 0) {
+        c.f = w0;
+        c.idx = rl;
+        c.hs = h0;
+      }
+      const uint32_t n = Q->n;
+      if (n == 1) {
+        if (lane == 0) {
+          lane_cnt = 1;
+          lane_hash = mix64(h0);
+          if (MODE == MODE_ENUM) {
+            unsigned long long s = atomicAdd(&ctl->emb_next, 1ull);
+            if (s < a.emb_cap) a.emb[s] = w0;
+          }
+        }
+        lvl = 0;  // nothing to iterate
+        base_lvl = 1;
+      } else if (MODE == MODE_COUNT && n == 2) {
+        st.nodes += lane == 0;
+        const uint64_t k = count_last(&Q->lv[1], backs, values, c, st);
+        if (lane == 0) lane_cnt += k;
+        lvl = 0;
+        base_lvl = 1;
+      } else {
+        st.nodes += lane == 0;
+        uint32_t nb, src;
+        uint64_t lo, hi, s_lo, s_hi;
+        level_lists(&Q->lv[1], backs, c, nb, lo, hi, src, s_lo, s_hi);
+        if (lane == 1) {
+          c.src = src;
+          c.pos = s_lo;
+          c.end = s_hi;
+          c.mask = 0;
+        }
+        lvl = base_lvl = 1;
+      }
+    } else {
+      Q = a.queries + q;
+    }
+
+    // ------------------------------------------------------------ DFS
+    const uint32_t n = Q->n;
+    uint32_t iter = 0;
+    bool abort = false;
+    while (lvl >= base_lvl && lvl != 0) {
+      const JLevel *__restrict__ L = &Q->lv[lvl];
+      uint32_t mask = __shfl_sync(FULL, c.mask, lvl);
+      if (mask == 0) {
+        const uint64_t pos = __shfl_sync(FULL, c.pos, lvl), end = __shfl_sync(FULL, c.end, lvl);
+        if (pos >= end) {
+          --lvl;
+          continue;
+        }
+        if ((++iter & 255u) == 0) {
+          int stop = 0;
+          if (lane == 0) {
+            if (ld_vol(&ctl->err) != DERR_NONE) stop = 1;
+            else if (globaltimer_ns() > deadline) {
+              set_error(&ctl->err, DERR_TIMEOUT);
+              stop = 1;
+            }
+          }
+          if (__shfl_sync(FULL, stop, 0)) {
+            abort = true;
+            break;
+          }
+        }
+        uint32_t nb;
+        uint64_t lo, hi;
+        level_ranges(L, backs, c, nb, lo, hi);
+        const uint32_t src = __shfl_sync(FULL, c.src, lvl);
+        uint32_t w;
+        const uint32_t m = eval_chunk(values, pos, end, nb, src, lo, hi, L->dup_mask, c, &w, st);
+        if (MODE != MODE_COUNT && lvl == n - 1) {
+          emit_last<MODE>(a, Q, lvl, m, w, c, lane_cnt, lane_hash);
+          if (lane == lvl) c.pos = pos + 32;
+        } else {
+          uint64_t new_end = end;
+          if (lvl <= a.donate_max_level && end > pos + 32 + 64 && ld_vol(&ctl->idle) > 0) {
+            const uint64_t rem = pos + 32;
+            const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
+            if (mid < end) {
+              const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
+              if (queue_push(ctl, a.queue, q, lvl, src, mid, end, hsp, c)) new_end = mid;
+            }
+          }
+          if (lane == lvl) {
+            c.cbase = pos;
+            c.pos = pos + 32;
+            c.mask = m;
+            c.end = new_end;
+          }
+        }
+        continue;
+      }
+      // descend into the lowest remaining candidate
+      const uint32_t b = __ffs(mask) - 1;
+      const uint64_t cb = __shfl_sync(FULL, c.cbase, lvl);
+      if (lane == lvl) c.mask = mask & (mask - 1);
+      const uint32_t w = __ldg(values + cb + b);
+      const uint32_t widx = index_of(L, w);
+      const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
+      if (lane == lvl) {
+        c.f = w;
+        c.idx = widx;
+        if (MODE != MODE_COUNT) c.hs = hsp + emb_term(L->u, w);
+      }
+      if (lane == 0) {
+        st.nodes += 1;
+        st.probes += L->idx_kind != IDX_NONE;
+      }
+      const uint32_t nxt = lvl + 1;
+      if (MODE == MODE_COUNT && nxt == n - 1) {
+        const uint64_t k = count_last(&Q->lv[nxt], backs, values, c, st);
+        if (lane == 0) lane_cnt += k;
+        continue;
+      }
+      uint32_t nb, src;
+      uint64_t lo, hi, s_lo, s_hi;
+      level_lists(&Q->lv[nxt], backs, c, nb, lo, hi, src, s_lo, s_hi);
+      if (lane == nxt) {
+        c.src = src;
+        c.pos = s_lo;
+        c.end = s_hi;
+        c.mask = 0;
+      }
+      lvl = nxt;
+    }
+
+    // ------------------------------------------------------------ retire
+    uint64_t tc = lane_cnt, th = lane_hash;
+#pragma unroll
+    for (int d = 16; d; d >>= 1) {
+      tc += __shfl_xor_sync(FULL, tc, d);
+      th += __shfl_xor_sync(FULL, th, d);
+    }
+    if (lane == 0) {
+      if (tc) atomicAdd(&a.out[q].count, (unsigned long long)tc);
+      if (MODE != MODE_COUNT && th) atomicAdd(&a.out[q].hash, (unsigned long long)th);
+      __threadfence();
+      atomicSub(&ctl->busy, 1u);
+    }
+    if (abort) break;
+    if (!from_root && !idle_registered) {
+      idle_registered = true;
+      if (lane == 0) atomicAdd(&ctl->idle, 1u);
+    }
+  }
+  if (lane == 0 && (st.nodes | st.scanned | st.probes)) {
+    atomicAdd(&a.out[0].nodes, (unsigned long long)st.nodes);
+    atomicAdd(&a.out[0].scanned, (unsigned long long)st.scanned);
+    atomicAdd(&a.out[0].probes, (unsigned long long)st.probes);
+  }
+}
+
+__global__ void queue_init_kernel(JTask *cells) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < TASK_CAP; i += gridDim.x * blockDim.x)
+    cells[i].seq = i;
+}
+
+void join_queue_init(JTask *queue, cudaStream_t s) { queue_init_kernel<<<32, 256, 0, s>>>(queue); }
+
+int join_blocks_per_sm(uint32_t mode) {
+  int n = 0;
+  cudaError_t e;
+  if (mode == MODE_COUNT) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, join_kernel<MODE_COUNT>, 256, 0);
+  else if (mode == MODE_HASH) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, join_kernel<MODE_HASH>, 256, 0);
+  else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, join_kernel<MODE_ENUM>, 256, 0);
+  if (e != cudaSuccess || n <= 0) n = 1;
+  return n;
+}
+
+uint32_t launch_join(const JoinArgs &a, int blocks_per_sm, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint32_t grid = (uint32_t)(sms * (blocks_per_sm > 0 ? blocks_per_sm : 1));
+  if (a.mode == MODE_COUNT) join_kernel<MODE_COUNT><<<grid, 256, 0, s>>>(a);
+  else if (a.mode == MODE_HASH) join_kernel<MODE_HASH><<<grid, 256, 0, s>>>(a);
+  else join_kernel<MODE_ENUM><<<grid, 256, 0, s>>>(a);
+  return grid;
+}
+
+}  // namespace gem

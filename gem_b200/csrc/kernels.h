@@ -1,0 +1,221 @@
+// Launch wrappers and descriptor structs shared by the host orchestration
+// (ctx.cu) and the kernel translation units.  All pointers are device
+// pointers unless named h_*.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gem {
+
+constexpr uint32_t QV = 32;           // max query vertices
+constexpr uint32_t NLC_MAX_LABELS = 64;  // per-vertex label-count table kept up to this many labels
+
+// ---------------------------------------------------------------------------
+// Graph (device-resident CSR plus derived per-vertex data)
+// ---------------------------------------------------------------------------
+struct DevGraph {
+  uint32_t nv = 0;
+  uint64_t narcs = 0;
+  uint32_t nlabels = 0;     // max label + 1
+  uint32_t nlc_stride = 0;  // bytes per vertex in nlc (0: no table)
+  const uint64_t *off = nullptr;
+  const uint32_t *nbr = nullptr;
+  const uint32_t *lab = nullptr;
+  const uint32_t *deg = nullptr;
+  const uint8_t *nlc = nullptr;  // saturating neighbour-label counts
+};
+
+// Per-graph derived data, built once at load time.
+void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s);
+void launch_nlc(const DevGraph &g, uint8_t *nlc, uint32_t stride, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Generic exclusive scan (u64 results, n + 1 entries: out[n] = total)
+// ---------------------------------------------------------------------------
+enum ScanInput : uint32_t {
+  SCAN_POPC_U64LO = 0,  // popcount of the low 32 bits of a u64 word
+  SCAN_POPC_U32 = 1,    // popcount of a u32 word
+  SCAN_U32 = 2,         // plain u32 values
+};
+// out[i] = in[i * stride] for i < n.
+void launch_gather_strided(const uint64_t *in, uint64_t stride, uint32_t n, uint64_t *out, cudaStream_t s);
+// *deadline = device global timer + cap_ns.
+void launch_set_deadline(unsigned long long *deadline, uint64_t cap_ns, cudaStream_t s);
+// tmp needs scan_tmp_words(n) u64 words.
+uint64_t scan_tmp_words(uint64_t n);
+void launch_scan(const void *in, ScanInput kind, uint64_t n, uint64_t *out, uint64_t *tmp,
+                 cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Filter
+// ---------------------------------------------------------------------------
+struct FilterDesc {          // one query of a wave
+  uint32_t nq;               // query vertices
+  uint32_t nql;              // distinct labels in the query
+  uint32_t threshold;
+  uint32_t row_base;         // first rank-bitmap row of this query
+  uint32_t ql[QV];           // distinct labels
+  uint32_t lab[QV];          // label of each query vertex
+  uint32_t deg[QV];          // query degree of each vertex
+  uint8_t nlc[QV][QV];       // nlc[u][k]: neighbours of u with label ql[k]
+};
+
+// Writes the candidate bit of every (query vertex, data vertex) pair into the
+// low halves of rb (rows of nwords u64, row = row_base + u).
+void launch_filter(const DevGraph &g, const FilterDesc *d_desc, uint32_t nquery, uint64_t *rb,
+                   uint32_t nwords, cudaStream_t s);
+// Given ex = exclusive scan of popcounts over all rows, writes the per-word
+// ranks into the high halves of rb and the sorted candidate lists
+// cand[c_base[row] ...].
+void launch_compact(uint64_t *rb, const uint64_t *ex, uint32_t nrows, uint32_t nwords,
+                    const uint64_t *c_base, uint32_t *cand, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Edge-candidate tables
+// ---------------------------------------------------------------------------
+struct TabSource {           // a (query, query vertex) whose candidates are table keys
+  const uint32_t *keys;      // C(u), sorted
+  uint32_t nkeys;
+  uint32_t pad;
+  uint64_t key_base;         // first index of this source in the flattened key space
+};
+struct TabEdge {             // a directed table T(u -> w)
+  uint32_t src;              // index into TabSource
+  uint32_t pad;
+  const uint64_t *rb_w;      // rank bitmap row of the target w (membership)
+  uint64_t tile_base;        // first tile of this edge in the flattened edge-tile space
+  uint64_t ntiles;
+  uint64_t off_base;         // first entry of this edge in the flattened offsets space
+  uint64_t *offsets;         // nkeys + 1 absolute positions into the values array
+};
+// tiles[k] = ceil(deg(key k) / 32) over the flattened key space.
+void launch_key_tiles(const DevGraph &g, const TabSource *d_src, uint32_t nsrc, uint64_t nkeys,
+                      uint32_t *tiles, cudaStream_t s);
+// mask[t] = 32-bit membership mask of tile t of every edge.
+void launch_table_count(const DevGraph &g, const TabSource *d_src, const TabEdge *d_edge,
+                        uint32_t nedge, const uint64_t *tp, uint64_t total_tiles, uint32_t *mask,
+                        cudaStream_t s);
+// out[i] = tp[d_src[i].key_base] for i < nsrc, out[nsrc] = tp[nkeys].
+void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp,
+                              uint64_t *out, cudaStream_t s);
+void launch_table_offsets(const TabSource *d_src, const TabEdge *d_edge, uint32_t nedge,
+                          const uint64_t *tp, const uint64_t *vp, uint64_t total_offsets,
+                          cudaStream_t s);
+void launch_table_write(const DevGraph &g, const TabSource *d_src, const TabEdge *d_edge,
+                        uint32_t nedge, const uint64_t *tp, uint64_t total_tiles,
+                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Cuckoo hash: vertex id -> position in C(u).  Two bucketised tables of
+// 128-byte buckets (16 slots of {key, pos}) plus a small stash.
+// ---------------------------------------------------------------------------
+constexpr uint32_t CK_SLOTS = 16;         // slots per bucket (one 128-byte line)
+constexpr uint32_t CK_STASH = 64;
+constexpr uint32_t CK_MAX_KICKS = 64;
+constexpr uint64_t CK_EMPTY = ~0ull;
+struct CuckooTable {
+  uint64_t *t0;              // nb0 * 16 slots
+  uint64_t *t1;              // nb1 * 16 slots
+  uint64_t *stash;           // CK_STASH slots
+  uint32_t *stash_n;
+  uint32_t nb0, nb1;
+  uint64_t a0, c0, a1, c1;   // multiply-add hash parameters
+  const uint32_t *keys;      // C(u)
+  uint32_t nkeys;
+  uint32_t pad;
+  uint64_t key_base;         // first key of this table in the flattened build space
+};
+uint64_t cuckoo_slots_for(uint32_t nkeys, uint32_t *nb0, uint32_t *nb1);
+// Builds every table (keys inserted with pos = index); small tables are
+// assembled in shared memory and written out with coalesced stores.
+// Slots (t0, t1, stash) must be preset to CK_EMPTY and stash_n to 0.
+void launch_cuckoo_build(const CuckooTable *d_tabs, const CuckooTable *h_tabs, uint32_t ntab,
+                         uint32_t *err, cudaStream_t s);
+void launch_cuckoo_probe(const CuckooTable *d_tab, const uint32_t *keys, uint32_t n, uint32_t *out,
+                         cudaStream_t s);
+void launch_rank_probe(const uint64_t *rb, const uint32_t *keys, uint32_t n, uint32_t *out,
+                       cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Join (warp-level DFS over the matching order)
+// ---------------------------------------------------------------------------
+constexpr uint32_t IDX_NONE = 0, IDX_RANK = 1, IDX_CUCKOO = 2;
+
+struct JLevel {
+  uint32_t u;          // query vertex matched at this level
+  uint32_t nback;      // backward neighbours (tables keyed by earlier levels)
+  uint32_t back_base;  // first entry in the JBack array
+  uint32_t dup_mask;   // earlier levels with the same label (injectivity)
+  uint32_t idx_kind;   // how this level's vertex finds its position in C(u)
+  uint32_t pad;
+  const uint64_t *rb;          // IDX_RANK
+  const CuckooTable *ck;       // IDX_CUCKOO
+};
+struct JBack {
+  uint32_t lvl;              // level of the key vertex
+  uint32_t pad;
+  const uint64_t *off;       // table offsets (absolute into the values array)
+};
+struct JQuery {
+  uint32_t n;                // query vertices (levels)
+  uint32_t root_u;
+  const uint32_t *root_cand; // C(root)
+  uint32_t n_root;
+  uint32_t pad;
+  uint64_t root_base;        // first global root index of this query
+  JLevel lv[QV];             // lv[0] describes the root's index only
+};
+struct JOut {                // per query, accumulated with atomics
+  unsigned long long count;
+  unsigned long long hash;
+  unsigned long long written;
+  unsigned long long nodes;      // extended partial embeddings
+  unsigned long long scanned;    // source-list elements evaluated
+  unsigned long long probes;     // binary-search and index probes
+  unsigned long long pad[2];
+};
+constexpr uint32_t TASK_CAP = 8192;  // donation queue cells
+struct JTask {
+  unsigned long long seq;
+  uint32_t q, lvl, src;      // query, level whose candidates are donated, source back entry
+  uint32_t pad;
+  uint64_t begin, end;       // range in the values array
+  uint64_t hs;               // hash prefix of levels < lvl
+  uint32_t f[QV];
+  uint32_t idx[QV];
+};
+struct JControl {            // zeroed before every launch (except queue seq init)
+  unsigned long long root_next;
+  unsigned long long tail;
+  unsigned long long head;
+  unsigned int busy;
+  unsigned int idle;
+  unsigned int err;
+  unsigned int pad;
+  unsigned long long deadline_ns;
+  unsigned long long emb_next;   // enumerate cursor
+};
+enum : uint32_t { MODE_COUNT = 0, MODE_HASH = 1, MODE_ENUM = 2 };
+struct JoinArgs {
+  const JQuery *queries;
+  uint32_t nquery;
+  uint32_t mode;
+  const JBack *backs;
+  const uint32_t *values;     // edge-table values of the whole wave
+  const uint64_t *root_prefix; // nquery + 1 global root offsets
+  uint64_t n_roots;
+  JOut *out;
+  JControl *ctl;
+  JTask *queue;
+  uint32_t *emb;             // ENUM: output buffer
+  uint64_t emb_cap;          // embeddings that fit
+  uint32_t donate_max_level; // donate candidates of levels <= this
+  uint32_t pad;
+};
+void join_queue_init(JTask *queue, cudaStream_t s);
+// Launches the persistent join; returns the grid size used.
+uint32_t launch_join(const JoinArgs &a, int blocks_per_sm, cudaStream_t s);
+int join_blocks_per_sm(uint32_t mode);
+
+}  // namespace gem

@@ -1,0 +1,252 @@
+/*
+ * gem.h — C-ABI of libgem, a B200-native (sm_100a) edge-centric subgraph matcher.
+ *
+ * The reference (Seungsu-J/GEM) exposes no library API: its boundary is the
+ * `GEM` executable (in-core/src/main.cu:23-275, out-of-core/src/main.cu:412-460),
+ * the `t/v/e` text graph format (in-core/lib/io/src/io.cu:45-220) and a chain of
+ * process-global C++ phase functions:
+ *   filterSSM                                  in-core/lib/filter/include/filter.h:10
+ *   HashTable::build                           in-core/lib/structure/include/unifiedTrie.cuh:58
+ *   UnifiedTrieManager::initVertexTries        in-core/lib/structure/include/unifiedTrie.cuh:230
+ *   UnifiedTrieManager::construct_edge_candidates  in-core/lib/structure/include/unifiedTrie.cuh:244
+ *   join                                       in-core/lib/join/include/join_trie.cuh:31
+ * Each entry point below names the reference piece it replaces.  All state hangs
+ * off explicit handles (no process globals, no exit()); every call returns a
+ * gem_status.  Plain pointers and sizes only: callers own every array they pass.
+ *
+ * Semantics of a match (identical to the reference at threshold 0): an
+ * embedding of query q in data graph G is an injective map f: V(q) -> V(G) with
+ * label(f(u)) == label(u) for every u and {f(u), f(w)} in E(G) for every query
+ * edge {u, w}.  It is non-induced and no symmetry breaking is applied, so
+ * automorphic copies count separately (in-core/lib/join/src/join_trie_kernel.cu
+ * :270-1099 joins without any ordering constraint; injectivity is the same-label
+ * duplicate check of in-core/lib/join/src/join_trie.cu:450-462).
+ */
+#ifndef GEM_H
+#define GEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes.  Replaces `cuchk` -> exit(code)                             */
+/* (in-core/lib/utils/include/cuda_helpers.cuh:20-36).                        */
+/* ------------------------------------------------------------------------ */
+typedef enum gem_status {
+  GEM_OK = 0,
+  GEM_ERR_ARG = 1,      /* invalid argument (null pointer, size out of range) */
+  GEM_ERR_OOM = 2,      /* device/pinned budget exceeded; server: admission busy */
+  GEM_ERR_LIMIT = 3,    /* outside supported envelope (query > 32 vertices, threshold > 0 ...) */
+  GEM_ERR_TIMEOUT = 4,  /* a bounded device wait or the per-query time cap ran out */
+  GEM_ERR_CUDA = 5,     /* CUDA runtime error (message in gem_last_error) */
+  GEM_ERR_IO = 6,       /* file missing, malformed or inconsistent */
+  GEM_ERR_STATE = 7,    /* call out of order (no graph loaded, unknown ticket ...) */
+  GEM_ERR_OVERFLOW = 8, /* a result exceeded a caller buffer or a u64 counter */
+  GEM_ERR_INTERNAL = 9  /* internal consistency check failed */
+} gem_status;
+
+const char *gem_strerror(gem_status s);
+
+/* Limits of this build. */
+#define GEM_MAX_QV 32u     /* query vertices (reference: MAX_VQ=16, defs.h:20) */
+#define GEM_MAX_QE 496u    /* query edges: complete graph on 32 vertices       */
+
+/* ------------------------------------------------------------------------ */
+/* Host graphs (CSR with sorted adjacency).                                   */
+/* Replaces cpuGraph + readGraphToCPUStandard (in-core/lib/io/src/io.cu:45).  */
+/* ------------------------------------------------------------------------ */
+typedef struct gem_hgraph gem_hgraph;
+
+/* Copy caller arrays into a new host graph.  offsets: nv+1 entries, nbrs:
+ * offsets[nv] entries, labels: nv entries.  The graph must be undirected
+ * (every arc has its reverse), free of self loops and duplicates, with each
+ * adjacency list sorted ascending; violations return GEM_ERR_ARG. */
+gem_status gem_hgraph_create(uint32_t nv, const uint64_t *offsets,
+                             const uint32_t *nbrs, const uint32_t *labels,
+                             gem_hgraph **out);
+/* Read the reference's text format: `t V E`, `v id label degree` per vertex,
+ * `e src dst` per undirected edge (in-core/lib/io/src/io.cu:45-127).  Vertex
+ * lines may come in any order; declared degrees must match the edges. */
+gem_status gem_hgraph_read_text(const char *path, gem_hgraph **out);
+/* Write the text format with ascending vertex lines and lexicographically
+ * sorted (src < dst) edge lines — the layout the reference's reader needs to
+ * build a sorted CSR. */
+gem_status gem_hgraph_write_text(const gem_hgraph *g, const char *path);
+/* R-MAT generator: 2^scale vertices, edge_factor * 2^scale sampled edges with
+ * quadrant probabilities (a, b, c, 1-a-b-c); self loops and duplicates are
+ * dropped and the result symmetrised.  Deterministic for a seed, independent
+ * of thread count.  All labels start at 0. */
+gem_status gem_hgraph_rmat(uint32_t scale, uint32_t edge_factor, double a,
+                           double b, double c, uint64_t seed, gem_hgraph **out);
+/* Assign labels 0..nlabels-1: uniform when zipf_s == 0, else Zipf(zipf_s)
+ * with P(l) proportional to 1/(l+1)^s.  Deterministic for a seed. */
+gem_status gem_hgraph_set_labels(gem_hgraph *g, uint32_t nlabels, double zipf_s,
+                                 uint64_t seed);
+gem_status gem_hgraph_info(const gem_hgraph *g, uint32_t *nv,
+                           uint64_t *n_arcs, uint32_t *max_label_plus1,
+                           uint32_t *max_degree);
+/* Borrow read-only views of the CSR arrays (valid until destroy). */
+gem_status gem_hgraph_view(const gem_hgraph *g, const uint64_t **offsets,
+                           const uint32_t **nbrs, const uint32_t **labels);
+void gem_hgraph_destroy(gem_hgraph *g);
+
+/* ------------------------------------------------------------------------ */
+/* Queries.                                                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct gem_query {
+  uint32_t nv;             /* vertices 0..nv-1, 1 <= nv <= GEM_MAX_QV */
+  uint32_t ne;             /* undirected edges */
+  const uint32_t *labels;  /* nv labels, compared by value with data labels */
+  const uint32_t *edges;   /* 2*ne entries: (src, dst) per undirected edge */
+} gem_query;
+
+/* Read a query in the text format (same reader as data graphs).  Writes
+ * nv labels and 2*ne edge endpoints (edges in file order). */
+gem_status gem_query_read_text(const char *path, uint32_t *nv, uint32_t *ne,
+                               uint32_t *labels /* >= GEM_MAX_QV */,
+                               uint32_t *edges /* >= 2*GEM_MAX_QE */);
+gem_status gem_query_write_text(const gem_query *q, const char *path);
+
+/* Random-walk query extraction: walk from a uniformly drawn vertex until k
+ * distinct vertices are visited, keep all induced edges, relabel vertices
+ * 0..k-1 in visit order and copy their labels (so every query has >= 1
+ * match).  density: 0 = any, 1 = sparse (average degree <= 3), 2 = dense
+ * (average degree > 3).  Sparse requests whose induced walk stays dense
+ * after `max_tries` walks keep the walk's first-visit tree plus induced edges
+ * in vertex order while the average degree stays <= 3.  Outputs for query i:
+ * ne_out[i], labels_out[i*k .. +k), edges_out[i*2*max_e .. +2*ne_out[i]). */
+gem_status gem_gen_queries(const gem_hgraph *g, uint32_t k, int density,
+                           uint32_t count, uint64_t seed, uint32_t max_e,
+                           uint32_t *ne_out, uint32_t *labels_out,
+                           uint32_t *edges_out);
+
+/* ------------------------------------------------------------------------ */
+/* Device context: one GPU, resident data graph, memory budget.              */
+/* Replaces main()'s global setup + aggressive_warmup                        */
+/* (in-core/src/main.cu:45-76, in-core/lib/utils/src/cuda_helpers.cu:24-73). */
+/* ------------------------------------------------------------------------ */
+typedef struct gem_ctx gem_ctx;
+
+typedef struct gem_opts {
+  int device;                   /* CUDA device ordinal */
+  uint64_t device_budget_bytes; /* 0 = 90% of free memory at create time */
+  uint64_t pinned_budget_bytes; /* pinned host pool (out-of-core mode) */
+  int ooc;                      /* 1 = keep the data graph in pinned host memory */
+  uint32_t time_cap_ms;         /* per-query/batch device time cap (0 = 600000) */
+  uint32_t index_kind;          /* 0 = auto, 1 = rank bitmap, 2 = cuckoo hash */
+  uint32_t reserved[6];
+} gem_opts;
+
+gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out);
+void gem_ctx_destroy(gem_ctx *ctx);
+/* Thread-local description of the last failure on this context. */
+const char *gem_last_error(const gem_ctx *ctx);
+
+/* Upload (in-core) or pin (out-of-core) a host graph; derived per-graph
+ * indexes (degrees, neighbour-label counts) are built on the device.
+ * Replaces allocateMemGPU/copyGraphToGPU (in-core/lib/io/src/io.cu:348-452). */
+gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *g);
+
+/* ------------------------------------------------------------------------ */
+/* Queries on the device.                                                     */
+/* ------------------------------------------------------------------------ */
+enum {
+  GEM_MODE_COUNT = 0,     /* u64 count only (the reference's output)        */
+  GEM_MODE_HASH = 1,      /* count + order-independent embedding hash        */
+  GEM_MODE_ENUMERATE = 2  /* count + hash + embeddings written to a buffer   */
+};
+
+/* Per-phase timing slots of gem_result.ms (device time from CUDA events). */
+enum {
+  GEM_PH_FILTER = 0, GEM_PH_INDEX = 1, GEM_PH_TABLES = 2, GEM_PH_JOIN = 3,
+  GEM_PH_TOTAL = 4, GEM_PH_H2D = 5, GEM_PH_D2H = 6, GEM_PH_HOST = 7
+};
+
+typedef struct gem_result {
+  uint64_t count;        /* number of embeddings (exact, u64) */
+  uint64_t emb_hash;     /* sum over embeddings of gem_embedding_hash (HASH/ENUMERATE) */
+  uint64_t n_written;    /* embeddings written (ENUMERATE) */
+  uint32_t status;       /* gem_status of this query */
+  uint32_t n_tables;     /* directed edge tables built */
+  uint64_t cand_total;   /* sum over query vertices of |C(u)| */
+  uint64_t table_total;  /* sum of edge-table value counts */
+  uint64_t nodes;        /* partial embeddings extended by the join (all levels) */
+  uint64_t bytes_alg[4]; /* algorithmic bytes: filter, index, tables, join */
+  float ms[8];           /* GEM_PH_* */
+} gem_result;
+
+/* Run one query end to end on the device (filter -> index -> edge tables ->
+ * join), synchronously.  threshold must be 0 (exact matching).  In
+ * ENUMERATE mode up to emb_cap embeddings are written to emb_out as nv u32
+ * per embedding in query-vertex order (order of embeddings unspecified);
+ * more than emb_cap embeddings return GEM_ERR_OVERFLOW with the exact count.
+ * Replaces main()'s phase chain (in-core/src/main.cu:140-236). */
+gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold,
+                         int mode, uint32_t *emb_out, uint64_t emb_cap,
+                         gem_result *res);
+
+/* Run many queries in one persistent join launch (waves sized to the device
+ * budget), each query's result identical to gem_query_run's.
+ * Replaces the out-of-core directory batch loop (out-of-core/src/main.cu:334-410). */
+gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n,
+                         int mode, gem_result *res);
+
+/* Embedding hash of one embedding f (f[u] = data vertex of query vertex u):
+ * h = mix(sum_u mix(f[u] | u << 32)) with mix the splitmix64 finaliser of
+ * (x + 0x9E3779B97F4A7C15); GEM_MODE_HASH reports the sum of h over all
+ * embeddings (mod 2^64), which does not depend on enumeration order. */
+uint64_t gem_embedding_hash(const uint32_t *f, uint32_t nv);
+
+/* ------------------------------------------------------------------------ */
+/* Phase entry points (parity testing and tooling).                           */
+/* ------------------------------------------------------------------------ */
+/* Candidate filter: C(u) for every query vertex u, sorted ascending:
+ * label(v) == label(u), deg(u) <= deg(v) + threshold and
+ * sum_l max(0, nlc_u[l] - nlc_v[l]) <= threshold over the labels present in
+ * the query.  counts[u] = |C(u)|; cand_out receives the lists back to back
+ * (u = 0 first); needs sum counts <= cand_cap.
+ * Replaces filterSSM (in-core/lib/filter/src/filter.cu:34-167). */
+gem_status gem_filter(gem_ctx *ctx, const gem_query *q, uint32_t threshold,
+                      uint32_t *counts, uint32_t *cand_out, uint64_t cand_cap);
+
+/* Edge-candidate table T(u -> w) for the query edge {u, w}: for the i-th
+ * candidate v of C(u), the values are N(v) ∩ C(w) in adjacency (ascending)
+ * order.  offsets_out has |C(u)|+1 entries; values_out needs offsets[|C(u)|]
+ * <= values_cap entries.  *n_keys and *n_values receive the sizes (also when
+ * the buffers are too small, which returns GEM_ERR_OVERFLOW).
+ * Replaces construct_edge_candidates for one directed edge
+ * (in-core/lib/structure/src/unifiedTrie.cu:1020-1240). */
+gem_status gem_edge_table(gem_ctx *ctx, const gem_query *q, uint32_t u,
+                          uint32_t w, uint64_t *offsets_out, uint64_t offsets_cap,
+                          uint32_t *values_out, uint64_t values_cap,
+                          uint64_t *n_keys, uint64_t *n_values);
+
+/* Index probe: position of each data vertex keys[i] in C(u) (or 0xFFFFFFFF
+ * when absent) through the device index of kind index_kind (1 = rank bitmap,
+ * 2 = cuckoo hash).  Replaces HashTable::build + hash_lookup
+ * (in-core/lib/structure/src/unifiedTrie.cu:175-433,
+ *  in-core/lib/structure/include/unifiedTrie.cuh:84-125). */
+gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t u,
+                           uint32_t index_kind, const uint32_t *keys,
+                           uint32_t n_keys, uint32_t *pos_out);
+
+/* ------------------------------------------------------------------------ */
+/* Serving: continuous batching with memory-based admission.                 */
+/* ------------------------------------------------------------------------ */
+/* Submit a query; returns GEM_ERR_OOM when its estimated device bytes do not
+ * fit the admission budget right now (caller retries later). */
+gem_status gem_submit(gem_ctx *ctx, const gem_query *q, int mode,
+                      uint64_t *ticket);
+/* Advance the server (admit queued work, launch, retire finished queries)
+ * and report whether `ticket` is done; *done = 1 fills *res. */
+gem_status gem_poll(gem_ctx *ctx, uint64_t ticket, gem_result *res, int *done);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GEM_H */

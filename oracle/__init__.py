@@ -1,0 +1,121 @@
+"""CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+ctypes binding to oracle/_build/liboracle.so (built from oracle/oracle.c by
+gem_b200.build / __graft_entry__.build).  Only the test suite, the smoke
+check and the CPU-baseline leg of bench.py may import this module; libgem
+never uses it.  See oracle/oracle.c for the reference semantics it restates.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_DIR, "_build", "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"oracle not built at {LIB_PATH}")
+        L = C.CDLL(LIB_PATH)
+        u32p, u64p = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)
+        L.oracle_emb_hash.argtypes = [u32p, C.c_uint32]
+        L.oracle_emb_hash.restype = C.c_uint64
+        L.oracle_filter.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p, C.c_uint32,
+                                    u32p, u32p, C.c_uint64]
+        L.oracle_edge_table.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u64p, u32p,
+                                        C.c_uint64]
+        L.oracle_edge_table.restype = C.c_int64
+        L.oracle_count.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p, C.c_int,
+                                   C.c_int, C.c_uint64, u64p, u64p, u64p]
+        L.oracle_brute.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p, u64p, u64p]
+        _lib = L
+    return _lib
+
+
+def _p32(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _p64(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint64))
+
+
+def _graph(g):
+    """Accepts (offsets, nbrs, labels) numpy arrays or any object with .arrays()."""
+    off, nbr, lab = g.arrays() if hasattr(g, "arrays") else g
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    nbr = np.ascontiguousarray(nbr, dtype=np.uint32)
+    if nbr.size == 0:
+        nbr = np.zeros(1, np.uint32)
+    lab = np.ascontiguousarray(lab, dtype=np.uint32)
+    return off, nbr, lab
+
+
+def _query(q):
+    lab = np.ascontiguousarray(q.labels, dtype=np.uint32)
+    edg = np.ascontiguousarray(q.edges, dtype=np.uint32).reshape(-1)
+    if edg.size == 0:
+        edg = np.zeros(2, np.uint32)
+    return lab, edg, int(q.labels.shape[0]), int(q.edges.shape[0])
+
+
+def emb_hash(f):
+    f = np.ascontiguousarray(f, dtype=np.uint32)
+    return int(lib().oracle_emb_hash(_p32(f), len(f)))
+
+
+def count(g, q, threads=0, want_hash=True, work_cap=0):
+    """(count, hash, complete) by backtracking; work_cap bounds scanned arcs."""
+    off, nbr, lab = _graph(g)
+    ql, qe, qn, qm = _query(q)
+    c, h, n = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    r = lib().oracle_count(len(lab), _p64(off), _p32(nbr), _p32(lab), qn, _p32(ql), qm, _p32(qe), threads,
+                           1 if want_hash else 0, work_cap, C.byref(c), C.byref(h), C.byref(n))
+    if r < 0:
+        raise ValueError("oracle_count rejected the query")
+    return int(c.value), int(h.value), r == 0
+
+
+def brute(g, q):
+    off, nbr, lab = _graph(g)
+    ql, qe, qn, qm = _query(q)
+    c, h = C.c_uint64(), C.c_uint64()
+    r = lib().oracle_brute(len(lab), _p64(off), _p32(nbr), _p32(lab), qn, _p32(ql), qm, _p32(qe), C.byref(c),
+                           C.byref(h))
+    if r != 0:
+        raise ValueError("brute force supports nv <= 64 data vertices and <= 8 query vertices")
+    return int(c.value), int(h.value)
+
+
+def filter(g, q, threshold=0):
+    off, nbr, lab = _graph(g)
+    ql, qe, qn, qm = _query(q)
+    counts = np.zeros(qn, np.uint32)
+    cap = qn * len(lab)
+    cand = np.zeros(max(cap, 1), np.uint32)
+    r = lib().oracle_filter(len(lab), _p64(off), _p32(nbr), _p32(lab), qn, _p32(ql), qm, _p32(qe), threshold,
+                            _p32(counts), _p32(cand), cap)
+    assert r == 0
+    out, at = [], 0
+    for u in range(qn):
+        out.append(cand[at:at + int(counts[u])].copy())
+        at += int(counts[u])
+    return out
+
+
+def edge_table(g, cu, cw):
+    off, nbr, lab = _graph(g)
+    cu = np.ascontiguousarray(cu, dtype=np.uint32)
+    cw = np.ascontiguousarray(cw, dtype=np.uint32)
+    offsets = np.zeros(len(cu) + 1, np.uint64)
+    cap = int(sum(int(off[v + 1] - off[v]) for v in cu)) + 1
+    vals = np.zeros(cap, np.uint32)
+    r = lib().oracle_edge_table(len(lab), _p64(off), _p32(nbr), _p32(cu if cu.size else np.zeros(1, np.uint32)),
+                                len(cu), _p32(cw if cw.size else np.zeros(1, np.uint32)), len(cw), _p64(offsets),
+                                _p32(vals), cap)
+    assert r >= 0
+    return offsets, vals[:r].copy()

@@ -1,0 +1,207 @@
+"""GPU path (libgem, sm_100a) against the CPU oracle and the golden fixtures.
+Bit-exact: integer counts, candidate lists, tables and hashes must be equal."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import gem_b200 as gem
+import oracle
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "cases.json")
+
+
+def cases():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def small():
+    # config-1 shape at reduced size: R-MAT scale 12, edge factor 8, 4 uniform labels
+    g = gem.HostGraph.rmat(12, 8, seed=0x47454D00 + 12).set_labels(4, 0.0, seed=0x47454D0C ^ 0x4C)
+    return g
+
+
+@pytest.fixture(scope="module")
+def gctx(small):
+    c = gem.Context(time_cap_ms=120000)
+    c.load_graph(small)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("case", cases(), ids=lambda c: c["name"])
+def test_golden_counts_and_hash(case):
+    g = gem.HostGraph.from_edges(case["nv"], case["edges"], case["labels"])
+    q = gem.Query(case["qlabels"], case["qedges"])
+    with gem.Context() as c:
+        c.load_graph(g)
+        r = c.run(q, mode=gem.MODE_HASH)
+    assert r["status"] == "OK"
+    assert r["count"] == case["count"]
+    assert r["emb_hash"] == int(case["hash"])
+
+
+def test_filter_matches_oracle(small, gctx):
+    for k, dens in ((4, gem.ANY), (8, gem.SPARSE), (8, gem.DENSE), (16, gem.ANY)):
+        for q in gem.gen_queries(small, k, dens, 3, seed=100 + k):
+            for T in (0, 1, 2):
+                got = gctx.filter(q, threshold=T)
+                exp = oracle.filter(small, q, threshold=T)
+                for u in range(q.nv):
+                    assert np.array_equal(got[u], exp[u]), (k, T, u)
+
+
+def test_edge_tables_match_oracle(small, gctx):
+    for q in gem.gen_queries(small, 6, gem.ANY, 3, seed=5):
+        cand = oracle.filter(small, q)
+        for a, b in q.edges.tolist():
+            for u, w in ((a, b), (b, a)):
+                off, vals = gctx.edge_table(q, u, w)
+                eo, ev = oracle.edge_table(small, cand[u], cand[w])
+                assert np.array_equal(off, eo), (u, w)
+                assert np.array_equal(vals, ev), (u, w)
+
+
+@pytest.mark.parametrize("kind", [gem.IDX_RANK, gem.IDX_CUCKOO])
+def test_index_probe_positions(small, gctx, kind):
+    for q in gem.gen_queries(small, 5, gem.ANY, 2, seed=9):
+        cand = oracle.filter(small, q)
+        for u in range(q.nv):
+            keys = cand[u]
+            pos = gctx.index_probe(q, u, keys, kind=kind)
+            assert np.array_equal(pos, np.arange(len(keys), dtype=np.uint32))
+            # absent keys report 0xFFFFFFFF
+            absent = np.setdiff1d(np.arange(0, small.nv, 7, dtype=np.uint32), keys)[:200]
+            if len(absent):
+                assert np.all(gctx.index_probe(q, u, absent, kind=kind) == 0xFFFFFFFF)
+
+
+def test_cuckoo_large_table():
+    # one label: every vertex is a candidate -> table far above the shared-memory path
+    g = gem.HostGraph.rmat(15, 4, seed=3).set_labels(1)
+    q = gem.Query([0, 0], [(0, 1)])
+    with gem.Context() as c:
+        c.load_graph(g)
+        cand = oracle.filter(g, q)[0]
+        pos = c.index_probe(q, 0, cand, kind=gem.IDX_CUCKOO)
+        assert np.array_equal(pos, np.arange(len(cand), dtype=np.uint32))
+
+
+@pytest.mark.parametrize("k,dens,n", [(3, gem.ANY, 6), (4, gem.ANY, 8), (5, gem.SPARSE, 6), (6, gem.DENSE, 6),
+                                      (8, gem.SPARSE, 4), (8, gem.DENSE, 4)])
+def test_counts_match_oracle(small, gctx, k, dens, n):
+    for q in gem.gen_queries(small, k, dens, n, seed=1000 + k * 10 + dens):
+        exp, eh, ok = oracle.count(small, q, threads=0, work_cap=400_000_000)
+        if not ok:
+            continue
+        r = gctx.run(q, mode=gem.MODE_HASH)
+        assert r["status"] == "OK"
+        assert r["count"] == exp, (q.labels.tolist(), q.edges.tolist())
+        assert r["emb_hash"] == eh
+        rc = gctx.run(q, mode=gem.MODE_COUNT)
+        assert rc["count"] == exp
+
+
+@pytest.mark.parametrize("kind", [gem.IDX_RANK, gem.IDX_CUCKOO])
+def test_index_kinds_same_counts(small, kind):
+    with gem.Context(index_kind=kind) as c:
+        c.load_graph(small)
+        for q in gem.gen_queries(small, 5, gem.ANY, 4, seed=31):
+            exp, eh, ok = oracle.count(small, q, work_cap=400_000_000)
+            if ok:
+                r = c.run(q, mode=gem.MODE_HASH)
+                assert (r["count"], r["emb_hash"]) == (exp, eh)
+
+
+def test_enumerate_embeddings(small, gctx):
+    for q in gem.gen_queries(small, 4, gem.ANY, 3, seed=77):
+        exp, eh, ok = oracle.count(small, q)
+        if not ok or exp > 2_000_000:
+            continue
+        r = gctx.run(q, mode=gem.MODE_ENUMERATE, emb_cap=exp + 10)
+        assert r["count"] == exp and r["n_written"] == exp and r["emb_hash"] == eh
+        emb = r["embeddings"]
+        # every row is a valid embedding, rows are distinct, hashes add up
+        off, nbr, lab = small.arrays()
+        assert np.all(lab[emb] == q.labels[None, :])
+        for a, b in q.edges.tolist():
+            x, y = emb[:, a].astype(np.int64), emb[:, b].astype(np.int64)
+            s = np.searchsorted(nbr[:0], [])  # noqa: keep numpy happy on empty
+            for i in range(0, len(emb), max(1, len(emb) // 200)):
+                lst = nbr[off[x[i]]:off[x[i] + 1]]
+                assert y[i] in lst
+        assert len(np.unique(emb, axis=0)) == len(emb)
+        h = 0
+        for row in emb[: min(len(emb), 3000)]:
+            h = (h + gem.embedding_hash(row)) % (1 << 64)
+        if len(emb) <= 3000:
+            assert h == eh
+
+
+def test_enumerate_overflow_keeps_exact_count(small, gctx):
+    q = gem.gen_queries(small, 4, gem.ANY, 1, seed=5)[0]
+    exp, _, ok = oracle.count(small, q)
+    assert ok and exp > 10
+    r = gctx.run(q, mode=gem.MODE_ENUMERATE, emb_cap=10)
+    assert r["status"] == "ERR_OVERFLOW" and r["count"] == exp and r["n_written"] == 10
+
+
+def test_batch_equals_plain(small, gctx):
+    qs = []
+    for k in (2, 3, 4, 5, 6, 8):
+        qs += gem.gen_queries(small, k, gem.ANY, 4, seed=500 + k)
+    plain = [gctx.run(q, mode=gem.MODE_HASH) for q in qs]
+    st, batch = gctx.batch(qs, mode=gem.MODE_HASH)
+    assert st == 0
+    for p, b in zip(plain, batch):
+        assert (p["count"], p["emb_hash"]) == (b["count"], b["emb_hash"])
+
+
+def test_edge_cases(small, gctx):
+    off, nbr, lab = small.arrays()
+    # single vertex: count = vertices with that label
+    q1 = gem.Query([lab[0]], [])
+    assert gctx.run(q1)["count"] == int(np.sum(lab == lab[0]))
+    # label absent from the data graph: 0
+    assert gctx.run(gem.Query([0, 99], [(0, 1)]))["count"] == 0
+    # single edge (the reference prints no result for |E_q| <= 1)
+    q2 = gem.Query([0, 1], [(0, 1)])
+    exp, _, _ = oracle.count(small, q2)
+    assert gctx.run(q2)["count"] == exp
+    # same-label star (injectivity among leaves)
+    q3 = gem.Query([0, 0, 0, 0], [(0, 1), (0, 2), (0, 3)])
+    exp, eh, ok = oracle.count(small, q3, work_cap=500_000_000)
+    if ok:
+        r = gctx.run(q3, mode=gem.MODE_HASH)
+        assert (r["count"], r["emb_hash"]) == (exp, eh)
+    # invalid queries are rejected on the host
+    with pytest.raises(gem.GemError):
+        gctx.run(gem.Query([0, 1, 2], [(0, 1)]))  # disconnected
+    with pytest.raises(gem.GemError):
+        gctx.run(gem.Query([0, 1], [(0, 0)]))  # self loop
+    with pytest.raises(gem.GemError):
+        gctx.run(gem.Query([0, 1], [(0, 1)]), threshold=1)
+
+
+def test_max_size_queries(small, gctx):
+    for q in gem.gen_queries(small, 32, gem.DENSE, 2, seed=3210):
+        exp, eh, ok = oracle.count(small, q, work_cap=200_000_000)
+        r = gctx.run(q, mode=gem.MODE_HASH)
+        if ok:
+            assert (r["count"], r["emb_hash"]) == (exp, eh)
+
+
+def test_time_cap_reports_timeout():
+    g = gem.HostGraph.rmat(16, 16, seed=1).set_labels(1)
+    q = gem.Query([0] * 6, [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5)])
+    with gem.Context(time_cap_ms=50) as c:
+        c.load_graph(g)
+        r = c.run(q, raise_on_error=False)
+        assert r["status"] == "ERR_TIMEOUT"
+        # the context stays usable after a timeout
+        r2 = c.run(gem.Query([0], []))
+        assert r2["status"] == "OK" and r2["count"] == g.nv

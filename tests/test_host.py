@@ -1,0 +1,127 @@
+"""Host-side logic of libgem: ABI exports, generators, text IO, validation.
+No device calls."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import gem_b200 as gem
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "gem.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gem_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(gem.LIB_PATH)
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) == set(gem.EXPORTS)
+
+
+def test_strerror():
+    L = gem.lib()
+    assert L.gem_strerror(0) == b"ok"
+    assert b"time" in L.gem_strerror(4)
+
+
+def test_rmat_deterministic_and_valid():
+    a = gem.HostGraph.rmat(12, 8, seed=99)
+    b = gem.HostGraph.rmat(12, 8, seed=99)
+    c = gem.HostGraph.rmat(12, 8, seed=100)
+    oa, na, _ = a.arrays()
+    ob, nb, _ = b.arrays()
+    oc, nc, _ = c.arrays()
+    assert np.array_equal(oa, ob) and np.array_equal(na, nb)
+    assert not (len(nc) == len(na) and np.array_equal(nc, na))
+    # sorted, no self loops, symmetric
+    for v in range(len(oa) - 1):
+        lst = na[oa[v]:oa[v + 1]]
+        assert np.all(np.diff(lst.astype(np.int64)) > 0)
+        assert v not in lst
+    src = np.repeat(np.arange(len(oa) - 1), np.diff(oa).astype(np.int64))
+    fwd = set(zip(src.tolist(), na.tolist()))
+    assert all((d, s) in fwd for s, d in list(fwd)[:5000])
+    # edge count close to the sampled count minus duplicates
+    assert 0.5 * 8 * 4096 * 2 < len(na) <= 8 * 4096 * 2
+
+
+def test_labels_uniform_and_zipf():
+    g = gem.HostGraph.rmat(14, 4, seed=5)
+    g.set_labels(8, 0.0, seed=1)
+    lab = g.arrays()[2]
+    h = np.bincount(lab, minlength=8) / len(lab)
+    assert np.all(np.abs(h - 1 / 8) < 0.02)
+    g.set_labels(16, 1.0, seed=1)
+    lab = g.arrays()[2]
+    h = np.bincount(lab, minlength=16) / len(lab)
+    expect = 1 / np.arange(1, 17)
+    expect /= expect.sum()
+    assert np.all(np.abs(h - expect) < 0.02)
+
+
+def test_text_roundtrip(tmp_path):
+    g = gem.HostGraph.rmat(9, 4, seed=2).set_labels(5, seed=3)
+    p = str(tmp_path / "g.graph")
+    g.write_text(p)
+    g2 = gem.HostGraph.read_text(p)
+    for x, y in zip(g.arrays(), g2.arrays()):
+        assert np.array_equal(x, y)
+
+
+def test_text_reader_accepts_unsorted_and_rejects_bad(tmp_path):
+    p = tmp_path / "u.graph"
+    p.write_text("t 3 2\nv 2 7 1\nv 0 5 1\nv 1 6 2\ne 2 1\ne 1 0\n")
+    g = gem.HostGraph.read_text(str(p))
+    off, nbr, lab = g.arrays()
+    assert off.tolist() == [0, 1, 3, 4] and nbr.tolist() == [1, 0, 2, 1] and lab.tolist() == [5, 6, 7]
+    bad = tmp_path / "b.graph"
+    bad.write_text("t 3 2\nv 0 5 1\nv 1 6 1\nv 2 7 1\ne 2 1\ne 1 0\n")  # degree of 1 is 2
+    with pytest.raises(gem.GemError):
+        gem.HostGraph.read_text(str(bad))
+    with pytest.raises(gem.GemError):
+        gem.HostGraph.read_text(str(tmp_path / "missing.graph"))
+
+
+def test_query_text_roundtrip(tmp_path):
+    q = gem.Query([3, 1, 3, 2], [(0, 1), (1, 2), (2, 3), (3, 0)])
+    p = str(tmp_path / "Q_0.in")
+    q.write_text(p)
+    q2 = gem.Query.read_text(p)
+    assert q2.labels.tolist() == q.labels.tolist() and q2.edges.tolist() == q.edges.tolist()
+
+
+@pytest.mark.parametrize("k,dens", [(4, gem.ANY), (8, gem.SPARSE), (8, gem.DENSE), (16, gem.SPARSE), (12, gem.DENSE)])
+def test_random_walk_queries(k, dens):
+    g = gem.HostGraph.rmat(12, 16, seed=4).set_labels(4, seed=4)
+    qs = gem.gen_queries(g, k, dens, 12, seed=77)
+    off, nbr, lab = g.arrays()
+    for q in qs:
+        assert q.nv == k
+        adj = {u: set() for u in range(k)}
+        for a, b in q.edges.tolist():
+            adj[a].add(b)
+            adj[b].add(a)
+        seen, st = {0}, [0]
+        while st:
+            x = st.pop()
+            for y in adj[x]:
+                if y not in seen:
+                    seen.add(y)
+                    st.append(y)
+        assert len(seen) == k
+        avg = 2 * q.ne / k
+        if dens == gem.SPARSE:
+            assert avg <= 3
+        if dens == gem.DENSE:
+            assert avg > 3
+    qs2 = gem.gen_queries(g, k, dens, 12, seed=77)
+    assert all(np.array_equal(a.edges, b.edges) and np.array_equal(a.labels, b.labels) for a, b in zip(qs, qs2))
