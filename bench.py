@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Benchmark: exact subgraph-matching throughput on one B200 (queries/s and
+embeddings/s, batched vs plain, p50/p99 latency).
+
+Workload (default `rmat22`): R-MAT scale 22 (4,194,304 vertices), edge
+factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), self loops and duplicates
+removed, uint32 CSR with sorted adjacency, 16 labels Zipf(s=1.0); four query
+sets of random-walk queries: 8 vertices sparse, 8 dense, 16 sparse, 16 dense
+(seeded synthetic stand-ins; the reference's datasets are not used).  A step
+is one gem_batch_run over a batch of queries drawn round-robin from the four
+sets (one persistent join launch per wave).  Every query runs under the same
+device time cap; a query that exceeds it is reported as capped, never as an
+exact count, and only exact queries enter `value`.
+
+`value` is device-timed (CUDA events around each batch, inputs resident in
+HBM), `e2e` is wall time around the C-ABI call from host buffers (query
+arrays in, results out).  L2 is flushed between steps (a 256 MiB write).
+With torchrun (N > 1) every rank runs an independent replica on its own share
+of the batches (the path has no exchange step); rank 0 reports the max time.
+`--impl reference` times the CPU restatement of the path (the reference has no
+CPU join) on the host cores with all threads.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+SETS = ((8, 1), (8, 2), (16, 1), (16, 2))  # (k, density: 1 sparse, 2 dense)
+METRIC = "queries/s & embeddings/s on 1 B200, batched vs plain, exact counts; p50/p99 ms"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class Clocks:
+    """nvidia-smi sampler during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu, self.samples, self.p = gpu, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, n in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def make_workload(gem, name):
+    if name == "rmat22":
+        t = time.time()
+        g = gem.HostGraph.rmat(22, 16, seed=0x47454D00 + 22).set_labels(16, 1.0, seed=(0x47454D00 + 22) ^ 0x4C)
+        gen_s = time.time() - t
+        desc = {"workload": "rmat22-ef16-zipf16", "scale": 22, "edge_factor": 16, "labels": 16, "zipf_s": 1.0}
+        sets = SETS
+    elif name == "rmat16":
+        t = time.time()
+        g = gem.HostGraph.rmat(16, 8, seed=0x47454D00 + 16).set_labels(8, 0.0, seed=(0x47454D00 + 16) ^ 0x4C)
+        gen_s = time.time() - t
+        desc = {"workload": "rmat16-ef8-uniform8", "scale": 16, "edge_factor": 8, "labels": 8, "zipf_s": 0.0}
+        sets = ((4, 0),)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return g, desc, sets, gen_s
+
+
+def query_pool(gem, g, sets, per_set):
+    pools = [gem.gen_queries(g, k, d, per_set, seed=0x51000 + i) for i, (k, d) in enumerate(sets)]
+    out = []
+    for j in range(per_set):
+        for p in pools:
+            out.append(p[j])
+    return out
+
+
+def flush_l2(torch_dev):
+    import torch
+    buf = torch.empty(256 << 20, dtype=torch.uint8, device=torch_dev)
+    buf.fill_(1)
+    torch.cuda.synchronize()
+
+
+def pctl(xs, p):
+    if not xs:
+        return None
+    xs = sorted(xs)
+    k = min(len(xs) - 1, max(0, int(round(p / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def run_gem(args):
+    import gem_b200 as gem
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    g, desc, sets, gen_s = make_workload(gem, args.workload)
+    pool = query_pool(gem, g, sets, args.per_set)
+    B = args.batch
+    ctx = gem.Context(device=local, time_cap_ms=args.cap_ms)
+    ctx.load_graph(g)
+
+    def batch_of(step):
+        i = (step * world + rank) * B
+        return [pool[(i + j) % len(pool)] for j in range(B)]
+
+    # warm-up (compiles nothing; touches code paths and the arena)
+    for s in range(args.warmup):
+        ctx.batch(batch_of(s))
+    steps = list(range(args.warmup, args.warmup + args.steps))
+    dev_ms, wall_ms, res_all = [], [], []
+    h2d = d2h = 0
+    with Clocks(local) as clk:
+        for s in steps:
+            qs = batch_of(s)
+            flush_l2(dev)
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st, rs = ctx.batch(qs)
+            torch.cuda.synchronize()
+            wall_ms.append((time.perf_counter() - t0) * 1e3)
+            # device time of the batch: sum over waves of first-kernel..last-kernel events
+            dev_ms.append(sum(r["ms"]["total"] for r in rs[:1]) if len({id(r) for r in rs}) else 0.0)
+            res_all.append(rs)
+            h2d += sum(4 * q.nv + 8 * q.ne for q in qs)
+            d2h += 8 * 4 * len(qs)
+    exact = sum(1 for rs in res_all for r in rs if r["status"] == "OK")
+    capped = sum(1 for rs in res_all for r in rs if r["status"] == "ERR_TIMEOUT")
+    emb = sum(r["count"] for rs in res_all for r in rs if r["status"] == "OK")
+    tdev = sum(dev_ms) / 1e3
+    twall = sum(wall_ms) / 1e3
+    # join-kernel roofline from the batches' algorithmic bytes and join times
+    jb = sum(rs[0]["bytes_alg"][3] for rs in res_all)
+    jt = sum(rs[0]["ms"]["join"] for rs in res_all) / 1e3
+    if dist:
+        t = torch.tensor([tdev, twall, float(exact), float(emb), float(capped)], dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx[:2], op=dist.ReduceOp.MAX)
+        sm = t[2:].clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        tdev, twall = float(mx[0]), float(mx[1])
+        exact, emb, capped = int(sm[0]), int(sm[1]), int(sm[2])
+    # plain mode: one query per call, latency distribution (rank 0, bounded sample)
+    plain = {}
+    if rank == 0 and args.plain > 0:
+        lat, pe, pn, pdev = [], 0, 0, 0.0
+        for q in batch_of(args.warmup)[: args.plain]:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = ctx.run(q, raise_on_error=False)
+            torch.cuda.synchronize()
+            lat.append((time.perf_counter() - t0) * 1e3)
+            pdev += r["ms"]["total"] / 1e3
+            if r["status"] == "OK":
+                pn += 1
+                pe += r["count"]
+        plain = {"queries": len(lat), "exact": pn, "queries_per_s": pn / (sum(lat) / 1e3) if lat else None,
+                 "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99)}
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = (jb / jt / 1e9) if jt > 0 else 0.0
+    line = {
+        "metric": METRIC,
+        "value": exact / tdev if tdev > 0 else 0.0,
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": tdev * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32/u64",
+        "data": "synthetic R-MAT graph and random-walk queries (seeded)",
+        "config": dict(desc, batch=B, query_sets=[f"{k}{'s' if d == 1 else 'd' if d == 2 else ''}" for k, d in sets],
+                       time_cap_ms=args.cap_ms, parallelism=f"replicas{world}", l2="flushed (256 MiB write)",
+                       exact_queries=exact, capped_queries=capped, graph_gen_s=round(gen_s, 2)),
+        "embeddings_per_s": emb / tdev if tdev > 0 else 0.0,
+        "plain": plain,
+        "e2e": {"value": exact / twall if twall > 0 else 0.0, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": None, "kernel": "join_kernel<COUNT>",
+                     "peak_source": peak_src},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+    if args.cpu_sample > 0:
+        line["cpu_baseline"] = cpu_baseline(g, pool, args)
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(g, pool, args):
+    import oracle
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    n_ok = 0
+    n = 0
+    for q in pool[: args.cpu_sample]:
+        c, h, ok = oracle.count(g, q, threads=threads, want_hash=False, work_cap=args.cpu_work_cap)
+        n += 1
+        n_ok += 1 if ok else 0
+    dt = time.perf_counter() - t0
+    return {"value": n_ok / dt if dt > 0 else 0.0, "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"first {n} queries of the pool, each capped at {args.cpu_work_cap} scanned arcs; "
+                      f"{n_ok} completed in {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import gem_b200 as gem
+    g, desc, sets, _ = make_workload(gem, args.workload)
+    pool = query_pool(gem, g, sets, args.per_set)
+    import oracle
+    threads = os.cpu_count() or 1
+    B = min(args.batch, 4)
+    times, exact, emb = [], 0, 0
+    for s in range(args.warmup + args.steps):
+        qs = [pool[(s * B + j) % len(pool)] for j in range(B)]
+        t0 = time.perf_counter()
+        for q in qs:
+            c, h, ok = oracle.count(g, q, threads=threads, want_hash=False, work_cap=args.cpu_work_cap)
+            if s >= args.warmup and ok:
+                exact += 1
+                emb += c
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    T = sum(times)
+    v = exact / T if T > 0 else 0.0
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": T * 1e3 / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64", "data": "synthetic (seeded)",
+        "config": dict(desc, batch=B, cpu_work_cap=args.cpu_work_cap),
+        "embeddings_per_s": emb / T if T > 0 else 0.0,
+        "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"{B} queries per step, each capped at {args.cpu_work_cap} scanned arcs"},
+        "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gem", choices=["gem", "reference"])
+    ap.add_argument("--workload", default="rmat22")
+    ap.add_argument("--per-set", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--cap-ms", type=int, default=2000)
+    ap.add_argument("--plain", type=int, default=16)
+    ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--cpu-work-cap", type=int, default=1_000_000_000)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gem(args)
+
+
+if __name__ == "__main__":
+    main()

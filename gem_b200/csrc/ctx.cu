@@ -639,6 +639,15 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   CU(cudaMemcpyAsync(&hc, ctx->d_ctl, sizeof hc, cudaMemcpyDeviceToHost, ctx->s));
   CU(cudaStreamSynchronize(ctx->s));
   w.join_ms = ev_ms(ctx->ev[6], ctx->ev[7]);
+  // Donated tasks still queued when the grid stopped (deadline) were never
+  // run: their queries are incomplete.
+  if (hc.head < hc.tail) {
+    for (unsigned long long t = hc.head; t < hc.tail && t < hc.head + TASK_CAP; ++t) {
+      uint32_t qq = 0;
+      CU(cudaMemcpy(&qq, &ctx->d_queue[t & (TASK_CAP - 1)].q, 4, cudaMemcpyDeviceToHost));
+      if (qq < out.size()) out[qq].pad[0] = 1;
+    }
+  }
   for (size_t qi = 0; qi < w.q.size(); ++qi)
     if (w.jq_index[qi] != UINT32_MAX) w.out[qi] = out[w.jq_index[qi]];
   w.join_nodes = out[0].nodes;
@@ -703,8 +712,8 @@ void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r) {
   const JOut &o = w.out[qi];
   r->count = o.count;
   r->emb_hash = o.hash;
-  if (w.join_err == 1) r->status = GEM_ERR_TIMEOUT;
-  else if (w.join_err) r->status = GEM_ERR_INTERNAL;
+  if (o.pad[0]) r->status = w.join_err == 1 || w.join_err == 0 ? GEM_ERR_TIMEOUT : GEM_ERR_INTERNAL;
+  else if (w.join_err > 1) r->status = GEM_ERR_INTERNAL;
   uint64_t ct = 0;
   for (uint32_t u = 0; u < w.q[qi].nv; ++u) ct += w.cnt[w.row_base[qi] + u];
   r->cand_total = ct;

@@ -276,6 +276,15 @@ __device__ __forceinline__ uint32_t find_query(const uint64_t *__restrict__ rp, 
   return lo;
 }
 
+// Marks query q incomplete and, once, withdraws every unclaimed root so the
+// grid drains quickly; the queries owning withdrawn roots are marked too.
+__device__ void abandon(const JoinArgs &a, uint32_t q) {
+  atomicOr(&a.out[q].pad[0], 1ull);
+  const unsigned long long r0 = atomicExch(&a.ctl->root_next, (unsigned long long)a.n_roots);
+  if (r0 < a.n_roots)
+    for (uint32_t k = find_query(a.root_prefix, a.nquery, r0); k < a.nquery; ++k) atomicOr(&a.out[k].pad[0], 1ull);
+}
+
 __device__ __forceinline__ uint32_t index_of(const JLevel *__restrict__ L, uint32_t w) {
   const uint32_t kind = L->idx_kind;
   if (kind == IDX_RANK) return rank_lookup(L->rb, w);
@@ -334,6 +343,14 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         if (rr >= a.n_roots) atomicSub(&ctl->busy, 1u);
       }
       r = __shfl_sync(FULL, rr, 0);
+      if (r < a.n_roots && ld_vol(&ctl->err) != DERR_NONE) {
+        // past the deadline: this root is not processed
+        if (lane == 0) {
+          abandon(a, find_query(a.root_prefix, a.nquery, r));
+          atomicSub(&ctl->busy, 1u);
+        }
+        r = a.n_roots;
+      }
       if (r < a.n_roots) {
         have = true;
         from_root = true;
@@ -345,13 +362,14 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
     if (!have) {
       uint32_t backoff = 64;
       for (;;) {
-        if (lane == 0) {
-          atomicAdd(&ctl->busy, 1u);
-          __threadfence();
-        }
+        // Only a warp that holds work counts as busy: pollers must not keep
+        // `busy` above zero, or no poller could ever observe quiescence.
         PoppedTask t;
         if (queue_pop(ctl, a.queue, t, c)) {
-          if (lane == 0) atomicSub(&ctl->idle, 1u);
+          if (lane == 0) {
+            atomicAdd(&ctl->busy, 1u);
+            atomicSub(&ctl->idle, 1u);
+          }
           idle_registered = false;  // a finished donated task re-registers as idle below
           q = t.q;
           lvl = base_lvl = t.lvl;
@@ -368,7 +386,6 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         }
         int leave = 0;
         if (lane == 0) {
-          atomicSub(&ctl->busy, 1u);
           __threadfence();
           const unsigned int b = ld_vol(&ctl->busy);
           __threadfence();
@@ -536,6 +553,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
       th += __shfl_xor_sync(FULL, th, d);
     }
     if (lane == 0) {
+      if (abort) abandon(a, q);
       if (tc) atomicAdd(&a.out[q].count, (unsigned long long)tc);
       if (MODE != MODE_COUNT && th) atomicAdd(&a.out[q].hash, (unsigned long long)th);
       __threadfence();

@@ -173,7 +173,7 @@ struct JOut {                // per query, accumulated with atomics
   unsigned long long nodes;      // extended partial embeddings
   unsigned long long scanned;    // source-list elements evaluated
   unsigned long long probes;     // binary-search and index probes
-  unsigned long long pad[2];
+  unsigned long long pad[2];     // pad[0] != 0: some work of this query was abandoned
 };
 constexpr uint32_t TASK_CAP = 8192;  // donation queue cells
 struct JTask {

@@ -42,6 +42,6 @@ def _built():
 @pytest.fixture(scope="session")
 def ctx():
     import gem_b200 as gem
-    c = gem.Context(time_cap_ms=120000)
+    c = gem.Context(time_cap_ms=30000)
     yield c
     c.close()

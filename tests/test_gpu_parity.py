@@ -27,7 +27,7 @@ def small():
 
 @pytest.fixture(scope="module")
 def gctx(small):
-    c = gem.Context(time_cap_ms=120000)
+    c = gem.Context(time_cap_ms=30000)
     c.load_graph(small)
     yield c
     c.close()
@@ -37,7 +37,7 @@ def gctx(small):
 def test_golden_counts_and_hash(case):
     g = gem.HostGraph.from_edges(case["nv"], case["edges"], case["labels"])
     q = gem.Query(case["qlabels"], case["qedges"])
-    with gem.Context() as c:
+    with gem.Context(time_cap_ms=20000) as c:
         c.load_graph(g)
         r = c.run(q, mode=gem.MODE_HASH)
     assert r["status"] == "OK"
@@ -84,7 +84,7 @@ def test_cuckoo_large_table():
     # one label: every vertex is a candidate -> table far above the shared-memory path
     g = gem.HostGraph.rmat(15, 4, seed=3).set_labels(1)
     q = gem.Query([0, 0], [(0, 1)])
-    with gem.Context() as c:
+    with gem.Context(time_cap_ms=20000) as c:
         c.load_graph(g)
         cand = oracle.filter(g, q)[0]
         pos = c.index_probe(q, 0, cand, kind=gem.IDX_CUCKOO)
@@ -108,7 +108,7 @@ def test_counts_match_oracle(small, gctx, k, dens, n):
 
 @pytest.mark.parametrize("kind", [gem.IDX_RANK, gem.IDX_CUCKOO])
 def test_index_kinds_same_counts(small, kind):
-    with gem.Context(index_kind=kind) as c:
+    with gem.Context(index_kind=kind, time_cap_ms=30000) as c:
         c.load_graph(small)
         for q in gem.gen_queries(small, 5, gem.ANY, 4, seed=31):
             exp, eh, ok = oracle.count(small, q, work_cap=400_000_000)
