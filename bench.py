@@ -155,7 +155,8 @@ def run_gem(args):
         ctx.batch(batch_of(s))
     steps = list(range(args.warmup, args.warmup + args.steps))
     dev_ms, wall_ms, res_all = [], [], []
-    h2d = d2h = 0
+    h2d = d2h = launches = jbytes = 0
+    jms = 0.0
     with Clocks(local) as clk:
         for s in steps:
             qs = batch_of(s)
@@ -167,8 +168,14 @@ def run_gem(args):
             st, rs = ctx.batch(qs)
             torch.cuda.synchronize()
             wall_ms.append((time.perf_counter() - t0) * 1e3)
-            # device time of the batch: sum over waves of first-kernel..last-kernel events
-            dev_ms.append(sum(r["ms"]["total"] for r in rs[:1]) if len({id(r) for r in rs}) else 0.0)
+            # device time of the batch: sum over its waves (first kernel .. last kernel, CUDA events)
+            waves = {}
+            for r in rs:
+                waves.setdefault(r["wave"], r)
+            dev_ms.append(sum(r["ms"]["total"] for r in waves.values()))
+            launches += sum(r["launches"] for r in waves.values())
+            jbytes += sum(r["bytes_alg"][3] for r in waves.values())
+            jms += sum(r["ms"]["join"] for r in waves.values())
             res_all.append(rs)
             h2d += sum(4 * q.nv + 8 * q.ne for q in qs)
             d2h += 8 * 4 * len(qs)
@@ -178,8 +185,8 @@ def run_gem(args):
     tdev = sum(dev_ms) / 1e3
     twall = sum(wall_ms) / 1e3
     # join-kernel roofline from the batches' algorithmic bytes and join times
-    jb = sum(rs[0]["bytes_alg"][3] for rs in res_all)
-    jt = sum(rs[0]["ms"]["join"] for rs in res_all) / 1e3
+    jb = jbytes
+    jt = jms / 1e3
     if dist:
         t = torch.tensor([tdev, twall, float(exact), float(emb), float(capped)], dtype=torch.float64)
         mx = t.clone()
@@ -239,7 +246,7 @@ def run_gem(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": None, "kernel": "join_kernel<COUNT>",
                      "peak_source": peak_src},
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     if args.cpu_sample > 0:

@@ -68,7 +68,7 @@ class _Result(C.Structure):
     _fields_ = [("count", C.c_uint64), ("emb_hash", C.c_uint64), ("n_written", C.c_uint64),
                 ("status", C.c_uint32), ("n_tables", C.c_uint32), ("cand_total", C.c_uint64),
                 ("table_total", C.c_uint64), ("nodes", C.c_uint64), ("bytes_alg", C.c_uint64 * 4),
-                ("ms", C.c_float * 8)]
+                ("ms", C.c_float * 8), ("wave", C.c_uint32), ("launches", C.c_uint32)]
 
 
 _lib = None
@@ -284,7 +284,8 @@ class Result(dict):
         d = Result(count=int(r.count), emb_hash=int(r.emb_hash), n_written=int(r.n_written),
                    status=STATUS.get(r.status, r.status), status_code=int(r.status), n_tables=int(r.n_tables),
                    cand_total=int(r.cand_total), table_total=int(r.table_total), nodes=int(r.nodes),
-                   bytes_alg=[int(x) for x in r.bytes_alg], ms={p: float(r.ms[i]) for i, p in enumerate(PHASES)})
+                   bytes_alg=[int(x) for x in r.bytes_alg], ms={p: float(r.ms[i]) for i, p in enumerate(PHASES)},
+                   wave=int(r.wave), launches=int(r.launches))
         return d
 
 

@@ -670,6 +670,7 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
     return GEM_ERR_STATE;
   }
   CU(cudaSetDevice(ctx->opts.device));
+  const uint64_t launches0 = g_launches.load();
   const size_t nq = w.q.size();
   w.row_base.assign(nq, 0);
   w.active.assign(nq, 1);
@@ -703,6 +704,7 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
   w.tables_ms = ev_ms(ctx->ev[1], ctx->ev[2]);
   w.index_ms = ev_ms(ctx->ev[2], ctx->ev[3]);
   w.total_ms = ev_ms(ctx->ev[0], ctx->ev[4]);
+  w.launches = (uint32_t)(g_launches.load() - launches0);
   return GEM_OK;
 }
 
@@ -734,6 +736,7 @@ void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r) {
   r->ms[GEM_PH_JOIN] = w.join_ms;
   r->ms[GEM_PH_TOTAL] = w.total_ms;
   r->ms[GEM_PH_HOST] = (float)w.plan_ms;
+  r->launches = w.launches;
   (void)ctx;
 }
 
@@ -783,7 +786,7 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
   }
   // waves: as many queries as the per-wave row limit allows
   const uint32_t max_rows = ctx->wave_max_rows;
-  uint32_t i = 0;
+  uint32_t i = 0, wave_no = 0;
   gem_status first_err = GEM_OK;
   while (i < n) {
     Wave w;
@@ -805,7 +808,11 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
       if (first_err == GEM_OK) first_err = st;
       continue;
     }
-    for (size_t k = 0; k < ids.size(); ++k) wave_result(ctx, w, k, &res[ids[k]]);
+    for (size_t k = 0; k < ids.size(); ++k) {
+      wave_result(ctx, w, k, &res[ids[k]]);
+      res[ids[k]].wave = wave_no;
+    }
+    ++wave_no;
   }
   for (uint32_t k = 0; k < n; ++k)
     if (res[k].status != GEM_OK && first_err == GEM_OK) first_err = (gem_status)res[k].status;

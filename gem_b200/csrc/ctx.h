@@ -66,6 +66,7 @@ struct Wave {
   float filter_ms = 0, tables_ms = 0, index_ms = 0, join_ms = 0, total_ms = 0;
   double plan_ms = 0;
   uint64_t bytes_filter = 0, bytes_tables = 0, bytes_index = 0, bytes_join = 0;
+  uint32_t launches = 0;
 };
 
 struct gem_ctx {

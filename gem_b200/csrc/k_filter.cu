@@ -79,6 +79,7 @@ void launch_filter(const DevGraph &g, const FilterDesc *d_desc, uint32_t nquery,
   if (nwords == 0 || nquery == 0) return;
   uint64_t blocks = (nwords + 7) / 8;
   if (blocks > 148ull * 16) blocks = 148ull * 16;
+  count_launch();
   filter_kernel<<<(uint32_t)blocks, 256, 0, s>>>(g, d_desc, nquery, rb, nwords);
 }
 
@@ -106,6 +107,7 @@ void launch_compact(uint64_t *rb, const uint64_t *ex, uint32_t nrows, uint32_t n
   if (n == 0) return;
   uint64_t blocks = (n + 255) / 256;
   if (blocks > 148ull * 32) blocks = 148ull * 32;
+  count_launch();
   compact_kernel<<<(uint32_t)blocks, 256, 0, s>>>(rb, ex, nrows, nwords, c_base, cand);
 }
 

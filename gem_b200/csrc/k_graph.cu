@@ -13,6 +13,8 @@
 
 namespace gem {
 
+std::atomic<uint64_t> g_launches{0};
+
 __global__ void degrees_kernel(const uint64_t *__restrict__ off, uint32_t nv, uint32_t *__restrict__ deg) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv;
        v += (uint64_t)gridDim.x * blockDim.x)
@@ -23,6 +25,7 @@ void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s) {
   if (g.nv == 0) return;
   uint32_t blocks = (uint32_t)((g.nv + 255) / 256);
   if (blocks > 148u * 32u) blocks = 148u * 32u;
+  count_launch();
   degrees_kernel<<<blocks, 256, 0, s>>>(g.off, g.nv, deg);
 }
 
@@ -57,6 +60,7 @@ void launch_nlc(const DevGraph &g, uint8_t *nlc, uint32_t stride, cudaStream_t s
   uint64_t warps = g.nv;
   uint64_t blocks = (warps + 7) / 8;
   if (blocks > 148ull * 64) blocks = 148ull * 64;
+  count_launch();
   nlc_kernel<<<(uint32_t)blocks, 256, 0, s>>>(g.off, g.nbr, g.lab, g.nv, g.nlabels, nlc, stride);
 }
 
@@ -179,6 +183,7 @@ __global__ void gather_strided_kernel(const uint64_t *__restrict__ in, uint64_t 
 
 void launch_gather_strided(const uint64_t *in, uint64_t stride, uint32_t n, uint64_t *out, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   gather_strided_kernel<<<(n + 255) / 256, 256, 0, s>>>(in, stride, n, out);
 }
 
@@ -187,6 +192,7 @@ __global__ void set_deadline_kernel(unsigned long long *deadline, unsigned long 
 }
 
 void launch_set_deadline(unsigned long long *deadline, uint64_t cap_ns, cudaStream_t s) {
+  count_launch();
   set_deadline_kernel<<<1, 1, 0, s>>>(deadline, cap_ns);
 }
 
@@ -200,18 +206,27 @@ void launch_scan(const void *in, ScanInput kind, uint64_t n, uint64_t *out, uint
   }
   switch (kind) {
     case SCAN_POPC_U64LO:
+      count_launch();
       scan_partial_kernel<SCAN_POPC_U64LO><<<(uint32_t)nb, SCAN_T, 0, s>>>(in, n, tmp);
+      count_launch();
       scan_top_kernel<<<1, 1024, 0, s>>>(tmp, nb, out, n);
+      count_launch();
       scan_final_kernel<SCAN_POPC_U64LO><<<(uint32_t)nb, SCAN_T, 0, s>>>(in, n, tmp, out);
       break;
     case SCAN_POPC_U32:
+      count_launch();
       scan_partial_kernel<SCAN_POPC_U32><<<(uint32_t)nb, SCAN_T, 0, s>>>(in, n, tmp);
+      count_launch();
       scan_top_kernel<<<1, 1024, 0, s>>>(tmp, nb, out, n);
+      count_launch();
       scan_final_kernel<SCAN_POPC_U32><<<(uint32_t)nb, SCAN_T, 0, s>>>(in, n, tmp, out);
       break;
     default:
+      count_launch();
       scan_partial_kernel<SCAN_U32><<<(uint32_t)nb, SCAN_T, 0, s>>>(in, n, tmp);
+      count_launch();
       scan_top_kernel<<<1, 1024, 0, s>>>(tmp, nb, out, n);
+      count_launch();
       scan_final_kernel<SCAN_U32><<<(uint32_t)nb, SCAN_T, 0, s>>>(in, n, tmp, out);
       break;
   }

@@ -149,12 +149,14 @@ void launch_cuckoo_build(const CuckooTable *d_tabs, const CuckooTable *h_tabs, u
   if (!small.empty()) {
     cudaFuncSetAttribute(cuckoo_build_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)CK_SMEM_MAX_BYTES);
+    count_launch();
     cuckoo_build_smem_kernel<<<(uint32_t)small.size(), 256, max_smem, s>>>(d_tabs, d_which, err);
   }
   if (!large.empty()) {
     uint64_t n = k1 - k0;
     uint64_t blocks = (n + 255) / 256;
     if (blocks > 148ull * 32) blocks = 148ull * 32;
+    count_launch();
     cuckoo_build_global_kernel<<<(uint32_t)blocks, 256, 0, s>>>(d_tabs, d_which + small.size(),
                                                                 (uint32_t)large.size(), k0, k1, err);
   }
@@ -172,11 +174,13 @@ __global__ void rank_probe_kernel(const uint64_t *rb, const uint32_t *keys, uint
 
 void launch_cuckoo_probe(const CuckooTable *d_tab, const uint32_t *keys, uint32_t n, uint32_t *out, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   cuckoo_probe_kernel<<<(n + 255) / 256 > 4096 ? 4096 : (n + 255) / 256, 256, 0, s>>>(d_tab, keys, n, out);
 }
 
 void launch_rank_probe(const uint64_t *rb, const uint32_t *keys, uint32_t n, uint32_t *out, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   rank_probe_kernel<<<(n + 255) / 256 > 4096 ? 4096 : (n + 255) / 256, 256, 0, s>>>(rb, keys, n, out);
 }
 

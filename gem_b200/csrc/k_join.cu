@@ -577,7 +577,10 @@ __global__ void queue_init_kernel(JTask *cells) {
     cells[i].seq = i;
 }
 
-void join_queue_init(JTask *queue, cudaStream_t s) { queue_init_kernel<<<32, 256, 0, s>>>(queue); }
+void join_queue_init(JTask *queue, cudaStream_t s) {
+  count_launch();
+  queue_init_kernel<<<32, 256, 0, s>>>(queue);
+}
 
 int join_blocks_per_sm(uint32_t mode) {
   int n = 0;
@@ -594,6 +597,7 @@ uint32_t launch_join(const JoinArgs &a, int blocks_per_sm, cudaStream_t s) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const uint32_t grid = (uint32_t)(sms * (blocks_per_sm > 0 ? blocks_per_sm : 1));
+  count_launch();
   if (a.mode == MODE_COUNT) join_kernel<MODE_COUNT><<<grid, 256, 0, s>>>(a);
   else if (a.mode == MODE_HASH) join_kernel<MODE_HASH><<<grid, 256, 0, s>>>(a);
   else join_kernel<MODE_ENUM><<<grid, 256, 0, s>>>(a);

@@ -57,6 +57,7 @@ void launch_key_tiles(const DevGraph &g, const TabSource *d_src, uint32_t nsrc, 
   if (nkeys == 0) return;
   uint64_t blocks = (nkeys + 255) / 256;
   if (blocks > 148ull * 32) blocks = 148ull * 32;
+  count_launch();
   key_tiles_kernel<<<(uint32_t)blocks, 256, 0, s>>>(g, d_src, nsrc, nkeys, tiles);
 }
 
@@ -68,6 +69,7 @@ __global__ void source_tile_bases_kernel(const TabSource *__restrict__ src, uint
 
 void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp,
                               uint64_t *out, cudaStream_t s) {
+  count_launch();
   source_tile_bases_kernel<<<(nsrc + 256) / 256, 256, 0, s>>>(d_src, nsrc, nkeys, tp, out);
 }
 
@@ -141,6 +143,7 @@ static uint32_t tile_blocks(uint64_t total_tiles) {
 void launch_table_count(const DevGraph &g, const TabSource *d_src, const TabEdge *d_edge, uint32_t nedge,
                         const uint64_t *tp, uint64_t total_tiles, uint32_t *mask, cudaStream_t s) {
   if (total_tiles == 0) return;
+  count_launch();
   table_tiles_kernel<false><<<tile_blocks(total_tiles), 256, 0, s>>>(g, d_src, d_edge, nedge, tp, total_tiles, mask,
                                                                      nullptr, nullptr);
 }
@@ -149,6 +152,7 @@ void launch_table_write(const DevGraph &g, const TabSource *d_src, const TabEdge
                         const uint64_t *tp, uint64_t total_tiles, const uint32_t *mask, const uint64_t *vp,
                         uint32_t *values, cudaStream_t s) {
   if (total_tiles == 0) return;
+  count_launch();
   table_tiles_kernel<true><<<tile_blocks(total_tiles), 256, 0, s>>>(g, d_src, d_edge, nedge, tp, total_tiles,
                                                                     const_cast<uint32_t *>(mask), vp, values);
 }
@@ -180,6 +184,7 @@ void launch_table_offsets(const TabSource *d_src, const TabEdge *d_edge, uint32_
   if (total_offsets == 0) return;
   uint64_t blocks = (total_offsets + 255) / 256;
   if (blocks > 148ull * 32) blocks = 148ull * 32;
+  count_launch();
   table_offsets_kernel<<<(uint32_t)blocks, 256, 0, s>>>(d_src, d_edge, nedge, tp, vp, total_offsets);
 }
 

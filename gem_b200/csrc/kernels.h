@@ -6,7 +6,14 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 namespace gem {
+
+// Number of kernels libgem has launched (all contexts); read by the C-ABI
+// results so callers can report their launch counts.
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 constexpr uint32_t QV = 32;           // max query vertices
 constexpr uint32_t NLC_MAX_LABELS = 64;  // per-vertex label-count table kept up to this many labels

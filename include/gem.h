@@ -176,7 +176,9 @@ typedef struct gem_result {
   uint64_t table_total;  /* sum of edge-table value counts */
   uint64_t nodes;        /* partial embeddings extended by the join (all levels) */
   uint64_t bytes_alg[4]; /* algorithmic bytes: filter, index, tables, join */
-  float ms[8];           /* GEM_PH_* */
+  float ms[8];           /* GEM_PH_* (batch: times of the wave that ran this query) */
+  uint32_t wave;         /* batch: index of the wave that ran this query */
+  uint32_t launches;     /* kernels launched for this query's wave */
 } gem_result;
 
 /* Run one query end to end on the device (filter -> index -> edge tables ->

@@ -153,7 +153,10 @@ def test_enumerate_overflow_keeps_exact_count(small, gctx):
 def test_batch_equals_plain(small, gctx):
     qs = []
     for k in (2, 3, 4, 5, 6, 8):
-        qs += gem.gen_queries(small, k, gem.ANY, 4, seed=500 + k)
+        for q in gem.gen_queries(small, k, gem.ANY, 6, seed=500 + k):
+            if oracle.count(small, q, want_hash=False, work_cap=200_000_000)[2]:
+                qs.append(q)
+    assert len(qs) >= 12
     plain = [gctx.run(q, mode=gem.MODE_HASH) for q in qs]
     st, batch = gctx.batch(qs, mode=gem.MODE_HASH)
     assert st == 0
