@@ -88,7 +88,16 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def make_workload(gem, name):
+def parse_sets(spec):
+    """'8s,8d,16s,16d' -> ((8, 1), (8, 2), (16, 1), (16, 2)); a = any density."""
+    out = []
+    for tok in spec.split(","):
+        tok = tok.strip()
+        out.append((int(tok[:-1]), {"a": 0, "s": 1, "d": 2}[tok[-1]]))
+    return tuple(out)
+
+
+def make_workload(gem, name, sets_spec=None):
     if name == "rmat22":
         t = time.time()
         g = gem.HostGraph.rmat(22, 16, seed=0x47454D00 + 22).set_labels(16, 1.0, seed=(0x47454D00 + 22) ^ 0x4C)
@@ -103,6 +112,8 @@ def make_workload(gem, name):
         sets = ((4, 0),)
     else:
         raise SystemExit(f"unknown workload {name}")
+    if sets_spec:
+        sets = parse_sets(sets_spec)
     return g, desc, sets, gen_s
 
 
@@ -140,7 +151,7 @@ def run_gem(args):
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    g, desc, sets, gen_s = make_workload(gem, args.workload)
+    g, desc, sets, gen_s = make_workload(gem, args.workload, args.sets)
     pool = query_pool(gem, g, sets, args.per_set)
     B = args.batch
     ctx = gem.Context(device=local, time_cap_ms=args.cap_ms)
@@ -236,7 +247,7 @@ def run_gem(args):
         "vs_baseline": None,
         "dtype": "u32/u64",
         "data": "synthetic R-MAT graph and random-walk queries (seeded)",
-        "config": dict(desc, batch=B, query_sets=[f"{k}{'s' if d == 1 else 'd' if d == 2 else ''}" for k, d in sets],
+        "config": dict(desc, batch=B, query_sets=[f"{k}{'s' if d == 1 else 'd' if d == 2 else 'a'}" for k, d in sets],
                        time_cap_ms=args.cap_ms, parallelism=f"replicas{world}", l2="flushed (256 MiB write)",
                        exact_queries=exact, capped_queries=capped, graph_gen_s=round(gen_s, 2)),
         "embeddings_per_s": emb / tdev if tdev > 0 else 0.0,
@@ -275,7 +286,7 @@ def run_reference(args):
     if rank != 0:
         return
     import gem_b200 as gem
-    g, desc, sets, _ = make_workload(gem, args.workload)
+    g, desc, sets, _ = make_workload(gem, args.workload, args.sets)
     pool = query_pool(gem, g, sets, args.per_set)
     import oracle
     threads = os.cpu_count() or 1
@@ -312,6 +323,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gem", choices=["gem", "reference"])
     ap.add_argument("--workload", default="rmat22")
+    ap.add_argument("--sets", default=None, help="query sets, e.g. '8s,8d,16s,16d' (s sparse, d dense, a any)")
     ap.add_argument("--per-set", type=int, default=200)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--cap-ms", type=int, default=2000)

@@ -61,7 +61,7 @@ class _Query(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("device_budget_bytes", C.c_uint64), ("pinned_budget_bytes", C.c_uint64),
                 ("ooc", C.c_int), ("time_cap_ms", C.c_uint32), ("index_kind", C.c_uint32),
-                ("reserved", C.c_uint32 * 6)]
+                ("admit_gb", C.c_uint32), ("reserved", C.c_uint32 * 5)]
 
 
 class _Result(C.Structure):
@@ -292,8 +292,10 @@ class Result(dict):
 class Context:
     """One GPU with a resident data graph (gem_ctx)."""
 
-    def __init__(self, device=0, budget_bytes=0, time_cap_ms=0, index_kind=IDX_AUTO, ooc=False, pinned_bytes=0):
+    def __init__(self, device=0, budget_bytes=0, time_cap_ms=0, index_kind=IDX_AUTO, ooc=False, pinned_bytes=0,
+                 admit_gb=0):
         o = _Opts()
+        o.admit_gb = admit_gb
         o.device = device
         o.device_budget_bytes = budget_bytes
         o.pinned_budget_bytes = pinned_bytes
@@ -347,6 +349,23 @@ class Context:
         st = lib().gem_batch_run(self._h, arr, len(qs), mode, rs)
         out = [Result._from(r) for r in rs]
         return st, out
+
+    def submit(self, q, mode=MODE_COUNT):
+        """Serving: returns a ticket, or None when admission is busy (retry later)."""
+        qc = q._c()
+        t = C.c_uint64()
+        st = lib().gem_submit(self._h, C.byref(qc), mode, C.byref(t))
+        if st == 2:
+            return None
+        _check(st, self._h, "submit")
+        return t.value
+
+    def poll(self, ticket):
+        """Serving: the Result of `ticket` once done, else None."""
+        r = _Result()
+        done = C.c_int()
+        _check(lib().gem_poll(self._h, ticket, C.byref(r), C.byref(done)), self._h, "poll")
+        return Result._from(r) if done.value else None
 
     def filter(self, q, threshold=0):
         counts = np.zeros(q.nv, np.uint32)

@@ -11,6 +11,7 @@
 // call exits the process.
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -154,6 +155,10 @@ extern "C" gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out) {
 }
 
 static void free_graph(gem_ctx *ctx) {
+  if (ctx->pinned_nbr) {
+    cudaFreeHost(ctx->pinned_nbr);
+    ctx->pinned_nbr = nullptr;
+  }
   if (ctx->graph_mem) {
     cudaFree(ctx->graph_mem);
     ctx->device_bytes -= ctx->graph_bytes;
@@ -166,6 +171,7 @@ static void free_graph(gem_ctx *ctx) {
 
 extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
   if (!ctx) return;
+  server_shutdown(ctx);
   cudaSetDevice(ctx->opts.device);
   cudaStreamSynchronize(ctx->s);
   ctx->arena.release(ctx);
@@ -184,6 +190,7 @@ extern "C" const char *gem_last_error(const gem_ctx *ctx) { return ctx ? ctx->er
 
 extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   if (!ctx || !hg) return GEM_ERR_ARG;
+  if (ctx->server) return GEM_ERR_STATE;
   CU(cudaSetDevice(ctx->opts.device));
   CU(cudaStreamSynchronize(ctx->s));
   ctx->arena.reset();
@@ -193,8 +200,9 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   const uint32_t L = hg->max_label_plus1;
   const uint32_t stride = (L > 0 && L <= NLC_MAX_LABELS) ? ((L + 15) / 16) * 16 : 0;
   auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
-  const uint64_t b_off = al(8ull * (nv + 1)), b_nbr = al(4ull * na), b_lab = al(4ull * nv), b_deg = al(4ull * nv),
-                 b_nlc = al((uint64_t)stride * nv);
+  const bool ooc = ctx->opts.ooc != 0;
+  const uint64_t b_off = al(8ull * (nv + 1)), b_nbr = ooc ? 0 : al(4ull * na), b_lab = al(4ull * nv),
+                 b_deg = al(4ull * nv), b_nlc = al((uint64_t)stride * nv);
   const uint64_t total = b_off + b_nbr + b_lab + b_deg + b_nlc;
   if (ctx->device_bytes + total > ctx->budget) {
     ctx->err = "graph does not fit the device budget";
@@ -216,7 +224,21 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   uint32_t *d_deg = (uint32_t *)(p + b_off + b_nbr + b_lab);
   uint8_t *d_nlc = stride ? (uint8_t *)(p + b_off + b_nbr + b_lab + b_deg) : nullptr;
   CU(cudaMemcpyAsync(d_off, hg->off.data(), 8ull * (nv + 1), cudaMemcpyHostToDevice, ctx->s));
-  if (na) CU(cudaMemcpyAsync(d_nbr, hg->nbr.data(), 4ull * na, cudaMemcpyHostToDevice, ctx->s));
+  if (ooc) {
+    // Out-of-core: the adjacency array stays in pinned host memory mapped
+    // into the device address space; kernels read it over the host link.
+    if (ctx->opts.pinned_budget_bytes && 4ull * na > ctx->opts.pinned_budget_bytes) {
+      ctx->err = "adjacency does not fit the pinned budget";
+      return GEM_ERR_OOM;
+    }
+    void *h = nullptr;
+    CU(cudaHostAlloc(&h, na ? 4ull * na : 4, cudaHostAllocMapped | cudaHostAllocPortable));
+    ctx->pinned_nbr = h;
+    if (na) std::memcpy(h, hg->nbr.data(), 4ull * na);
+    CU(cudaHostGetDevicePointer((void **)&d_nbr, h, 0));
+  } else if (na) {
+    CU(cudaMemcpyAsync(d_nbr, hg->nbr.data(), 4ull * na, cudaMemcpyHostToDevice, ctx->s));
+  }
   if (nv) CU(cudaMemcpyAsync(d_lab, hg->lab.data(), 4ull * nv, cudaMemcpyHostToDevice, ctx->s));
   DevGraph g;
   g.nv = nv;
@@ -235,27 +257,121 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   ctx->g = g;
   ctx->loaded = true;
   ctx->label_freq.assign(L, 0);
-  for (uint32_t v = 0; v < nv; ++v) ctx->label_freq[hg->lab[v]]++;
+  ctx->label_arcs.assign(L, 0);
+  for (uint32_t v = 0; v < nv; ++v) {
+    ctx->label_freq[hg->lab[v]]++;
+    ctx->label_arcs[hg->lab[v]] += hg->off[v + 1] - hg->off[v];
+  }
   return GEM_OK;
 }
 
 // ---------------------------------------------------------------------------
 // Planner: matching order for the DFS join.
+//
+// Replaces the lattice + greedy edge choice of the reference
+// (in-core/lib/structure/src/lattice.cpp:41-185, unifiedTrie.cu:939-1018),
+// which at threshold 0 only decides the order of single-edge extensions.
+// Here: root = fewest candidates per incident edge; then repeatedly the
+// vertex with most already-placed neighbours (non-leaves first, then fewest
+// candidates).  In count mode an independent set S of the query graph whose
+// removal leaves the rest connected is moved to the end: no two suffix
+// vertices are adjacent, so once the prefix is matched the suffix
+// completions are counted by inclusion-exclusion over same-label groups
+// (different labels have disjoint candidates) instead of being enumerated.
 // ---------------------------------------------------------------------------
-void make_plan(const HostQuery &q, const uint32_t *cnt, Plan &p) {
+static bool connected_without(const HostQuery &q, uint32_t removed) {
+  const uint32_t all = (q.nv == 32 ? 0xFFFFFFFFu : ((1u << q.nv) - 1)) & ~removed;
+  if (!all) return false;
+  uint32_t seen = all & (~all + 1), frontier = seen;
+  while (frontier) {
+    uint32_t nxt = 0;
+    for (uint32_t u = 0; u < q.nv; ++u)
+      if (frontier & (1u << u)) nxt |= q.adj[u];
+    nxt &= all & ~seen;
+    seen |= nxt;
+    frontier = nxt;
+  }
+  return seen == all;
+}
+
+// All set partitions of {0..g-1}: term = coefficient prod_B (-1)^{|B|-1} (|B|-1)!
+// with the blocks packed as 4-bit masks.
+static void partition_terms(uint32_t g, std::vector<uint64_t> &out) {
+  std::vector<uint32_t> blk(g, 0);
+  std::function<void(uint32_t, uint32_t)> rec = [&](uint32_t i, uint32_t nb) {
+    if (i == g) {
+      uint32_t masks[MAX_GROUP] = {0, 0, 0, 0};
+      for (uint32_t k = 0; k < g; ++k) masks[blk[k]] |= 1u << k;
+      int32_t coef = 1;
+      uint32_t packed = 0;
+      for (uint32_t b = 0; b < nb; ++b) {
+        const int sz = __builtin_popcount(masks[b]);
+        int32_t f = 1;
+        for (int t = 2; t < sz; ++t) f *= t;
+        coef *= ((sz - 1) & 1) ? -f : f;
+        packed |= masks[b] << (4 * b);
+      }
+      out.push_back(make_term(coef, packed));
+      return;
+    }
+    for (uint32_t b = 0; b <= nb; ++b) {
+      blk[i] = b;
+      rec(i + 1, b == nb ? nb + 1 : nb);
+    }
+  };
+  rec(0, 0);
+}
+
+void make_plan(const HostQuery &q, const uint32_t *cnt, bool count_suffix, Plan &p) {
   const uint32_t n = q.nv;
   p.n = n;
+  // ---- closed-form suffix (independent set, prefix stays connected)
+  uint32_t S = 0;
+  if (count_suffix && n >= 2) {
+    std::vector<uint32_t> cand(n);
+    for (uint32_t u = 0; u < n; ++u) cand[u] = u;
+    std::sort(cand.begin(), cand.end(), [&](uint32_t a, uint32_t b) {
+      if (q.deg(a) != q.deg(b)) return q.deg(a) < q.deg(b);
+      if (cnt[a] != cnt[b]) return cnt[a] > cnt[b];
+      return a < b;
+    });
+    for (uint32_t u : cand) {
+      if (q.adj[u] & S) continue;
+      const uint32_t S2 = S | (1u << u);
+      if (!connected_without(q, S2)) continue;
+      uint32_t same = 0, nback = q.deg(u), groups = 0;
+      for (uint32_t w = 0; w < n; ++w)
+        if (S2 & (1u << w)) {
+          if (q.lab[w] == q.lab[u]) {
+            ++same;
+            if (w != u) nback += q.deg(w);
+          }
+        }
+      if (same > MAX_GROUP || nback > 32) continue;
+      uint32_t seen_labels[QV], nl = 0;
+      for (uint32_t w = 0; w < n; ++w)
+        if (S2 & (1u << w)) {
+          bool f = false;
+          for (uint32_t t = 0; t < nl; ++t) f |= seen_labels[t] == q.lab[w];
+          if (!f) seen_labels[nl++] = q.lab[w];
+        }
+      groups = nl;
+      if (groups > MAX_GROUPS) continue;
+      S = S2;
+    }
+  }
+  const uint32_t nenum = n - (uint32_t)__builtin_popcount(S);
+  p.n_enum = nenum;
+  // ---- prefix order
   uint32_t used = 0;
-  for (uint32_t k = 0; k < n; ++k) {
+  for (uint32_t k = 0; k < nenum; ++k) {
     int best = -1;
     uint64_t bkey[5] = {0, 0, 0, 0, 0};
     for (uint32_t u = 0; u < n; ++u) {
-      if (used & (1u << u)) continue;
+      if ((used | S) & (1u << u)) continue;
       const uint32_t back = __builtin_popcount(q.adj[u] & used);
       if (k > 0 && back == 0) continue;
       const uint32_t d = q.deg(u);
-      // Root: fewest candidates per incident edge.  Later: most backward
-      // neighbours, non-leaves before leaves, fewest candidates, most edges.
       uint64_t key[5];
       if (k == 0) {
         key[0] = (uint64_t)((double)cnt[u] / (double)(d + 1) * 1024.0);
@@ -279,14 +395,36 @@ void make_plan(const HostQuery &q, const uint32_t *cnt, Plan &p) {
     p.level_of[u] = k;
     used |= 1u << u;
   }
+  // ---- suffix levels grouped by label
+  std::vector<uint32_t> suf;
+  for (uint32_t u = 0; u < n; ++u)
+    if (S & (1u << u)) suf.push_back(u);
+  std::stable_sort(suf.begin(), suf.end(), [&](uint32_t a, uint32_t b) { return q.lab[a] < q.lab[b]; });
+  for (size_t i = 0; i < suf.size(); ++i) {
+    p.order[nenum + i] = suf[i];
+    p.level_of[suf[i]] = nenum + (uint32_t)i;
+  }
+  p.groups.clear();
+  for (size_t i = 0; i < suf.size();) {
+    size_t j = i;
+    while (j < suf.size() && q.lab[suf[j]] == q.lab[suf[i]]) ++j;
+    Plan::Group gr;
+    gr.first = nenum + (uint32_t)i;
+    gr.size = (uint32_t)(j - i);
+    partition_terms(gr.size, gr.terms);
+    p.groups.push_back(gr);
+    i = j;
+  }
+  // ---- backward neighbours, injectivity masks, index needs
   for (uint32_t k = 0; k < n; ++k) {
     const uint32_t u = p.order[k];
     p.back[k].clear();
     p.dup_mask[k] = 0;
-    for (uint32_t j = 0; j < k; ++j) {
+    const uint32_t lim = k < nenum ? k : nenum;  // suffix levels see the prefix only
+    for (uint32_t j = 0; j < k; ++j)
       if (q.adj[u] & (1u << p.order[j])) p.back[k].push_back(j);
+    for (uint32_t j = 0; j < lim; ++j)
       if (q.lab[p.order[j]] == q.lab[u]) p.dup_mask[k] |= 1u << j;
-    }
     p.need_idx[k] = 0;
   }
   for (uint32_t k = 0; k < n; ++k)
@@ -559,7 +697,9 @@ static gem_status wave_index(gem_ctx *ctx, Wave &w) {
 static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, uint64_t emb_cap) {
   std::vector<JQuery> jq;
   std::vector<JBack> jb;
-  std::vector<uint64_t> rp;
+  std::vector<uint64_t> rp, terms, lpp;
+  std::vector<uint32_t> lpq;
+  uint64_t lp_roots = 0;
   w.jq_index.assign(w.q.size(), UINT32_MAX);
   uint64_t roots = 0;
   for (size_t qi = 0; qi < w.q.size(); ++qi) {
@@ -568,6 +708,15 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
     JQuery J;
     std::memset(&J, 0, sizeof J);
     J.n = p.n;
+    J.n_enum = p.n_enum;
+    J.n_groups = (uint32_t)p.groups.size();
+    for (uint32_t gi = 0; gi < J.n_groups; ++gi) {
+      J.grp_first[gi] = p.groups[gi].first;
+      J.grp_size[gi] = p.groups[gi].size;
+      J.term_base[gi] = (uint32_t)terms.size();
+      J.term_count[gi] = (uint32_t)p.groups[gi].terms.size();
+      terms.insert(terms.end(), p.groups[gi].terms.begin(), p.groups[gi].terms.end());
+    }
     J.root_u = p.order[0];
     const uint32_t r0 = w.row_base[qi] + p.order[0];
     J.root_cand = w.d_cand + w.c_base[r0];
@@ -591,17 +740,36 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
       }
     }
     w.jq_index[qi] = (uint32_t)jq.size();
-    rp.push_back(roots);
-    roots += J.n_root;
+    if (J.n == 1 || (mode == GEM_MODE_COUNT && J.n_enum == 1)) {
+      // lane-parallel pool; an empty range in the ordinary pool
+      lpq.push_back((uint32_t)jq.size());
+      lpp.push_back(lp_roots);
+      lp_roots += J.n_root;
+      J.root_base = roots;
+      rp.push_back(roots);
+    } else {
+      rp.push_back(roots);
+      roots += J.n_root;
+    }
     jq.push_back(J);
   }
   rp.push_back(roots);
+  lpp.push_back(lp_roots);
   w.out.assign(w.q.size(), JOut());
   if (jq.empty()) return GEM_OK;
   JQuery *d_jq;
   JBack *d_jb;
-  uint64_t *d_rp;
+  uint64_t *d_rp, *d_terms;
   JOut *d_out;
+  ST(aalloc(ctx, terms.size() ? terms.size() : 1, &d_terms));
+  uint32_t *d_lpq;
+  uint64_t *d_lpp;
+  ST(aalloc(ctx, lpq.size() ? lpq.size() : 1, &d_lpq));
+  ST(aalloc(ctx, lpp.size(), &d_lpp));
+  if (!lpq.empty()) CU(cudaMemcpyAsync(d_lpq, lpq.data(), lpq.size() * 4, cudaMemcpyHostToDevice, ctx->s));
+  CU(cudaMemcpyAsync(d_lpp, lpp.data(), lpp.size() * 8, cudaMemcpyHostToDevice, ctx->s));
+  if (!terms.empty())
+    CU(cudaMemcpyAsync(d_terms, terms.data(), terms.size() * 8, cudaMemcpyHostToDevice, ctx->s));
   ST(aalloc(ctx, jq.size(), &d_jq));
   ST(aalloc(ctx, jb.size() ? jb.size() : 1, &d_jb));
   ST(aalloc(ctx, rp.size(), &d_rp));
@@ -622,7 +790,12 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   a.backs = d_jb;
   a.values = w.d_values;
   a.root_prefix = d_rp;
+  a.terms = d_terms;
   a.n_roots = roots;
+  a.lp_query = d_lpq;
+  a.lp_prefix = d_lpp;
+  a.lp_nq = (uint32_t)lpq.size();
+  a.lp_roots = lp_roots;
   a.out = d_out;
   a.ctl = ctx->d_ctl;
   a.queue = ctx->d_queue;
@@ -690,7 +863,7 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
       w.active[qi] = 0;
       continue;
     }
-    make_plan(q, &w.cnt[w.row_base[qi]], w.plan[qi]);
+    make_plan(q, &w.cnt[w.row_base[qi]], mode == GEM_MODE_COUNT && ctx->closed_form_suffix, w.plan[qi]);
   }
   w.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
   ST(wave_tables(ctx, w));
@@ -746,9 +919,11 @@ void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r) {
 extern "C" gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold, int mode,
                                     uint32_t *emb_out, uint64_t emb_cap, gem_result *res) {
   if (!ctx || !q || !res) return GEM_ERR_ARG;
+  if (ctx->server) return GEM_ERR_STATE;
   if (mode < GEM_MODE_COUNT || mode > GEM_MODE_ENUMERATE) return GEM_ERR_ARG;
   if (mode == GEM_MODE_ENUMERATE && emb_cap && !emb_out) return GEM_ERR_ARG;
   std::memset(res, 0, sizeof *res);
+  ctx->err.clear();
   if (threshold != 0) {
     ctx->err = "relaxed matching (threshold > 0) is not supported";
     res->status = GEM_ERR_LIMIT;
@@ -763,6 +938,7 @@ extern "C" gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t t
   if (mode == GEM_MODE_ENUMERATE && emb_cap) ST(aalloc(ctx, emb_cap * q->nv, &d_emb));
   ST(run_wave(ctx, w, 0, mode, d_emb, emb_cap));
   wave_result(ctx, w, 0, res);
+  if (res->status == GEM_ERR_TIMEOUT) ctx->err = "device time cap reached before the count completed";
   if (mode == GEM_MODE_ENUMERATE) {
     uint64_t nw = std::min<uint64_t>(w.emb_written, emb_cap);
     res->n_written = nw;
@@ -775,6 +951,7 @@ extern "C" gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t t
 
 extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode, gem_result *res) {
   if (!ctx || (n && (!qs || !res))) return GEM_ERR_ARG;
+  if (ctx->server) return GEM_ERR_STATE;
   if (mode != GEM_MODE_COUNT && mode != GEM_MODE_HASH) return GEM_ERR_ARG;
   std::vector<HostQuery> all(n);
   std::vector<gem_status> vs(n, GEM_OK);
@@ -825,6 +1002,7 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
 extern "C" gem_status gem_filter(gem_ctx *ctx, const gem_query *q, uint32_t threshold, uint32_t *counts,
                                  uint32_t *cand_out, uint64_t cand_cap) {
   if (!ctx || !q || !counts) return GEM_ERR_ARG;
+  if (ctx->server) return GEM_ERR_STATE;
   if (!ctx->loaded) return GEM_ERR_STATE;
   Wave w;
   w.q.resize(1);
@@ -844,7 +1022,7 @@ extern "C" gem_status gem_edge_table(gem_ctx *ctx, const gem_query *q, uint32_t 
                                      uint64_t *offsets_out, uint64_t offsets_cap, uint32_t *values_out,
                                      uint64_t values_cap, uint64_t *n_keys, uint64_t *n_values) {
   if (!ctx || !q || !n_keys || !n_values) return GEM_ERR_ARG;
-  if (!ctx->loaded) return GEM_ERR_STATE;
+  if (!ctx->loaded || ctx->server) return GEM_ERR_STATE;
   Wave w;
   w.q.resize(1);
   ST(make_host_query(q, w.q[0], ctx->err));
@@ -857,6 +1035,7 @@ extern "C" gem_status gem_edge_table(gem_ctx *ctx, const gem_query *q, uint32_t 
   // a two-level plan: u then w
   Plan p;
   p.n = 2;
+  p.n_enum = 2;
   p.order[0] = u;
   p.order[1] = wv;
   p.back[1] = {0};
@@ -880,7 +1059,7 @@ extern "C" gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t
                                       const uint32_t *keys, uint32_t n_keys, uint32_t *pos_out) {
   if (!ctx || !q || (n_keys && (!keys || !pos_out))) return GEM_ERR_ARG;
   if (index_kind != IDX_RANK && index_kind != IDX_CUCKOO) return GEM_ERR_ARG;
-  if (!ctx->loaded) return GEM_ERR_STATE;
+  if (!ctx->loaded || ctx->server) return GEM_ERR_STATE;
   Wave w;
   w.q.resize(1);
   ST(make_host_query(q, w.q[0], ctx->err));
@@ -900,6 +1079,7 @@ extern "C" gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t
   } else {
     Plan p;
     p.n = 2;
+    p.n_enum = 2;
     p.order[0] = u == 0 ? 1 % w.q[0].nv : 0;
     p.order[1] = u;
     p.need_idx[1] = 1;

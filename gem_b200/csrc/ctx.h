@@ -11,6 +11,8 @@
 #include "kernels.h"
 
 struct gem_ctx;
+struct Server;
+void server_shutdown(gem_ctx *ctx);
 
 // Device memory in chunks obtained from cudaMalloc; bump-allocated, reset
 // between waves so steady-state queries never call cudaMalloc.
@@ -28,16 +30,25 @@ struct Arena {
   void release(gem_ctx *ctx);
 };
 
-// Matching order of one query.
+// Matching order of one query.  In count mode the last n - n_enum levels
+// (the suffix) form an independent set of the query graph whose completions
+// are counted in closed form; suffix levels are grouped by label.
 struct Plan {
   uint32_t n = 0;
+  uint32_t n_enum = 0;              // levels enumerated depth-first
   uint32_t order[gem::QV] = {};     // level -> query vertex
   uint32_t level_of[gem::QV] = {};  // query vertex -> level
   std::vector<uint32_t> back[gem::QV];  // backward neighbour levels
-  uint32_t dup_mask[gem::QV] = {};  // earlier levels with the same label
+  uint32_t dup_mask[gem::QV] = {};  // earlier enumerated levels with the same label
   uint32_t need_idx[gem::QV] = {};  // level's vertex keys a later table
+  struct Group {
+    uint32_t first = 0, size = 0;
+    std::vector<uint64_t> terms;    // inclusion-exclusion terms (see gem::JTerm packing)
+  };
+  std::vector<Group> groups;
 };
-void make_plan(const gem::HostQuery &q, const uint32_t *cnt, Plan &p);
+// count_suffix: choose a closed-form suffix (count mode only).
+void make_plan(const gem::HostQuery &q, const uint32_t *cnt, bool count_suffix, Plan &p);
 
 // One wave: a set of queries processed by shared launches.
 struct Wave {
@@ -81,8 +92,11 @@ struct gem_ctx {
   bool loaded = false;
   gem::DevGraph g;
   char *graph_mem = nullptr;
+  void *pinned_nbr = nullptr;        // out-of-core: mapped pinned adjacency
   uint64_t graph_bytes = 0;
-  std::vector<uint64_t> label_freq;
+  std::vector<uint64_t> label_freq;  // vertices per label
+  std::vector<uint64_t> label_arcs;  // sum of degrees per label
+  Server *server = nullptr;          // serving thread (gem_submit / gem_poll)
   // scratch
   Arena arena;
   gem::JControl *d_ctl = nullptr;
@@ -91,6 +105,7 @@ struct gem_ctx {
   void *h_small = nullptr;
   // tunables
   uint32_t donate_max_level = 30;
+  bool closed_form_suffix = true;
   uint32_t wave_max_rows = 4096;
 };
 

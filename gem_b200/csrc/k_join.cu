@@ -18,9 +18,11 @@
 //    label only (the reference's dup_check_type, join_trie.cu:450-462);
 //  * the state of level L lives in lane L's registers (levels <= 32), so a
 //    warp's whole DFS stack costs a few registers per lane and no memory;
-//  * the last level is never materialised; in count mode a last level with a
-//    single backward neighbour is counted in O(#same-label earlier levels)
-//    binary searches instead of scanning its list;
+//  * the last level is never materialised; in count mode the planner's
+//    closed-form suffix (an independent set of query vertices, e.g. the leaves
+//    of a tree) is counted by inclusion-exclusion per prefix match, and a
+//    suffix list with a single backward neighbour costs
+//    O(#same-label prefix levels) binary searches instead of a scan;
 //  * one persistent grid serves every query of a wave: warps take root
 //    candidates from a global counter and, once roots run out, receive work
 //    donated by busy warps (half of the unread candidates of a shallow
@@ -139,15 +141,57 @@ __device__ __forceinline__ uint32_t eval_chunk(const uint32_t *__restrict__ valu
   return __ballot_sync(FULL, ok);
 }
 
-// Count-mode last level: number of valid candidates of level lvl.
-__device__ __forceinline__ uint64_t count_last(const JLevel *__restrict__ L, const JBack *__restrict__ backs,
-                                               const uint32_t *__restrict__ values, const LaneState &c, Stats &st) {
-  uint32_t nback, src;
-  uint64_t my_lo, my_hi, s_lo, s_hi;
-  level_lists(L, backs, c, nback, my_lo, my_hi, src, s_lo, s_hi);
-  const uint32_t dup_mask = L->dup_mask;
+// Count mode, closed-form suffix.  The suffix levels form an independent set
+// of the query graph, so once the prefix is matched each suffix level's
+// candidates are fixed: A_i = intersection of its backward lists minus the
+// prefix vertices of its label.  Levels of different labels have disjoint
+// candidates; within a label group the number of injective assignments is
+// sum over set partitions pi of the group of
+//   prod_{B in pi} (-1)^{|B|-1} (|B|-1)! * |intersection_{i in B} A_i|
+// (inclusion-exclusion over coincidences).  All arithmetic wraps mod 2^64,
+// which is exact whenever the count itself fits in 64 bits.
+
+// |{x in A_i for every level i of `members`}| for the group starting at
+// level `first`; lists are spread one per lane (the planner keeps their
+// number <= 32).
+__device__ __forceinline__ uint64_t subset_count(const JQuery *__restrict__ Q, const JBack *__restrict__ backs,
+                                                 const uint32_t *__restrict__ values, const LaneState &c,
+                                                 uint32_t first, uint32_t members, uint32_t dup_mask, Stats &st) {
   const uint32_t lane = lane_id();
-  if (nback == 1) {
+  uint32_t nl = 0;
+  uint64_t my_lo = 0, my_hi = 0;
+  for (uint32_t m = members; m; m &= m - 1) {
+    const JLevel *__restrict__ L = &Q->lv[first + __ffs(m) - 1];
+    const uint32_t nb = L->nback;
+    const bool mine = lane >= nl && lane < nl + nb;
+    uint32_t klvl = 0;
+    const uint64_t *off = nullptr;
+    if (mine) {
+      const JBack *b = backs + L->back_base + (lane - nl);
+      klvl = b->lvl;
+      off = b->off;
+    }
+    const uint32_t kidx = __shfl_sync(FULL, c.idx, klvl);
+    if (mine) {
+      my_lo = __ldg(off + kidx);
+      my_hi = __ldg(off + kidx + 1);
+    }
+    nl += nb;
+  }
+  uint64_t best = lane < nl ? my_hi - my_lo : ~0ull;
+  uint32_t bl = lane;
+#pragma unroll
+  for (int d = 16; d; d >>= 1) {
+    const uint64_t ob = __shfl_xor_sync(FULL, best, d);
+    const uint32_t ol = __shfl_xor_sync(FULL, bl, d);
+    if (ob < best || (ob == best && ol < bl)) {
+      best = ob;
+      bl = ol;
+    }
+  }
+  const uint32_t src = bl;
+  const uint64_t s_lo = __shfl_sync(FULL, my_lo, src), s_hi = __shfl_sync(FULL, my_hi, src);
+  if (nl == 1) {
     bool hit = false;
     if ((dup_mask >> lane) & 1u) hit = contains_u32(values, s_lo, s_hi, c.f);
     if (lane == 0) st.probes += __popc(dup_mask);
@@ -156,9 +200,169 @@ __device__ __forceinline__ uint64_t count_last(const JLevel *__restrict__ L, con
   uint64_t cnt = 0;
   for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
     uint32_t w;
-    cnt += __popc(eval_chunk(values, cp, s_hi, nback, src, my_lo, my_hi, dup_mask, c, &w, st));
+    cnt += __popc(eval_chunk(values, cp, s_hi, nl, src, my_lo, my_hi, dup_mask, c, &w, st));
   }
   return cnt;
+}
+
+__device__ __noinline__ uint64_t suffix_count(const JQuery *__restrict__ Q, const JBack *__restrict__ backs,
+                                              const uint32_t *__restrict__ values, const uint64_t *__restrict__ terms,
+                                              const LaneState &c, Stats &st) {
+  uint64_t total = 1;
+  const uint32_t ng = Q->n_groups;
+  for (uint32_t g = 0; g < ng && total; ++g) {
+    const uint32_t first = Q->grp_first[g], gs = Q->grp_size[g];
+    const uint32_t dup_mask = Q->lv[first].dup_mask;
+    if (gs == 1) {
+      total *= subset_count(Q, backs, values, c, first, 1u, dup_mask, st);
+      continue;
+    }
+    uint64_t sv[1u << MAX_GROUP];
+    bool empty = false;
+    for (uint32_t S = 1; S < (1u << gs); ++S) {
+      sv[S] = subset_count(Q, backs, values, c, first, S, dup_mask, st);
+      if (sv[S] == 0 && __popc(S) == 1) {
+        empty = true;
+        break;
+      }
+    }
+    if (empty) {
+      total = 0;
+      break;
+    }
+    uint64_t G = 0;
+    const uint32_t tb = Q->term_base[g], tc = Q->term_count[g];
+    for (uint32_t t = 0; t < tc; ++t) {
+      const uint64_t term = __ldg(terms + tb + t);
+      uint64_t prod = (uint64_t)(int64_t)(int32_t)(uint32_t)(term >> 32);
+      const uint32_t blocks = (uint32_t)term;
+#pragma unroll
+      for (uint32_t b = 0; b < MAX_GROUP; ++b) {
+        const uint32_t mk = (blocks >> (4 * b)) & 15u;
+        if (!mk) break;
+        prod *= sv[mk];
+      }
+      G += prod;
+    }
+    total *= G;
+  }
+  return total;
+}
+
+// Lane-parallel form of the suffix count used at the last enumerated level:
+// every lane owns one candidate w of level L = n_enum - 1 (position widx in
+// C(u_L)); the earlier levels' vertices and positions come from the warp's
+// shared copy (sf, sidx).  Lists are addressed by index through the members'
+// backward entries, so no per-lane arrays are needed.
+struct LaneCtx {
+  const JQuery *Q;
+  const JBack *backs;
+  const uint32_t *values;
+  uint32_t L, w, widx;
+  const uint32_t *sf, *sidx;
+};
+
+__device__ __forceinline__ void lane_list(const LaneCtx &x, uint32_t first, uint32_t members, uint32_t li,
+                                          uint64_t &lo, uint64_t &hi) {
+  for (uint32_t m = members; m; m &= m - 1) {
+    const JLevel *M = &x.Q->lv[first + __ffs(m) - 1];
+    const uint32_t nb = M->nback;
+    if (li < nb) {
+      const JBack *b = x.backs + M->back_base + li;
+      const uint32_t kl = b->lvl;
+      const uint32_t kidx = kl == x.L ? x.widx : x.sidx[kl];
+      lo = __ldg(b->off + kidx);
+      hi = __ldg(b->off + kidx + 1);
+      return;
+    }
+    li -= nb;
+  }
+  lo = hi = 0;
+}
+
+__device__ uint64_t lane_subset_count(const LaneCtx &x, uint32_t first, uint32_t members, uint32_t dup_mask,
+                                      Stats &st) {
+  uint32_t nl = 0;
+  for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[first + __ffs(m) - 1].nback;
+  uint32_t s = 0;
+  uint64_t s_lo = 0, s_hi = 0;
+  for (uint32_t i = 0; i < nl; ++i) {
+    uint64_t lo, hi;
+    lane_list(x, first, members, i, lo, hi);
+    if (i == 0 || hi - lo < s_hi - s_lo) {
+      s = i;
+      s_lo = lo;
+      s_hi = hi;
+    }
+  }
+  if (nl == 1) {
+    uint64_t c = s_hi - s_lo;
+    for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
+      const uint32_t j = __ffs(dm) - 1;
+      const uint32_t v = j == x.L ? x.w : x.sf[j];
+      if (contains_u32(x.values, s_lo, s_hi, v)) --c;
+    }
+    st.probes += __popc(dup_mask);
+    return c;
+  }
+  uint64_t c = 0;
+  for (uint64_t e = s_lo; e < s_hi; ++e) {
+    const uint32_t v = __ldg(x.values + e);
+    bool ok = true;
+    for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
+      const uint32_t j = __ffs(dm) - 1;
+      ok = v != (j == x.L ? x.w : x.sf[j]);
+    }
+    for (uint32_t i = 0; i < nl && ok; ++i) {
+      if (i == s) continue;
+      uint64_t lo, hi;
+      lane_list(x, first, members, i, lo, hi);
+      ok = contains_u32(x.values, lo, hi, v);
+    }
+    c += ok;
+  }
+  st.scanned += s_hi - s_lo;
+  st.probes += (s_hi - s_lo) * (nl - 1);
+  return c;
+}
+
+__device__ uint64_t lane_suffix_count(const LaneCtx &x, const uint64_t *__restrict__ terms, Stats &st) {
+  const JQuery *Q = x.Q;
+  uint64_t total = 1;
+  const uint32_t ng = Q->n_groups;
+  for (uint32_t g = 0; g < ng && total; ++g) {
+    const uint32_t first = Q->grp_first[g], gs = Q->grp_size[g];
+    const uint32_t dup_mask = Q->lv[first].dup_mask;
+    if (gs == 1) {
+      total *= lane_subset_count(x, first, 1u, dup_mask, st);
+      continue;
+    }
+    uint64_t sv[1u << MAX_GROUP];
+    bool empty = false;
+    for (uint32_t S = 1; S < (1u << gs); ++S) {
+      sv[S] = lane_subset_count(x, first, S, dup_mask, st);
+      if (sv[S] == 0 && __popc(S) == 1) {
+        empty = true;
+        break;
+      }
+    }
+    if (empty) return 0;
+    uint64_t G = 0;
+    const uint32_t tb = Q->term_base[g], tc = Q->term_count[g];
+    for (uint32_t t = 0; t < tc; ++t) {
+      const uint64_t term = __ldg(terms + tb + t);
+      uint64_t prod = (uint64_t)(int64_t)(int32_t)(uint32_t)(term >> 32);
+      const uint32_t blocks = (uint32_t)term;
+      for (uint32_t b = 0; b < MAX_GROUP; ++b) {
+        const uint32_t mk = (blocks >> (4 * b)) & 15u;
+        if (!mk) break;
+        prod *= sv[mk];
+      }
+      G += prod;
+    }
+    total *= G;
+  }
+  return total;
 }
 
 __device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
@@ -324,10 +528,73 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
   const uint32_t *__restrict__ values = a.values;
   const JBack *__restrict__ backs = a.backs;
   const uint64_t deadline = ctl->deadline_ns;
+  __shared__ uint32_t s_pref[8][2][QV];  // per warp: f and idx of the enumerated prefix
+  uint32_t *sf = s_pref[threadIdx.x >> 5][0], *sidx = s_pref[threadIdx.x >> 5][1];
   LaneState c;
   c.f = 0; c.idx = 0; c.hs = 0; c.pos = 0; c.end = 0; c.cbase = 0; c.mask = 0; c.src = 0;
   Stats st;
   bool idle_registered = false;
+
+  // ---------------------------------------------------------------- lane-parallel roots
+  // Queries whose only enumerated level is the root: one root per lane.
+  if (a.lp_roots) {
+    uint32_t it = 0;
+    for (;;) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&ctl->lp_next, 32ull);
+      base = __shfl_sync(FULL, base, 0);
+      if (base >= a.lp_roots) break;
+      if ((++it & 15u) == 0) {
+        int stop = 0;
+        if (lane == 0) {
+          if (ld_vol(&ctl->err) != DERR_NONE) stop = 1;
+          else if (globaltimer_ns() > deadline) {
+            set_error(&ctl->err, DERR_TIMEOUT);
+            stop = 1;
+          }
+          if (stop) {
+            // this block and every unclaimed root of the pool are abandoned
+            const unsigned long long r0 = atomicExch(&ctl->lp_next, (unsigned long long)a.lp_roots);
+            const unsigned long long from = base < r0 ? base : r0;
+            for (uint32_t k = find_query(a.lp_prefix, a.lp_nq, from); k < a.lp_nq; ++k)
+              atomicOr(&a.out[a.lp_query[k]].pad[0], 1ull);
+          }
+        }
+        if (__shfl_sync(FULL, stop, 0)) break;
+      }
+      const uint64_t r = base + lane;
+      if (r < a.lp_roots) {
+        const uint32_t k = find_query(a.lp_prefix, a.lp_nq, r);
+        const uint32_t q = a.lp_query[k];
+        const JQuery *Q = a.queries + q;
+        const uint32_t rl = (uint32_t)(r - __ldg(a.lp_prefix + k));
+        const uint32_t w0 = __ldg(Q->root_cand + rl);
+        uint64_t cnt = 0, h = 0;
+        if (Q->n == 1) {
+          cnt = 1;
+          if (MODE != MODE_COUNT) h = mix64(emb_term(Q->root_u, w0));
+          if (MODE == MODE_ENUM) {
+            const unsigned long long s = atomicAdd(&ctl->emb_next, 1ull);
+            if (s < a.emb_cap) a.emb[s] = w0;
+          }
+        } else {
+          LaneCtx x;
+          x.Q = Q;
+          x.backs = backs;
+          x.values = values;
+          x.L = 0;
+          x.w = w0;
+          x.widx = rl;
+          x.sf = sf;
+          x.sidx = sidx;
+          cnt = lane_suffix_count(x, a.terms, st);
+        }
+        if (cnt) atomicAdd(&a.out[q].count, (unsigned long long)cnt);
+        if (h) atomicAdd(&a.out[q].hash, (unsigned long long)h);
+      }
+      if (lane == 0) st.nodes += (a.lp_roots - base) < 32 ? (a.lp_roots - base) : 32;
+    }
+  }
 
   for (;;) {
     // ------------------------------------------------------------ acquire
@@ -433,9 +700,9 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         }
         lvl = 0;  // nothing to iterate
         base_lvl = 1;
-      } else if (MODE == MODE_COUNT && n == 2) {
+      } else if (MODE == MODE_COUNT && Q->n_enum == 1) {
         st.nodes += lane == 0;
-        const uint64_t k = count_last(&Q->lv[1], backs, values, c, st);
+        const uint64_t k = suffix_count(Q, backs, values, a.terms, c, st);
         if (lane == 0) lane_cnt += k;
         lvl = 0;
         base_lvl = 1;
@@ -492,6 +759,38 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         if (MODE != MODE_COUNT && lvl == n - 1) {
           emit_last<MODE>(a, Q, lvl, m, w, c, lane_cnt, lane_hash);
           if (lane == lvl) c.pos = pos + 32;
+        } else if (MODE == MODE_COUNT && lvl + 1 == Q->n_enum) {
+          // last enumerated level: each lane counts its own candidate's
+          // suffix completions (32 prefix matches in flight per warp)
+          if (lane < lvl) {
+            sf[lane] = c.f;
+            sidx[lane] = c.idx;
+          }
+          __syncwarp();
+          if ((m >> lane) & 1u) {
+            LaneCtx x;
+            x.Q = Q;
+            x.backs = backs;
+            x.values = values;
+            x.L = lvl;
+            x.w = w;
+            x.widx = index_of(L, w);
+            x.sf = sf;
+            x.sidx = sidx;
+            lane_cnt += lane_suffix_count(x, a.terms, st);
+          }
+          __syncwarp();
+          if (lane == 0) st.nodes += __popc(m);
+          uint64_t new_end = end;
+          if (lvl <= a.donate_max_level && end > pos + 32 + 64 && ld_vol(&ctl->idle) > 0) {
+            const uint64_t rem = pos + 32;
+            const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
+            if (mid < end && queue_push(ctl, a.queue, q, lvl, src, mid, end, 0ull, c)) new_end = mid;
+          }
+          if (lane == lvl) {
+            c.pos = pos + 32;
+            c.end = new_end;
+          }
         } else {
           uint64_t new_end = end;
           if (lvl <= a.donate_max_level && end > pos + 32 + 64 && ld_vol(&ctl->idle) > 0) {
@@ -528,8 +827,8 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         st.probes += L->idx_kind != IDX_NONE;
       }
       const uint32_t nxt = lvl + 1;
-      if (MODE == MODE_COUNT && nxt == n - 1) {
-        const uint64_t k = count_last(&Q->lv[nxt], backs, values, c, st);
+      if (MODE == MODE_COUNT && nxt == Q->n_enum) {
+        const uint64_t k = suffix_count(Q, backs, values, a.terms, c, st);
         if (lane == 0) lane_cnt += k;
         continue;
       }

@@ -164,13 +164,27 @@ struct JBack {
   uint32_t pad;
   const uint64_t *off;       // table offsets (absolute into the values array)
 };
+constexpr uint32_t MAX_GROUPS = 16;   // label groups of a closed-form suffix
+constexpr uint32_t MAX_GROUP = 4;     // members of one group (15 subsets, 15 partitions)
+// Inclusion-exclusion term: coefficient in the high 32 bits (two's
+// complement), then up to four 4-bit block masks over the group's members
+// (block b in bits 4b..4b+3; a zero mask ends the list).
+inline uint64_t make_term(int32_t coef, uint32_t packed_blocks) {
+  return ((uint64_t)(uint32_t)coef << 32) | packed_blocks;
+}
 struct JQuery {
   uint32_t n;                // query vertices (levels)
   uint32_t root_u;
   const uint32_t *root_cand; // C(root)
   uint32_t n_root;
-  uint32_t pad;
+  uint32_t n_enum;           // levels enumerated; levels n_enum..n-1 are counted in closed form
   uint64_t root_base;        // first global root index of this query
+  uint32_t n_groups;         // label groups of the suffix
+  uint32_t pad2;
+  uint32_t grp_first[MAX_GROUPS];
+  uint32_t grp_size[MAX_GROUPS];
+  uint32_t term_base[MAX_GROUPS];
+  uint32_t term_count[MAX_GROUPS];
   JLevel lv[QV];             // lv[0] describes the root's index only
 };
 struct JOut {                // per query, accumulated with atomics
@@ -193,6 +207,7 @@ struct JTask {
   uint32_t idx[QV];
 };
 struct JControl {            // zeroed before every launch (except queue seq init)
+  unsigned long long lp_next;    // next root of the lane-parallel pool
   unsigned long long root_next;
   unsigned long long tail;
   unsigned long long head;
@@ -211,6 +226,14 @@ struct JoinArgs {
   const JBack *backs;
   const uint32_t *values;     // edge-table values of the whole wave
   const uint64_t *root_prefix; // nquery + 1 global root offsets
+  // Lane-parallel root pool: queries whose only enumerated level is the root
+  // (count mode with n_enum == 1, or single-vertex queries); 32 roots per warp.
+  const uint32_t *lp_query;    // query index of each pool segment
+  const uint64_t *lp_prefix;   // lp_nq + 1 root offsets
+  uint32_t lp_nq;
+  uint32_t pad_lp;
+  uint64_t lp_roots;
+  const uint64_t *terms;      // inclusion-exclusion terms of every query's suffix groups
   uint64_t n_roots;
   JOut *out;
   JControl *ctl;

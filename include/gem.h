@@ -138,7 +138,8 @@ typedef struct gem_opts {
   int ooc;                      /* 1 = keep the data graph in pinned host memory */
   uint32_t time_cap_ms;         /* per-query/batch device time cap (0 = 600000) */
   uint32_t index_kind;          /* 0 = auto, 1 = rank bitmap, 2 = cuckoo hash */
-  uint32_t reserved[6];
+  uint32_t admit_gb;            /* serving admission budget in GiB (0 = 120) */
+  uint32_t reserved[5];
 } gem_opts;
 
 gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out);
@@ -238,6 +239,10 @@ gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t u,
 
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching with memory-based admission.                 */
+/* The first gem_submit starts a server thread on the context; from then on  */
+/* only gem_submit and gem_poll are accepted (others return GEM_ERR_STATE)   */
+/* until gem_ctx_destroy.  Admitted requests run in waves: everything        */
+/* admitted while a wave is on the GPU forms the next wave.                  */
 /* ------------------------------------------------------------------------ */
 /* Submit a query; returns GEM_ERR_OOM when its estimated device bytes do not
  * fit the admission budget right now (caller retries later). */

@@ -190,12 +190,21 @@ def test_edge_cases(small, gctx):
         gctx.run(gem.Query([0, 1], [(0, 1)]), threshold=1)
 
 
-def test_max_size_queries(small, gctx):
-    for q in gem.gen_queries(small, 32, gem.DENSE, 2, seed=3210):
-        exp, eh, ok = oracle.count(small, q, work_cap=200_000_000)
-        r = gctx.run(q, mode=gem.MODE_HASH)
-        if ok:
-            assert (r["count"], r["emb_hash"]) == (exp, eh)
+def test_max_size_queries(tiny):
+    with gem.Context(time_cap_ms=20000) as c:
+        c.load_graph(tiny)
+        done = 0
+        for q in gem.gen_queries(tiny, 32, gem.DENSE, 4, seed=3210):
+            assert q.nv == 32
+            exp, eh, ok = oracle.count(tiny, q, work_cap=300_000_000)
+            if not ok:
+                continue
+            r = c.run(q, mode=gem.MODE_HASH, raise_on_error=False)
+            assert r["status"] in ("OK", "ERR_TIMEOUT")
+            if r["status"] == "OK":
+                assert (r["count"], r["emb_hash"]) == (exp, eh)
+                assert c.run(q)["count"] == exp
+                done += 1
 
 
 def test_time_cap_reports_timeout():
@@ -208,3 +217,97 @@ def test_time_cap_reports_timeout():
         # the context stays usable after a timeout
         r2 = c.run(gem.Query([0], []))
         assert r2["status"] == "OK" and r2["count"] == g.nv
+
+
+SUFFIX_SHAPES = {
+    # name: (labels, edges)
+    "star4_same": ([0, 1, 1, 1, 1], [(0, 1), (0, 2), (0, 3), (0, 4)]),
+    "star3_mixed": ([0, 1, 1, 2], [(0, 1), (0, 2), (0, 3)]),
+    "star3_all_same": ([1, 1, 1, 1], [(0, 1), (0, 2), (0, 3)]),
+    "double_star": ([0, 0, 1, 1, 1, 1], [(0, 1), (0, 2), (0, 3), (1, 4), (1, 5)]),
+    "path5_same": ([1, 1, 1, 1, 1], [(0, 1), (1, 2), (2, 3), (3, 4)]),
+    "cycle4_leaves": ([0, 1, 0, 1, 2, 2], [(0, 1), (1, 2), (2, 3), (3, 0), (0, 4), (2, 5)]),
+    "triangle_tail": ([0, 0, 1, 1], [(0, 1), (1, 2), (2, 0), (2, 3)]),
+    "k4_leaves": ([0, 1, 2, 0, 1, 1], [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3), (3, 4), (0, 5)]),
+    "two_parents_same_leaf_label": ([0, 1, 2, 2, 2], [(0, 1), (0, 2), (1, 3), (1, 4), (0, 4)]),
+}
+
+
+@pytest.fixture(scope="module")
+def tiny():
+    return gem.HostGraph.rmat(10, 8, seed=77).set_labels(3, 0.0, seed=78)
+
+
+@pytest.mark.parametrize("shape", sorted(SUFFIX_SHAPES))
+def test_closed_form_suffix_shapes(tiny, shape):
+    labels, edges = SUFFIX_SHAPES[shape]
+    q = gem.Query(labels, edges)
+    exp, eh, ok = oracle.count(tiny, q, work_cap=2_000_000_000)
+    assert ok
+    with gem.Context(time_cap_ms=30000) as c:
+        c.load_graph(tiny)
+        rc = c.run(q, mode=gem.MODE_COUNT)
+        rh = c.run(q, mode=gem.MODE_HASH)
+    assert rc["count"] == exp, (shape, rc["count"], exp)
+    assert (rh["count"], rh["emb_hash"]) == (exp, eh)
+
+
+def test_suffix_random_queries_tiny(tiny):
+    for k in (3, 4, 5, 6, 7):
+        for d in (gem.SPARSE, gem.ANY):
+            for q in gem.gen_queries(tiny, k, d, 5, seed=900 + 10 * k + d):
+                exp, _, ok = oracle.count(tiny, q, want_hash=False, work_cap=500_000_000)
+                if not ok:
+                    continue
+                with gem.Context(time_cap_ms=30000) as c:
+                    c.load_graph(tiny)
+                    assert c.run(q)["count"] == exp, (q.labels.tolist(), q.edges.tolist())
+
+
+def test_serving_matches_plain(small):
+    qs = []
+    for k in (3, 4, 5):
+        for q in gem.gen_queries(small, k, gem.ANY, 8, seed=4000 + k):
+            if oracle.count(small, q, want_hash=False, work_cap=100_000_000)[2]:
+                qs.append(q)
+    with gem.Context(time_cap_ms=30000) as plain_ctx:
+        plain_ctx.load_graph(small)
+        alone = [plain_ctx.run(q, mode=gem.MODE_HASH) for q in qs]
+    import random
+    import time
+    rng = random.Random(5)
+    with gem.Context(time_cap_ms=30000) as srv:
+        srv.load_graph(small)
+        tickets, pending, results = {}, list(range(len(qs))), {}
+        # staggered arrivals: submit a few, poll, submit more while waves run
+        while pending or tickets:
+            for _ in range(rng.randint(1, 4)):
+                if pending:
+                    i = pending.pop(0)
+                    t = srv.submit(qs[i], mode=gem.MODE_HASH)
+                    if t is None:
+                        pending.insert(0, i)
+                        break
+                    tickets[t] = i
+            for t in list(tickets):
+                r = srv.poll(t)
+                if r is not None:
+                    results[tickets.pop(t)] = r
+            time.sleep(0.001)
+        with pytest.raises(gem.GemError):
+            srv.run(qs[0])  # the serving context accepts only submit/poll
+    waves = {r["wave"] for r in results.values()}
+    for i, a in enumerate(alone):
+        assert (results[i]["count"], results[i]["emb_hash"]) == (a["count"], a["emb_hash"])
+    assert len(waves) >= 1
+
+
+def test_out_of_core_same_counts(small):
+    qs = [q for q in gem.gen_queries(small, 5, gem.ANY, 6, seed=6100)
+          if oracle.count(small, q, want_hash=False, work_cap=100_000_000)[2]]
+    with gem.Context(time_cap_ms=30000) as a, gem.Context(time_cap_ms=30000, ooc=True, budget_bytes=2 << 30) as b:
+        a.load_graph(small)
+        b.load_graph(small)
+        for q in qs:
+            ra, rb = a.run(q, mode=gem.MODE_HASH), b.run(q, mode=gem.MODE_HASH)
+            assert (ra["count"], ra["emb_hash"]) == (rb["count"], rb["emb_hash"])
