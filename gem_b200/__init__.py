@@ -43,7 +43,7 @@ EXPORTS = (
     "gem_hgraph_destroy", "gem_query_read_text", "gem_query_write_text", "gem_gen_queries",
     "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
-    "gem_submit", "gem_poll",
+    "gem_submit", "gem_poll", "gem_autotune",
 )
 
 
@@ -114,6 +114,7 @@ def lib():
         L.gem_index_probe.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_uint32, u32p, C.c_uint32, u32p]
         L.gem_submit.argtypes = [vp, C.POINTER(_Query), C.c_int, u64p]
         L.gem_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Result), C.POINTER(C.c_int)]
+        L.gem_autotune.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, C.c_uint32, u32p]
         _lib = L
     return _lib
 
@@ -333,6 +334,11 @@ class Context:
         st = lib().gem_query_run(self._h, C.byref(qc), threshold, mode, _p32(buf) if buf is not None else None,
                                  emb_cap, C.byref(r))
         res = Result._from(r)
+        if st != 0 and res["status_code"] == 0:
+            res["status"], res["status_code"] = STATUS.get(st, st), st
+        if st != 0:
+            m = lib().gem_last_error(self._h)
+            res["error"] = m.decode() if m else ""
         if mode == MODE_ENUMERATE:
             res["embeddings"] = buf[: res["n_written"] * q.nv].reshape(-1, q.nv)
         if st != 0 and raise_on_error and st != 8:
@@ -348,7 +354,21 @@ class Context:
         rs = (_Result * len(qs))()
         st = lib().gem_batch_run(self._h, arr, len(qs), mode, rs)
         out = [Result._from(r) for r in rs]
+        if st != 0:
+            m = lib().gem_last_error(self._h)
+            for r in out:
+                r["error"] = m.decode() if m else ""
         return st, out
+
+    def autotune(self, qs, mode=MODE_COUNT, trial_cap_ms=2000):
+        """Tune the join schedule per query-size bucket; returns {bucket: (blocks/SM, donate level, us)}."""
+        arr = (_Query * max(len(qs), 1))()
+        for i, q in enumerate(qs):
+            arr[i] = q._c()
+        rep = np.zeros(18, np.uint32)
+        _check(lib().gem_autotune(self._h, arr, len(qs), mode, trial_cap_ms, _p32(rep)), self._h, "autotune")
+        names = ("<=4", "<=8", "<=12", "<=16", "<=24", "<=32")
+        return {names[b]: tuple(int(x) for x in rep[3 * b:3 * b + 3]) for b in range(6) if rep[3 * b]}
 
     def submit(self, q, mode=MODE_COUNT):
         """Serving: returns a ticket, or None when admission is busy (retry later)."""

@@ -13,6 +13,7 @@
 #include <chrono>
 #include <functional>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -176,6 +177,7 @@ extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
   cudaStreamSynchronize(ctx->s);
   ctx->arena.release(ctx);
   free_graph(ctx);
+  destroy_join_graph(ctx->jgraph);
   if (ctx->d_ctl) cudaFree(ctx->d_ctl);
   if (ctx->d_queue) cudaFree(ctx->d_queue);
   if (ctx->d_err) cudaFree(ctx->d_err);
@@ -429,6 +431,34 @@ void make_plan(const HostQuery &q, const uint32_t *cnt, bool count_suffix, Plan 
   }
   for (uint32_t k = 0; k < n; ++k)
     for (uint32_t j : p.back[k]) p.need_idx[j] = 1;
+}
+
+// Structural checks of a plan (host side, before anything reaches the device).
+static bool validate_plan(const HostQuery &q, const Plan &p, std::string &why) {
+  if (p.n != q.nv || p.n_enum < 1 || p.n_enum > p.n) return why = "level counts", false;
+  uint32_t seen = 0;
+  for (uint32_t k = 0; k < p.n; ++k) {
+    if (p.order[k] >= q.nv || (seen & (1u << p.order[k]))) return why = "order is not a permutation", false;
+    seen |= 1u << p.order[k];
+    if (k > 0 && p.back[k].empty()) return why = "level without backward neighbour", false;
+    for (uint32_t j : p.back[k]) {
+      if (j >= k) return why = "backward neighbour after its level", false;
+      if (k >= p.n_enum && j >= p.n_enum) return why = "suffix level keyed by a suffix level", false;
+      if (!p.need_idx[j]) return why = "key level without index", false;
+    }
+    if (p.dup_mask[k] >> (k < p.n_enum ? k : p.n_enum)) return why = "injectivity mask beyond the prefix", false;
+  }
+  uint32_t covered = 0;
+  for (const auto &g : p.groups) {
+    if (g.size == 0 || g.size > MAX_GROUP || g.first < p.n_enum || g.first + g.size > p.n)
+      return why = "suffix group bounds", false;
+    uint32_t nb = 0;
+    for (uint32_t k = g.first; k < g.first + g.size; ++k) nb += (uint32_t)p.back[k].size();
+    if (nb > 32) return why = "suffix group lists", false;
+    covered += g.size;
+  }
+  if (p.groups.size() > MAX_GROUPS || covered != p.n - p.n_enum) return why = "suffix groups", false;
+  return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -732,10 +762,15 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
       L.rb = w.d_rb + (uint64_t)(w.row_base[qi] + p.order[k]) * w.nwords;
       L.ck = w.ck_of[qi][k];
       for (uint32_t j : p.back[k]) {
+        const uint32_t ei = w.edge_of[qi][j * QV + k];
+        if (ei >= w.edges.size()) {
+          ctx->err = "internal: missing edge table for a backward neighbour";
+          return GEM_ERR_INTERNAL;
+        }
         JBack b;
         b.lvl = j;
-        b.pad = 0;
-        b.off = w.edges[w.edge_of[qi][j * QV + k]].offsets;
+        b.nkeys = w.cnt[w.row_base[qi] + p.order[j]];
+        b.off = w.edges[ei].offsets;
         jb.push_back(b);
       }
     }
@@ -777,11 +812,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   CU(cudaMemcpyAsync(d_jq, jq.data(), jq.size() * sizeof(JQuery), cudaMemcpyHostToDevice, ctx->s));
   if (!jb.empty()) CU(cudaMemcpyAsync(d_jb, jb.data(), jb.size() * sizeof(JBack), cudaMemcpyHostToDevice, ctx->s));
   CU(cudaMemcpyAsync(d_rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, ctx->s));
-  CU(cudaMemsetAsync(d_out, 0, jq.size() * sizeof(JOut), ctx->s));
-  CU(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(JControl), ctx->s));
-  join_queue_init(ctx->d_queue, ctx->s);
   const uint64_t cap_ms = ctx->opts.time_cap_ms ? ctx->opts.time_cap_ms : 600000u;
-  launch_set_deadline(&ctx->d_ctl->deadline_ns, cap_ms * 1000000ull, ctx->s);
   JoinArgs a;
   std::memset(&a, 0, sizeof a);
   a.queries = d_jq;
@@ -801,9 +832,19 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   a.queue = ctx->d_queue;
   a.emb = emb_dev;
   a.emb_cap = emb_cap;
-  a.donate_max_level = ctx->donate_max_level;
+  // schedule: tuned per query-size bucket (largest query of the wave)
+  uint32_t maxnv = 0;
+  for (auto &J : jq) maxnv = std::max(maxnv, J.n);
+  const Tune &tu = ctx->tune[size_bucket(maxnv)];
+  a.donate_max_level = tu.donate_max_level ? tu.donate_max_level : ctx->donate_max_level;
+  a.nv = ctx->g.nv;
+  a.n_values = w.table_values;
+  a.n_backs = (uint32_t)jb.size();
+  a.n_terms = (uint32_t)terms.size();
+  int bps = ctx->join_bps[mode];
+  if (tu.blocks_per_sm && (int)tu.blocks_per_sm < bps) bps = (int)tu.blocks_per_sm;
   CU(cudaEventRecord(ctx->ev[6], ctx->s));
-  launch_join(a, ctx->join_bps[mode], ctx->s);
+  CU(launch_join_graph(ctx->jgraph, a, cap_ms * 1000000ull, (uint32_t)(ctx->sms * bps), ctx->s));
   CU(cudaEventRecord(ctx->ev[7], ctx->s));
   CU(cudaGetLastError());
   std::vector<JOut> out(jq.size());
@@ -828,6 +869,13 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   w.join_probes = out[0].probes;
   w.emb_written = hc.emb_next;
   w.join_err = hc.err;
+  if (hc.err == 4u /* bounds check failed (device_common.cuh DERR_BOUNDS) */) {
+    static const char *sites[] = {"?", "back entry", "table key", "table range", "vertex id", "task query",
+                                  "level", "root position", "suffix term", "key level"};
+    ctx->err = std::string("join bounds check failed: ") + sites[hc.bad_site < 10 ? hc.bad_site : 0] +
+               " index " + std::to_string(hc.bad_value) + " >= limit " + std::to_string(hc.bad_limit);
+    return GEM_ERR_INTERNAL;
+  }
   // algorithmic bytes: per extended partial embedding its index word and the
   // offsets pair of each table it keys; per evaluated candidate its id; per
   // binary search a 16-byte sector beyond the cached upper levels.
@@ -850,8 +898,22 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
   w.plan.assign(nq, Plan());
   w.idx_kind.assign(nq, std::vector<uint32_t>(QV, 0));
   w.ck_of.assign(nq, std::vector<const CuckooTable *>(QV, nullptr));
+  // GEM_DEBUG_SYNC=1: synchronise after every phase so a device fault is
+  // attributed to the phase that caused it.
+  static const bool dbg = getenv("GEM_DEBUG_SYNC") && getenv("GEM_DEBUG_SYNC")[0] == '1';
+  auto phase_sync = [&](const char *name) -> gem_status {
+    if (!dbg) return GEM_OK;
+    cudaError_t e = cudaStreamSynchronize(ctx->s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      ctx->err = std::string("device error after ") + name + ": " + cudaGetErrorString(e);
+      return GEM_ERR_CUDA;
+    }
+    return GEM_OK;
+  };
   CU(cudaEventRecord(ctx->ev[0], ctx->s));
   ST(wave_filter(ctx, w, threshold));
+  ST(phase_sync("filter"));
   CU(cudaEventRecord(ctx->ev[1], ctx->s));
   auto h0 = std::chrono::steady_clock::now();
   for (size_t qi = 0; qi < nq; ++qi) {
@@ -864,13 +926,21 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
       continue;
     }
     make_plan(q, &w.cnt[w.row_base[qi]], mode == GEM_MODE_COUNT && ctx->closed_form_suffix, w.plan[qi]);
+    std::string why;
+    if (!validate_plan(q, w.plan[qi], why)) {
+      ctx->err = "internal: invalid plan (" + why + ")";
+      return GEM_ERR_INTERNAL;
+    }
   }
   w.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
   ST(wave_tables(ctx, w));
+  ST(phase_sync("edge tables"));
   CU(cudaEventRecord(ctx->ev[2], ctx->s));
   ST(wave_index(ctx, w));
+  ST(phase_sync("index"));
   CU(cudaEventRecord(ctx->ev[3], ctx->s));
   ST(wave_join(ctx, w, mode, emb_dev, emb_cap));
+  ST(phase_sync("join"));
   CU(cudaEventRecord(ctx->ev[4], ctx->s));
   CU(cudaStreamSynchronize(ctx->s));
   w.filter_ms = ev_ms(ctx->ev[0], ctx->ev[1]);
@@ -936,7 +1006,13 @@ extern "C" gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t t
   ctx->arena.reset();
   uint32_t *d_emb = nullptr;
   if (mode == GEM_MODE_ENUMERATE && emb_cap) ST(aalloc(ctx, emb_cap * q->nv, &d_emb));
-  ST(run_wave(ctx, w, 0, mode, d_emb, emb_cap));
+  {
+    const gem_status st = run_wave(ctx, w, 0, mode, d_emb, emb_cap);
+    if (st != GEM_OK) {
+      res->status = st;
+      return st;
+    }
+  }
   wave_result(ctx, w, 0, res);
   if (res->status == GEM_ERR_TIMEOUT) ctx->err = "device time cap reached before the count completed";
   if (mode == GEM_MODE_ENUMERATE) {
@@ -1095,4 +1171,65 @@ extern "C" gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t
   if (n_keys) CU(cudaMemcpyAsync(pos_out, d_out, 4ull * n_keys, cudaMemcpyDeviceToHost, ctx->s));
   CU(cudaStreamSynchronize(ctx->s));
   return GEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: per query-size bucket, the join schedule (blocks per SM of the
+// persistent grid, deepest level that donates work) with the lowest join
+// time on a sample of the caller's queries.
+// ---------------------------------------------------------------------------
+extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode, uint32_t trial_cap_ms,
+                                   uint32_t *report) {
+  if (!ctx || (n && !qs)) return GEM_ERR_ARG;
+  if (mode != GEM_MODE_COUNT && mode != GEM_MODE_HASH) return GEM_ERR_ARG;
+  if (!ctx->loaded || ctx->server) return GEM_ERR_STATE;
+  std::vector<HostQuery> byb[6];
+  for (uint32_t i = 0; i < n; ++i) {
+    HostQuery h;
+    std::string e;
+    if (make_host_query(&qs[i], h, e) != GEM_OK) continue;
+    auto &v = byb[size_bucket(h.nv)];
+    if (v.size() < 8) v.push_back(h);
+  }
+  const int occ = ctx->join_bps[mode];
+  std::vector<uint32_t> bps_c = {(uint32_t)occ};
+  if (occ > 1) bps_c.push_back((uint32_t)occ - 1);
+  if (occ > 2) bps_c.push_back((uint32_t)(occ + 1) / 2);
+  const uint32_t don_c[3] = {2, 6, 30};
+  const uint32_t saved_cap = ctx->opts.time_cap_ms;
+  ctx->opts.time_cap_ms = trial_cap_ms ? trial_cap_ms : 2000;
+  gem_status st = GEM_OK;
+  for (uint32_t b = 0; b < 6 && st == GEM_OK; ++b) {
+    if (byb[b].empty()) continue;
+    Tune best;
+    double best_cost = 1e300;
+    for (uint32_t bps : bps_c)
+      for (uint32_t dm : don_c) {
+        ctx->tune[b].blocks_per_sm = bps;
+        ctx->tune[b].donate_max_level = dm;
+        Wave w;
+        w.q = byb[b];
+        ctx->arena.reset();
+        st = run_wave(ctx, w, 0, mode, nullptr, 0);
+        if (st != GEM_OK) break;
+        uint32_t timeouts = 0;
+        for (size_t i = 0; i < w.q.size(); ++i) timeouts += w.out[i].pad[0] ? 1 : 0;
+        const double cost = w.join_ms + (double)timeouts * ctx->opts.time_cap_ms;
+        if (cost < best_cost) {
+          best_cost = cost;
+          best.blocks_per_sm = bps;
+          best.donate_max_level = dm;
+          best.best_ms = (float)cost;
+        }
+      }
+    ctx->tune[b] = best;
+  }
+  ctx->opts.time_cap_ms = saved_cap;
+  if (report)
+    for (uint32_t b = 0; b < 6; ++b) {
+      report[3 * b] = ctx->tune[b].blocks_per_sm;
+      report[3 * b + 1] = ctx->tune[b].donate_max_level;
+      report[3 * b + 2] = (uint32_t)(ctx->tune[b].best_ms * 1000.0f);
+    }
+  return st;
 }

@@ -80,6 +80,17 @@ struct Wave {
   uint32_t launches = 0;
 };
 
+// Join schedule for one query-size bucket (0 = library default).
+struct Tune {
+  uint32_t blocks_per_sm = 0;
+  uint32_t donate_max_level = 0;
+  float best_ms = 0;
+};
+// Buckets by query size: <=4, <=8, <=12, <=16, <=24, <=32 vertices.
+inline uint32_t size_bucket(uint32_t nv) {
+  return nv <= 4 ? 0 : nv <= 8 ? 1 : nv <= 12 ? 2 : nv <= 16 ? 3 : nv <= 24 ? 4 : 5;
+}
+
 struct gem_ctx {
   gem_opts opts{};
   cudaStream_t s = nullptr;
@@ -103,6 +114,9 @@ struct gem_ctx {
   gem::JTask *d_queue = nullptr;
   uint32_t *d_err = nullptr;
   void *h_small = nullptr;
+  // join schedule: CUDA graph and per-size-bucket tuning (gem_autotune)
+  gem::JoinGraph jgraph;
+  Tune tune[6];
   // tunables
   uint32_t donate_max_level = 30;
   bool closed_form_suffix = true;

@@ -14,7 +14,8 @@ enum : uint32_t {
   DERR_NONE = 0,
   DERR_TIMEOUT = 1,   // a bounded wait or the time cap ran out
   DERR_OVERFLOW = 2,  // a fixed-capacity structure (cuckoo stash, output) overflowed
-  DERR_INTERNAL = 3   // an index or invariant check failed
+  DERR_INTERNAL = 3,  // an index or invariant check failed
+  DERR_BOUNDS = 4     // a bounds check failed; the kernel skipped the access
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }

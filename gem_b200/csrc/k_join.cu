@@ -18,16 +18,18 @@
 //    label only (the reference's dup_check_type, join_trie.cu:450-462);
 //  * the state of level L lives in lane L's registers (levels <= 32), so a
 //    warp's whole DFS stack costs a few registers per lane and no memory;
-//  * the last level is never materialised; in count mode the planner's
-//    closed-form suffix (an independent set of query vertices, e.g. the leaves
-//    of a tree) is counted by inclusion-exclusion per prefix match, and a
-//    suffix list with a single backward neighbour costs
-//    O(#same-label prefix levels) binary searches instead of a scan;
+//  * count mode: the planner's closed-form suffix (an independent set of
+//    query vertices, e.g. the leaves of a tree) is counted by
+//    inclusion-exclusion instead of being enumerated, one candidate of the
+//    last enumerated level per lane (32 prefix matches in flight per warp);
 //  * one persistent grid serves every query of a wave: warps take root
 //    candidates from a global counter and, once roots run out, receive work
 //    donated by busy warps (half of the unread candidates of a shallow
 //    level) through a bounded lock-free queue.  Every wait is bounded by the
-//    device deadline; an expired deadline sets a TIMEOUT status.
+//    device deadline; an expired deadline sets a TIMEOUT status;
+//  * every indexed access is bounds-checked against the wave's sizes; a
+//    failed check records (site, value, limit) in the control block, skips
+//    the access and stops the grid.
 #include "device_common.cuh"
 #include "index_device.cuh"
 #include "kernels.h"
@@ -51,134 +53,73 @@ struct Stats {
   uint64_t nodes = 0, scanned = 0, probes = 0;
 };
 
-// Per back entry i (lane i < nback): the list T(u_j -> u_lvl)[idx_j] as the
-// absolute range [lo, hi) of the values array.  Returns the shortest entry
-// (lowest index on ties) and its range, identical in every lane.
-__device__ __forceinline__ void level_lists(const JLevel *__restrict__ L, const JBack *__restrict__ backs,
-                                            const LaneState &c, uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi,
-                                            uint32_t &src, uint64_t &s_lo, uint64_t &s_hi) {
+// Bounds-check sites (reported through JControl::bad_site).
+enum : uint32_t {
+  SITE_BACK = 1,     // back-entry index
+  SITE_KEY = 2,      // table key (position of the key vertex)
+  SITE_RANGE = 3,    // table range outside the values array
+  SITE_VERTEX = 4,   // data vertex id of an index probe
+  SITE_QUERY = 5,    // query index of a task
+  SITE_LEVEL = 6,    // level of a task or of a descent
+  SITE_ROOT = 7,     // root position
+  SITE_TERM = 8,     // inclusion-exclusion term index
+  SITE_KEYLVL = 9    // key level after the probing level
+};
+
+__device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
+  return *reinterpret_cast<const volatile unsigned long long *>(p);
+}
+__device__ __forceinline__ unsigned int ld_vol(const unsigned int *p) {
+  return *reinterpret_cast<const volatile unsigned int *>(p);
+}
+
+// True when idx < lim; otherwise records the first violation and stops the grid.
+__device__ __forceinline__ bool inb(const JoinArgs &a, uint32_t site, uint64_t idx, uint64_t lim) {
+  if (idx < lim) return true;
+  if (atomicCAS(&a.ctl->err, DERR_NONE, DERR_BOUNDS) == DERR_NONE) {
+    a.ctl->bad_site = site;
+    a.ctl->bad_value = idx;
+    a.ctl->bad_limit = lim;
+  }
+  return false;
+}
+
+// Range [lo, hi) of table entry b at key position kidx (checked).
+__device__ __forceinline__ void table_range(const JoinArgs &a, const JBack *b, uint32_t kidx, uint64_t &lo,
+                                            uint64_t &hi) {
+  lo = hi = 0;
+  if (!inb(a, SITE_KEY, kidx, b->nkeys)) return;
+  const uint64_t l = __ldg(b->off + kidx), h = __ldg(b->off + kidx + 1);
+  if (!inb(a, SITE_RANGE, h, a.n_values + 1) || !inb(a, SITE_RANGE, l, h + 1)) return;
+  lo = l;
+  hi = h;
+}
+
+// Per back entry i (lane i < nback): the list T(u_j -> u_L)[idx_j] as the
+// absolute range [lo, hi) of the values array.
+__device__ __forceinline__ void level_ranges(const JoinArgs &a, const JLevel *__restrict__ L, const LaneState &c,
+                                             uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi) {
   const uint32_t lane = lane_id();
   nback = L->nback;
   uint32_t klvl = 0;
-  const uint64_t *off = nullptr;
-  if (lane < nback) {
-    const JBack *b = backs + L->back_base + lane;
-    klvl = b->lvl;
-    off = b->off;
+  const JBack *b = nullptr;
+  if (lane < nback && inb(a, SITE_BACK, (uint64_t)L->back_base + lane, a.n_backs)) {
+    b = a.backs + L->back_base + lane;
+    klvl = b->lvl & 31u;
   }
   const uint32_t kidx = __shfl_sync(FULL, c.idx, klvl);
-  my_lo = 0;
-  my_hi = 0;
-  if (lane < nback) {
-    my_lo = __ldg(off + kidx);
-    my_hi = __ldg(off + kidx + 1);
-  }
+  my_lo = my_hi = 0;
+  if (b) table_range(a, b, kidx, my_lo, my_hi);
+}
+
+// level_ranges plus the shortest entry (lowest index on ties) and its range,
+// identical in every lane.
+__device__ __forceinline__ void level_lists(const JoinArgs &a, const JLevel *__restrict__ L, const LaneState &c,
+                                            uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi, uint32_t &src,
+                                            uint64_t &s_lo, uint64_t &s_hi) {
+  const uint32_t lane = lane_id();
+  level_ranges(a, L, c, nback, my_lo, my_hi);
   uint64_t best = lane < nback ? my_hi - my_lo : ~0ull;
-  uint32_t bl = lane;
-#pragma unroll
-  for (int d = 16; d; d >>= 1) {
-    uint64_t ob = __shfl_xor_sync(FULL, best, d);
-    uint32_t ol = __shfl_xor_sync(FULL, bl, d);
-    if (ob < best || (ob == best && ol < bl)) {
-      best = ob;
-      bl = ol;
-    }
-  }
-  src = bl;
-  s_lo = __shfl_sync(FULL, my_lo, src);
-  s_hi = __shfl_sync(FULL, my_hi, src);
-}
-
-// Ranges of every back entry (lane i holds entry i), for a level whose
-// source entry is already known.
-__device__ __forceinline__ void level_ranges(const JLevel *__restrict__ L, const JBack *__restrict__ backs,
-                                             const LaneState &c, uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi) {
-  const uint32_t lane = lane_id();
-  nback = L->nback;
-  uint32_t klvl = 0;
-  const uint64_t *off = nullptr;
-  if (lane < nback) {
-    const JBack *b = backs + L->back_base + lane;
-    klvl = b->lvl;
-    off = b->off;
-  }
-  const uint32_t kidx = __shfl_sync(FULL, c.idx, klvl);
-  my_lo = 0;
-  my_hi = 0;
-  if (lane < nback) {
-    my_lo = __ldg(off + kidx);
-    my_hi = __ldg(off + kidx + 1);
-  }
-}
-
-// Evaluates the chunk [cpos, min(cpos + 32, end)) of the source list: a lane's
-// candidate survives if every other backward list contains it and no earlier
-// same-label level holds it.  Returns the ballot; *w receives the lane's value.
-__device__ __forceinline__ uint32_t eval_chunk(const uint32_t *__restrict__ values, uint64_t cpos, uint64_t end,
-                                               uint32_t nback, uint32_t src, uint64_t my_lo, uint64_t my_hi,
-                                               uint32_t dup_mask, const LaneState &c, uint32_t *w_out, Stats &st) {
-  const uint32_t lane = lane_id();
-  const uint64_t e = cpos + lane;
-  bool ok = e < end;
-  uint32_t w = ok ? __ldg(values + e) : 0u;
-  for (uint32_t i = 0; i < nback; ++i) {
-    const uint64_t lo = __shfl_sync(FULL, my_lo, i), hi = __shfl_sync(FULL, my_hi, i);
-    if (i == src) continue;
-    if (ok) ok = contains_u32(values, lo, hi, w);
-  }
-  uint32_t dm = dup_mask;
-  while (dm) {
-    const uint32_t j = __ffs(dm) - 1;
-    dm &= dm - 1;
-    const uint32_t fj = __shfl_sync(FULL, c.f, j);
-    if (w == fj) ok = false;
-  }
-  if (lane == 0) {
-    st.scanned += (end - cpos) < 32 ? (end - cpos) : 32;
-    st.probes += (uint64_t)(nback - 1) * ((end - cpos) < 32 ? (end - cpos) : 32);
-  }
-  *w_out = w;
-  return __ballot_sync(FULL, ok);
-}
-
-// Count mode, closed-form suffix.  The suffix levels form an independent set
-// of the query graph, so once the prefix is matched each suffix level's
-// candidates are fixed: A_i = intersection of its backward lists minus the
-// prefix vertices of its label.  Levels of different labels have disjoint
-// candidates; within a label group the number of injective assignments is
-// sum over set partitions pi of the group of
-//   prod_{B in pi} (-1)^{|B|-1} (|B|-1)! * |intersection_{i in B} A_i|
-// (inclusion-exclusion over coincidences).  All arithmetic wraps mod 2^64,
-// which is exact whenever the count itself fits in 64 bits.
-
-// |{x in A_i for every level i of `members`}| for the group starting at
-// level `first`; lists are spread one per lane (the planner keeps their
-// number <= 32).
-__device__ __forceinline__ uint64_t subset_count(const JQuery *__restrict__ Q, const JBack *__restrict__ backs,
-                                                 const uint32_t *__restrict__ values, const LaneState &c,
-                                                 uint32_t first, uint32_t members, uint32_t dup_mask, Stats &st) {
-  const uint32_t lane = lane_id();
-  uint32_t nl = 0;
-  uint64_t my_lo = 0, my_hi = 0;
-  for (uint32_t m = members; m; m &= m - 1) {
-    const JLevel *__restrict__ L = &Q->lv[first + __ffs(m) - 1];
-    const uint32_t nb = L->nback;
-    const bool mine = lane >= nl && lane < nl + nb;
-    uint32_t klvl = 0;
-    const uint64_t *off = nullptr;
-    if (mine) {
-      const JBack *b = backs + L->back_base + (lane - nl);
-      klvl = b->lvl;
-      off = b->off;
-    }
-    const uint32_t kidx = __shfl_sync(FULL, c.idx, klvl);
-    if (mine) {
-      my_lo = __ldg(off + kidx);
-      my_hi = __ldg(off + kidx + 1);
-    }
-    nl += nb;
-  }
-  uint64_t best = lane < nl ? my_hi - my_lo : ~0ull;
   uint32_t bl = lane;
 #pragma unroll
   for (int d = 16; d; d >>= 1) {
@@ -189,106 +130,98 @@ __device__ __forceinline__ uint64_t subset_count(const JQuery *__restrict__ Q, c
       bl = ol;
     }
   }
-  const uint32_t src = bl;
-  const uint64_t s_lo = __shfl_sync(FULL, my_lo, src), s_hi = __shfl_sync(FULL, my_hi, src);
-  if (nl == 1) {
-    bool hit = false;
-    if ((dup_mask >> lane) & 1u) hit = contains_u32(values, s_lo, s_hi, c.f);
-    if (lane == 0) st.probes += __popc(dup_mask);
-    return (s_hi - s_lo) - (uint64_t)__popc(__ballot_sync(FULL, hit));
-  }
-  uint64_t cnt = 0;
-  for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
-    uint32_t w;
-    cnt += __popc(eval_chunk(values, cp, s_hi, nl, src, my_lo, my_hi, dup_mask, c, &w, st));
-  }
-  return cnt;
+  src = bl;
+  s_lo = __shfl_sync(FULL, my_lo, src);
+  s_hi = __shfl_sync(FULL, my_hi, src);
 }
 
-__device__ __noinline__ uint64_t suffix_count(const JQuery *__restrict__ Q, const JBack *__restrict__ backs,
-                                              const uint32_t *__restrict__ values, const uint64_t *__restrict__ terms,
-                                              const LaneState &c, Stats &st) {
-  uint64_t total = 1;
-  const uint32_t ng = Q->n_groups;
-  for (uint32_t g = 0; g < ng && total; ++g) {
-    const uint32_t first = Q->grp_first[g], gs = Q->grp_size[g];
-    const uint32_t dup_mask = Q->lv[first].dup_mask;
-    if (gs == 1) {
-      total *= subset_count(Q, backs, values, c, first, 1u, dup_mask, st);
-      continue;
-    }
-    uint64_t sv[1u << MAX_GROUP];
-    bool empty = false;
-    for (uint32_t S = 1; S < (1u << gs); ++S) {
-      sv[S] = subset_count(Q, backs, values, c, first, S, dup_mask, st);
-      if (sv[S] == 0 && __popc(S) == 1) {
-        empty = true;
-        break;
-      }
-    }
-    if (empty) {
-      total = 0;
-      break;
-    }
-    uint64_t G = 0;
-    const uint32_t tb = Q->term_base[g], tc = Q->term_count[g];
-    for (uint32_t t = 0; t < tc; ++t) {
-      const uint64_t term = __ldg(terms + tb + t);
-      uint64_t prod = (uint64_t)(int64_t)(int32_t)(uint32_t)(term >> 32);
-      const uint32_t blocks = (uint32_t)term;
-#pragma unroll
-      for (uint32_t b = 0; b < MAX_GROUP; ++b) {
-        const uint32_t mk = (blocks >> (4 * b)) & 15u;
-        if (!mk) break;
-        prod *= sv[mk];
-      }
-      G += prod;
-    }
-    total *= G;
+// Evaluates the chunk [cpos, min(cpos + 32, end)) of the source list: a lane's
+// candidate survives if every other backward list contains it and no earlier
+// same-label level holds it.  Returns the ballot; *w receives the lane's value.
+__device__ __forceinline__ uint32_t eval_chunk(const JoinArgs &a, uint64_t cpos, uint64_t end, uint32_t nback,
+                                               uint32_t src, uint64_t my_lo, uint64_t my_hi, uint32_t dup_mask,
+                                               const LaneState &c, uint32_t *w_out, Stats &st) {
+  const uint32_t lane = lane_id();
+  const uint64_t e = cpos + lane;
+  bool ok = e < end;
+  uint32_t w = ok ? __ldg(a.values + e) : 0u;
+  for (uint32_t i = 0; i < nback; ++i) {
+    const uint64_t lo = __shfl_sync(FULL, my_lo, i), hi = __shfl_sync(FULL, my_hi, i);
+    if (i == src) continue;
+    if (ok) ok = contains_u32(a.values, lo, hi, w);
   }
-  return total;
+  for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
+    const uint32_t j = __ffs(dm) - 1;
+    const uint32_t fj = __shfl_sync(FULL, c.f, j);
+    if (w == fj) ok = false;
+  }
+  if (lane == 0) {
+    const uint64_t k = (end - cpos) < 32 ? (end - cpos) : 32;
+    st.scanned += k;
+    st.probes += (uint64_t)(nback - 1) * k;
+  }
+  *w_out = w;
+  return __ballot_sync(FULL, ok);
 }
 
-// Lane-parallel form of the suffix count used at the last enumerated level:
-// every lane owns one candidate w of level L = n_enum - 1 (position widx in
-// C(u_L)); the earlier levels' vertices and positions come from the warp's
-// shared copy (sf, sidx).  Lists are addressed by index through the members'
-// backward entries, so no per-lane arrays are needed.
+__device__ __forceinline__ uint32_t index_of(const JoinArgs &a, const JLevel *__restrict__ L, uint32_t w) {
+  const uint32_t kind = L->idx_kind;
+  if (kind == IDX_NONE) return 0u;
+  if (!inb(a, SITE_VERTEX, w, a.nv)) return 0xFFFFFFFFu;
+  if (kind == IDX_RANK) return rank_lookup(L->rb, w);
+  return ck_lookup(L->ck, w);
+}
+
+// ---------------------------------------------------------------------------
+// Count mode, closed-form suffix.  The suffix levels form an independent set
+// of the query graph, so once the prefix is matched each suffix level's
+// candidates are fixed: A_i = intersection of its backward lists minus the
+// prefix vertices of its label.  Levels of different labels have disjoint
+// candidates; within a label group the number of injective assignments is
+// sum over set partitions pi of the group of
+//   prod_{B in pi} (-1)^{|B|-1} (|B|-1)! * |intersection_{i in B} A_i|
+// (inclusion-exclusion over coincidences).  All arithmetic wraps mod 2^64,
+// which is exact whenever the count itself fits in 64 bits.
+//
+// Every lane owns one candidate w of the last enumerated level L (position
+// widx in C(u_L)); the earlier levels' vertices and positions come from the
+// warp's shared copy (sf, sidx).  Lists are addressed by index through the
+// members' backward entries, so no per-lane arrays are needed.
+// ---------------------------------------------------------------------------
 struct LaneCtx {
   const JQuery *Q;
-  const JBack *backs;
-  const uint32_t *values;
   uint32_t L, w, widx;
   const uint32_t *sf, *sidx;
 };
 
-__device__ __forceinline__ void lane_list(const LaneCtx &x, uint32_t first, uint32_t members, uint32_t li,
-                                          uint64_t &lo, uint64_t &hi) {
+__device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
+                                          uint32_t li, uint64_t &lo, uint64_t &hi) {
+  lo = hi = 0;
   for (uint32_t m = members; m; m &= m - 1) {
-    const JLevel *M = &x.Q->lv[first + __ffs(m) - 1];
+    const JLevel *M = &x.Q->lv[(first + __ffs(m) - 1) & 31u];
     const uint32_t nb = M->nback;
     if (li < nb) {
-      const JBack *b = x.backs + M->back_base + li;
+      if (!inb(a, SITE_BACK, (uint64_t)M->back_base + li, a.n_backs)) return;
+      const JBack *b = a.backs + M->back_base + li;
       const uint32_t kl = b->lvl;
+      if (!inb(a, SITE_KEYLVL, kl, (uint64_t)x.L + 1)) return;
       const uint32_t kidx = kl == x.L ? x.widx : x.sidx[kl];
-      lo = __ldg(b->off + kidx);
-      hi = __ldg(b->off + kidx + 1);
+      table_range(a, b, kidx, lo, hi);
       return;
     }
     li -= nb;
   }
-  lo = hi = 0;
 }
 
-__device__ uint64_t lane_subset_count(const LaneCtx &x, uint32_t first, uint32_t members, uint32_t dup_mask,
-                                      Stats &st) {
+__device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
+                                      uint32_t dup_mask, Stats &st) {
   uint32_t nl = 0;
-  for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[first + __ffs(m) - 1].nback;
+  for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[(first + __ffs(m) - 1) & 31u].nback;
   uint32_t s = 0;
   uint64_t s_lo = 0, s_hi = 0;
   for (uint32_t i = 0; i < nl; ++i) {
     uint64_t lo, hi;
-    lane_list(x, first, members, i, lo, hi);
+    lane_list(a, x, first, members, i, lo, hi);
     if (i == 0 || hi - lo < s_hi - s_lo) {
       s = i;
       s_lo = lo;
@@ -300,14 +233,14 @@ __device__ uint64_t lane_subset_count(const LaneCtx &x, uint32_t first, uint32_t
     for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
       const uint32_t v = j == x.L ? x.w : x.sf[j];
-      if (contains_u32(x.values, s_lo, s_hi, v)) --c;
+      if (contains_u32(a.values, s_lo, s_hi, v)) --c;
     }
     st.probes += __popc(dup_mask);
     return c;
   }
   uint64_t c = 0;
   for (uint64_t e = s_lo; e < s_hi; ++e) {
-    const uint32_t v = __ldg(x.values + e);
+    const uint32_t v = __ldg(a.values + e);
     bool ok = true;
     for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
@@ -316,8 +249,8 @@ __device__ uint64_t lane_subset_count(const LaneCtx &x, uint32_t first, uint32_t
     for (uint32_t i = 0; i < nl && ok; ++i) {
       if (i == s) continue;
       uint64_t lo, hi;
-      lane_list(x, first, members, i, lo, hi);
-      ok = contains_u32(x.values, lo, hi, v);
+      lane_list(a, x, first, members, i, lo, hi);
+      ok = contains_u32(a.values, lo, hi, v);
     }
     c += ok;
   }
@@ -326,31 +259,29 @@ __device__ uint64_t lane_subset_count(const LaneCtx &x, uint32_t first, uint32_t
   return c;
 }
 
-__device__ uint64_t lane_suffix_count(const LaneCtx &x, const uint64_t *__restrict__ terms, Stats &st) {
+__device__ uint64_t lane_suffix_count(const JoinArgs &a, const LaneCtx &x, Stats &st) {
   const JQuery *Q = x.Q;
   uint64_t total = 1;
-  const uint32_t ng = Q->n_groups;
+  const uint32_t ng = Q->n_groups < MAX_GROUPS ? Q->n_groups : MAX_GROUPS;
   for (uint32_t g = 0; g < ng && total; ++g) {
-    const uint32_t first = Q->grp_first[g], gs = Q->grp_size[g];
-    const uint32_t dup_mask = Q->lv[first].dup_mask;
+    const uint32_t first = Q->grp_first[g];
+    const uint32_t gs = Q->grp_size[g] < MAX_GROUP ? Q->grp_size[g] : MAX_GROUP;
+    const uint32_t dup_mask = Q->lv[first & 31u].dup_mask;
     if (gs == 1) {
-      total *= lane_subset_count(x, first, 1u, dup_mask, st);
+      total *= lane_subset_count(a, x, first, 1u, dup_mask, st);
       continue;
     }
     uint64_t sv[1u << MAX_GROUP];
-    bool empty = false;
+    for (uint32_t S = 0; S < (1u << MAX_GROUP); ++S) sv[S] = 0;
     for (uint32_t S = 1; S < (1u << gs); ++S) {
-      sv[S] = lane_subset_count(x, first, S, dup_mask, st);
-      if (sv[S] == 0 && __popc(S) == 1) {
-        empty = true;
-        break;
-      }
+      sv[S] = lane_subset_count(a, x, first, S, dup_mask, st);
+      if (sv[S] == 0 && __popc(S) == 1) return 0;
     }
-    if (empty) return 0;
     uint64_t G = 0;
     const uint32_t tb = Q->term_base[g], tc = Q->term_count[g];
     for (uint32_t t = 0; t < tc; ++t) {
-      const uint64_t term = __ldg(terms + tb + t);
+      if (!inb(a, SITE_TERM, (uint64_t)tb + t, a.n_terms)) return 0;
+      const uint64_t term = __ldg(a.terms + tb + t);
       uint64_t prod = (uint64_t)(int64_t)(int32_t)(uint32_t)(term >> 32);
       const uint32_t blocks = (uint32_t)term;
       for (uint32_t b = 0; b < MAX_GROUP; ++b) {
@@ -365,15 +296,10 @@ __device__ uint64_t lane_suffix_count(const LaneCtx &x, const uint64_t *__restri
   return total;
 }
 
-__device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
-  return *reinterpret_cast<const volatile unsigned long long *>(p);
-}
-__device__ __forceinline__ unsigned int ld_vol(const unsigned int *p) {
-  return *reinterpret_cast<const volatile unsigned int *>(p);
-}
-
+// ---------------------------------------------------------------------------
 // Bounded MPMC queue (sequence-numbered cells).  Called by a whole warp;
 // lane 0 reserves, every lane writes its share, lane 0 publishes.
+// ---------------------------------------------------------------------------
 __device__ bool queue_push(JControl *ctl, JTask *cells, uint32_t q, uint32_t lvl, uint32_t src, uint64_t begin,
                            uint64_t end, uint64_t hs, const LaneState &c) {
   const uint32_t lane = lane_id();
@@ -461,7 +387,7 @@ __device__ bool queue_pop(JControl *ctl, JTask *cells, PoppedTask &t, LaneState 
   t.begin = __ldcg(reinterpret_cast<const unsigned long long *>(&cell->begin));
   t.end = __ldcg(reinterpret_cast<const unsigned long long *>(&cell->end));
   t.hs = __ldcg(reinterpret_cast<const unsigned long long *>(&cell->hs));
-  if (lane < t.lvl) {
+  if (lane < t.lvl && lane < QV) {
     c.f = __ldcg(&cell->f[lane]);
     c.idx = __ldcg(&cell->idx[lane]);
   }
@@ -483,17 +409,10 @@ __device__ __forceinline__ uint32_t find_query(const uint64_t *__restrict__ rp, 
 // Marks query q incomplete and, once, withdraws every unclaimed root so the
 // grid drains quickly; the queries owning withdrawn roots are marked too.
 __device__ void abandon(const JoinArgs &a, uint32_t q) {
-  atomicOr(&a.out[q].pad[0], 1ull);
+  if (q < a.nquery) atomicOr(&a.out[q].pad[0], 1ull);
   const unsigned long long r0 = atomicExch(&a.ctl->root_next, (unsigned long long)a.n_roots);
   if (r0 < a.n_roots)
     for (uint32_t k = find_query(a.root_prefix, a.nquery, r0); k < a.nquery; ++k) atomicOr(&a.out[k].pad[0], 1ull);
-}
-
-__device__ __forceinline__ uint32_t index_of(const JLevel *__restrict__ L, uint32_t w) {
-  const uint32_t kind = L->idx_kind;
-  if (kind == IDX_RANK) return rank_lookup(L->rb, w);
-  if (kind == IDX_CUCKOO) return ck_lookup(L->ck, w);
-  return 0u;
 }
 
 template <uint32_t MODE>
@@ -525,8 +444,6 @@ template <uint32_t MODE>
 __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
   const uint32_t lane = lane_id();
   JControl *ctl = a.ctl;
-  const uint32_t *__restrict__ values = a.values;
-  const JBack *__restrict__ backs = a.backs;
   const uint64_t deadline = ctl->deadline_ns;
   __shared__ uint32_t s_pref[8][2][QV];  // per warp: f and idx of the enumerated prefix
   uint32_t *sf = s_pref[threadIdx.x >> 5][0], *sidx = s_pref[threadIdx.x >> 5][1];
@@ -566,31 +483,33 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
       if (r < a.lp_roots) {
         const uint32_t k = find_query(a.lp_prefix, a.lp_nq, r);
         const uint32_t q = a.lp_query[k];
-        const JQuery *Q = a.queries + q;
-        const uint32_t rl = (uint32_t)(r - __ldg(a.lp_prefix + k));
-        const uint32_t w0 = __ldg(Q->root_cand + rl);
-        uint64_t cnt = 0, h = 0;
-        if (Q->n == 1) {
-          cnt = 1;
-          if (MODE != MODE_COUNT) h = mix64(emb_term(Q->root_u, w0));
-          if (MODE == MODE_ENUM) {
-            const unsigned long long s = atomicAdd(&ctl->emb_next, 1ull);
-            if (s < a.emb_cap) a.emb[s] = w0;
+        if (inb(a, SITE_QUERY, q, a.nquery)) {
+          const JQuery *Q = a.queries + q;
+          const uint64_t rl = r - __ldg(a.lp_prefix + k);
+          if (inb(a, SITE_ROOT, rl, Q->n_root)) {
+            const uint32_t w0 = __ldg(Q->root_cand + rl);
+            uint64_t cnt = 0, h = 0;
+            if (Q->n == 1) {
+              cnt = 1;
+              if (MODE != MODE_COUNT) h = mix64(emb_term(Q->root_u, w0));
+              if (MODE == MODE_ENUM) {
+                const unsigned long long s = atomicAdd(&ctl->emb_next, 1ull);
+                if (s < a.emb_cap) a.emb[s] = w0;
+              }
+            } else {
+              LaneCtx x;
+              x.Q = Q;
+              x.L = 0;
+              x.w = w0;
+              x.widx = (uint32_t)rl;
+              x.sf = sf;
+              x.sidx = sidx;
+              cnt = lane_suffix_count(a, x, st);
+            }
+            if (cnt) atomicAdd(&a.out[q].count, (unsigned long long)cnt);
+            if (h) atomicAdd(&a.out[q].hash, (unsigned long long)h);
           }
-        } else {
-          LaneCtx x;
-          x.Q = Q;
-          x.backs = backs;
-          x.values = values;
-          x.L = 0;
-          x.w = w0;
-          x.widx = rl;
-          x.sf = sf;
-          x.sidx = sidx;
-          cnt = lane_suffix_count(x, a.terms, st);
         }
-        if (cnt) atomicAdd(&a.out[q].count, (unsigned long long)cnt);
-        if (h) atomicAdd(&a.out[q].hash, (unsigned long long)h);
       }
       if (lane == 0) st.nodes += (a.lp_roots - base) < 32 ? (a.lp_roots - base) : 32;
     }
@@ -610,7 +529,9 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         if (rr >= a.n_roots) atomicSub(&ctl->busy, 1u);
       }
       r = __shfl_sync(FULL, rr, 0);
-      if (r < a.n_roots && ld_vol(&ctl->err) != DERR_NONE) {
+      // warp-uniform: lane 0 reads the error word for the whole warp
+      const int err_set = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->err) != DERR_NONE) : 0, 0);
+      if (r < a.n_roots && err_set) {
         // past the deadline: this root is not processed
         if (lane == 0) {
           abandon(a, find_query(a.root_prefix, a.nquery, r));
@@ -640,15 +561,20 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
           idle_registered = false;  // a finished donated task re-registers as idle below
           q = t.q;
           lvl = base_lvl = t.lvl;
-          const uint64_t hsp = __shfl_sync(FULL, t.hs, 0);
-          if (lane == lvl - 1) c.hs = hsp;
-          if (lane == lvl) {
-            c.src = t.src;
-            c.pos = t.begin;
-            c.end = t.end;
-            c.mask = 0;
-          }
           have = true;
+          if (!inb(a, SITE_QUERY, q, a.nquery) || !inb(a, SITE_LEVEL, lvl, a.queries[q].n) || lvl == 0) {
+            lvl = 0;  // unusable task: nothing to run (a failed check stops the grid)
+            base_lvl = 1;
+            q = 0;
+          } else {
+            if (lane == lvl - 1) c.hs = t.hs;
+            if (lane == lvl) {
+              c.src = t.src;
+              c.pos = t.begin;
+              c.end = t.end;
+              c.mask = 0;
+            }
+          }
           break;
         }
         int leave = 0;
@@ -676,51 +602,35 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
 
     // ------------------------------------------------------------ set up
     uint64_t lane_cnt = 0, lane_hash = 0;
-    const JQuery *__restrict__ Q;
+    const JQuery *__restrict__ Q = a.queries + q;
     if (from_root) {
       q = find_query(a.root_prefix, a.nquery, r);
       Q = a.queries + q;
-      const uint32_t rl = (uint32_t)(r - Q->root_base);
-      const uint32_t w0 = __ldg(Q->root_cand + rl);
-      const uint64_t h0 = MODE == MODE_COUNT ? 0ull : emb_term(Q->root_u, w0);
-      if (lane == 0) {
-        c.f = w0;
-        c.idx = rl;
-        c.hs = h0;
-      }
-      const uint32_t n = Q->n;
-      if (n == 1) {
+      const uint64_t rl = r - Q->root_base;
+      lvl = 0;
+      base_lvl = 1;
+      if (inb(a, SITE_ROOT, rl, Q->n_root)) {
+        const uint32_t w0 = __ldg(Q->root_cand + rl);
+        const uint64_t h0 = MODE == MODE_COUNT ? 0ull : emb_term(Q->root_u, w0);
         if (lane == 0) {
-          lane_cnt = 1;
-          lane_hash = mix64(h0);
-          if (MODE == MODE_ENUM) {
-            unsigned long long s = atomicAdd(&ctl->emb_next, 1ull);
-            if (s < a.emb_cap) a.emb[s] = w0;
+          c.f = w0;
+          c.idx = (uint32_t)rl;
+          c.hs = h0;
+        }
+        st.nodes += lane == 0;
+        if (Q->n >= 2) {
+          uint32_t nb, src;
+          uint64_t lo, hi, s_lo, s_hi;
+          level_lists(a, &Q->lv[1], c, nb, lo, hi, src, s_lo, s_hi);
+          if (lane == 1) {
+            c.src = src;
+            c.pos = s_lo;
+            c.end = s_hi;
+            c.mask = 0;
           }
+          lvl = base_lvl = 1;
         }
-        lvl = 0;  // nothing to iterate
-        base_lvl = 1;
-      } else if (MODE == MODE_COUNT && Q->n_enum == 1) {
-        st.nodes += lane == 0;
-        const uint64_t k = suffix_count(Q, backs, values, a.terms, c, st);
-        if (lane == 0) lane_cnt += k;
-        lvl = 0;
-        base_lvl = 1;
-      } else {
-        st.nodes += lane == 0;
-        uint32_t nb, src;
-        uint64_t lo, hi, s_lo, s_hi;
-        level_lists(&Q->lv[1], backs, c, nb, lo, hi, src, s_lo, s_hi);
-        if (lane == 1) {
-          c.src = src;
-          c.pos = s_lo;
-          c.end = s_hi;
-          c.mask = 0;
-        }
-        lvl = base_lvl = 1;
       }
-    } else {
-      Q = a.queries + q;
     }
 
     // ------------------------------------------------------------ DFS
@@ -728,15 +638,15 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
     uint32_t iter = 0;
     bool abort = false;
     while (lvl >= base_lvl && lvl != 0) {
-      const JLevel *__restrict__ L = &Q->lv[lvl];
-      uint32_t mask = __shfl_sync(FULL, c.mask, lvl);
+      const JLevel *__restrict__ L = &Q->lv[lvl & 31u];
+      const uint32_t mask = __shfl_sync(FULL, c.mask, lvl);
       if (mask == 0) {
         const uint64_t pos = __shfl_sync(FULL, c.pos, lvl), end = __shfl_sync(FULL, c.end, lvl);
         if (pos >= end) {
           --lvl;
           continue;
         }
-        if ((++iter & 255u) == 0) {
+        if ((++iter & 63u) == 0) {
           int stop = 0;
           if (lane == 0) {
             if (ld_vol(&ctl->err) != DERR_NONE) stop = 1;
@@ -752,14 +662,27 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         }
         uint32_t nb;
         uint64_t lo, hi;
-        level_ranges(L, backs, c, nb, lo, hi);
+        level_ranges(a, L, c, nb, lo, hi);
         const uint32_t src = __shfl_sync(FULL, c.src, lvl);
         uint32_t w;
-        const uint32_t m = eval_chunk(values, pos, end, nb, src, lo, hi, L->dup_mask, c, &w, st);
+        const uint32_t m = eval_chunk(a, pos, end, nb, src, lo, hi, L->dup_mask, c, &w, st);
         if (MODE != MODE_COUNT && lvl == n - 1) {
           emit_last<MODE>(a, Q, lvl, m, w, c, lane_cnt, lane_hash);
           if (lane == lvl) c.pos = pos + 32;
-        } else if (MODE == MODE_COUNT && lvl + 1 == Q->n_enum) {
+          continue;
+        }
+        uint64_t new_end = end;
+        // warp-uniform: lane 0 reads the idle count for the whole warp
+        const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->idle) > 0) : 0, 0);
+        if (lvl <= a.donate_max_level && end > pos + 32 + 64 && idle_now) {
+          const uint64_t rem = pos + 32;
+          const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
+          if (mid < end) {
+            const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
+            if (queue_push(ctl, a.queue, q, lvl, src, mid, end, hsp, c)) new_end = mid;
+          }
+        }
+        if (MODE == MODE_COUNT && lvl + 1 >= Q->n_enum) {
           // last enumerated level: each lane counts its own candidate's
           // suffix completions (32 prefix matches in flight per warp)
           if (lane < lvl) {
@@ -770,43 +693,24 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
           if ((m >> lane) & 1u) {
             LaneCtx x;
             x.Q = Q;
-            x.backs = backs;
-            x.values = values;
             x.L = lvl;
             x.w = w;
-            x.widx = index_of(L, w);
+            x.widx = index_of(a, L, w);
             x.sf = sf;
             x.sidx = sidx;
-            lane_cnt += lane_suffix_count(x, a.terms, st);
+            lane_cnt += lane_suffix_count(a, x, st);
           }
           __syncwarp();
           if (lane == 0) st.nodes += __popc(m);
-          uint64_t new_end = end;
-          if (lvl <= a.donate_max_level && end > pos + 32 + 64 && ld_vol(&ctl->idle) > 0) {
-            const uint64_t rem = pos + 32;
-            const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
-            if (mid < end && queue_push(ctl, a.queue, q, lvl, src, mid, end, 0ull, c)) new_end = mid;
-          }
           if (lane == lvl) {
             c.pos = pos + 32;
             c.end = new_end;
           }
-        } else {
-          uint64_t new_end = end;
-          if (lvl <= a.donate_max_level && end > pos + 32 + 64 && ld_vol(&ctl->idle) > 0) {
-            const uint64_t rem = pos + 32;
-            const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
-            if (mid < end) {
-              const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
-              if (queue_push(ctl, a.queue, q, lvl, src, mid, end, hsp, c)) new_end = mid;
-            }
-          }
-          if (lane == lvl) {
-            c.cbase = pos;
-            c.pos = pos + 32;
-            c.mask = m;
-            c.end = new_end;
-          }
+        } else if (lane == lvl) {
+          c.cbase = pos;
+          c.pos = pos + 32;
+          c.mask = m;
+          c.end = new_end;
         }
         continue;
       }
@@ -814,8 +718,8 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
       const uint32_t b = __ffs(mask) - 1;
       const uint64_t cb = __shfl_sync(FULL, c.cbase, lvl);
       if (lane == lvl) c.mask = mask & (mask - 1);
-      const uint32_t w = __ldg(values + cb + b);
-      const uint32_t widx = index_of(L, w);
+      const uint32_t w = __ldg(a.values + cb + b);
+      const uint32_t widx = index_of(a, L, w);
       const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
       if (lane == lvl) {
         c.f = w;
@@ -827,14 +731,13 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         st.probes += L->idx_kind != IDX_NONE;
       }
       const uint32_t nxt = lvl + 1;
-      if (MODE == MODE_COUNT && nxt == Q->n_enum) {
-        const uint64_t k = suffix_count(Q, backs, values, a.terms, c, st);
-        if (lane == 0) lane_cnt += k;
-        continue;
+      if (!inb(a, SITE_LEVEL, nxt, n)) {
+        abort = true;
+        break;
       }
       uint32_t nb, src;
       uint64_t lo, hi, s_lo, s_hi;
-      level_lists(&Q->lv[nxt], backs, c, nb, lo, hi, src, s_lo, s_hi);
+      level_lists(a, &Q->lv[nxt], c, nb, lo, hi, src, s_lo, s_hi);
       if (lane == nxt) {
         c.src = src;
         c.pos = s_lo;
@@ -871,14 +774,20 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
   }
 }
 
-__global__ void queue_init_kernel(JTask *cells) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < TASK_CAP; i += gridDim.x * blockDim.x)
-    cells[i].seq = i;
-}
-
-void join_queue_init(JTask *queue, cudaStream_t s) {
-  count_launch();
-  queue_init_kernel<<<32, 256, 0, s>>>(queue);
+// Zeroes the control block and the per-query outputs, resets the task queue
+// and sets the deadline; runs right before the join in the same graph.
+__global__ void join_prepare_kernel(JControl *ctl, JOut *out, uint32_t nquery, JTask *cells, uint64_t cap_ns) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  for (uint32_t i = t; i < TASK_CAP; i += nt) cells[i].seq = i;
+  unsigned long long *o = reinterpret_cast<unsigned long long *>(out);
+  const uint32_t words = nquery * (uint32_t)(sizeof(JOut) / 8);
+  for (uint32_t i = t; i < words; i += nt) o[i] = 0ull;
+  if (t == 0) {
+    JControl z;
+    memset(&z, 0, sizeof z);
+    z.deadline_ns = globaltimer_ns() + cap_ns;
+    *ctl = z;
+  }
 }
 
 int join_blocks_per_sm(uint32_t mode) {
@@ -891,16 +800,52 @@ int join_blocks_per_sm(uint32_t mode) {
   return n;
 }
 
-uint32_t launch_join(const JoinArgs &a, int blocks_per_sm, cudaStream_t s) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const uint32_t grid = (uint32_t)(sms * (blocks_per_sm > 0 ? blocks_per_sm : 1));
-  count_launch();
-  if (a.mode == MODE_COUNT) join_kernel<MODE_COUNT><<<grid, 256, 0, s>>>(a);
-  else if (a.mode == MODE_HASH) join_kernel<MODE_HASH><<<grid, 256, 0, s>>>(a);
-  else join_kernel<MODE_ENUM><<<grid, 256, 0, s>>>(a);
-  return grid;
+static void *join_fn(uint32_t mode) {
+  if (mode == MODE_COUNT) return (void *)join_kernel<MODE_COUNT>;
+  if (mode == MODE_HASH) return (void *)join_kernel<MODE_HASH>;
+  return (void *)join_kernel<MODE_ENUM>;
+}
+
+void destroy_join_graph(JoinGraph &jg) {
+  if (jg.exec) cudaGraphExecDestroy(jg.exec);
+  if (jg.graph) cudaGraphDestroy(jg.graph);
+  jg = JoinGraph();
+}
+
+cudaError_t launch_join_graph(JoinGraph &jg, const JoinArgs &a, uint64_t cap_ns, uint32_t grid, cudaStream_t s) {
+  JoinArgs args = a;
+  JControl *ctl = a.ctl;
+  JOut *out = a.out;
+  uint32_t nq = a.nquery;
+  JTask *cells = a.queue;
+  uint64_t cap = cap_ns;
+  void *prep_params[] = {&ctl, &out, &nq, &cells, &cap};
+  void *join_params[] = {&args};
+  cudaKernelNodeParams pp = {};
+  pp.func = (void *)join_prepare_kernel;
+  pp.gridDim = dim3(32);
+  pp.blockDim = dim3(256);
+  pp.kernelParams = prep_params;
+  cudaKernelNodeParams jp = {};
+  jp.func = join_fn(a.mode);
+  jp.gridDim = dim3(grid);
+  jp.blockDim = dim3(256);
+  jp.kernelParams = join_params;
+  cudaError_t e;
+  if (!jg.exec || jg.mode != a.mode || jg.grid != grid) {
+    destroy_join_graph(jg);
+    if ((e = cudaGraphCreate(&jg.graph, 0)) != cudaSuccess) return e;
+    if ((e = cudaGraphAddKernelNode(&jg.prep, jg.graph, nullptr, 0, &pp)) != cudaSuccess) return e;
+    if ((e = cudaGraphAddKernelNode(&jg.join, jg.graph, &jg.prep, 1, &jp)) != cudaSuccess) return e;
+    if ((e = cudaGraphInstantiate(&jg.exec, jg.graph, 0)) != cudaSuccess) return e;
+    jg.mode = a.mode;
+    jg.grid = grid;
+  } else {
+    if ((e = cudaGraphExecKernelNodeSetParams(jg.exec, jg.prep, &pp)) != cudaSuccess) return e;
+    if ((e = cudaGraphExecKernelNodeSetParams(jg.exec, jg.join, &jp)) != cudaSuccess) return e;
+  }
+  count_launch(2);
+  return cudaGraphLaunch(jg.exec, s);
 }
 
 }  // namespace gem

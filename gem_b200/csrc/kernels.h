@@ -161,7 +161,7 @@ struct JLevel {
 };
 struct JBack {
   uint32_t lvl;              // level of the key vertex
-  uint32_t pad;
+  uint32_t nkeys;            // keys of the table (offsets has nkeys + 1 entries)
   const uint64_t *off;       // table offsets (absolute into the values array)
 };
 constexpr uint32_t MAX_GROUPS = 16;   // label groups of a closed-form suffix
@@ -217,6 +217,9 @@ struct JControl {            // zeroed before every launch (except queue seq ini
   unsigned int pad;
   unsigned long long deadline_ns;
   unsigned long long emb_next;   // enumerate cursor
+  unsigned long long bad_site;   // first failed bounds check: site id
+  unsigned long long bad_value;  // ... the offending index
+  unsigned long long bad_limit;  // ... and its limit
 };
 enum : uint32_t { MODE_COUNT = 0, MODE_HASH = 1, MODE_ENUM = 2 };
 struct JoinArgs {
@@ -241,11 +244,24 @@ struct JoinArgs {
   uint32_t *emb;             // ENUM: output buffer
   uint64_t emb_cap;          // embeddings that fit
   uint32_t donate_max_level; // donate candidates of levels <= this
-  uint32_t pad;
+  uint32_t nv;               // data vertices (bounds of rank-bitmap probes)
+  uint64_t n_values;         // entries of `values`
+  uint32_t n_backs;          // entries of `backs`
+  uint32_t n_terms;          // entries of `terms`
 };
-void join_queue_init(JTask *queue, cudaStream_t s);
-// Launches the persistent join; returns the grid size used.
-uint32_t launch_join(const JoinArgs &a, int blocks_per_sm, cudaStream_t s);
+// The join of a wave as a CUDA graph: a prepare kernel (zero the control
+// block and the per-query outputs, reset the task queue, set the device
+// deadline) followed by the persistent join.  One executable graph is built
+// per (mode, grid) and reused; each wave only updates the two kernel nodes'
+// parameters before cudaGraphLaunch.
+struct JoinGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t prep = nullptr, join = nullptr;
+  uint32_t mode = 0, grid = 0;
+};
+cudaError_t launch_join_graph(JoinGraph &jg, const JoinArgs &a, uint64_t cap_ns, uint32_t grid, cudaStream_t s);
+void destroy_join_graph(JoinGraph &jg);
 int join_blocks_per_sm(uint32_t mode);
 
 }  // namespace gem

@@ -198,6 +198,16 @@ gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold,
 gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n,
                          int mode, gem_result *res);
 
+/* Autotuner (no counterpart in the reference): for each query-size bucket
+ * (<=4, <=8, <=12, <=16, <=24, <=32 vertices) present in qs, runs a sample of
+ * up to 8 of its queries under each candidate join schedule (blocks per SM of
+ * the persistent grid, deepest level that donates work), each trial capped at
+ * trial_cap_ms, and keeps the fastest for later waves of this context.
+ * report (optional, 18 entries): per bucket {blocks_per_sm,
+ * donate_max_level, best join time in us}; zeros for untuned buckets. */
+gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode,
+                        uint32_t trial_cap_ms, uint32_t *report);
+
 /* Embedding hash of one embedding f (f[u] = data vertex of query vertex u):
  * h = mix(sum_u mix(f[u] | u << 32)) with mix the splitmix64 finaliser of
  * (x + 0x9E3779B97F4A7C15); GEM_MODE_HASH reports the sum of h over all

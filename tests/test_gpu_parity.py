@@ -311,3 +311,18 @@ def test_out_of_core_same_counts(small):
         for q in qs:
             ra, rb = a.run(q, mode=gem.MODE_HASH), b.run(q, mode=gem.MODE_HASH)
             assert (ra["count"], ra["emb_hash"]) == (rb["count"], rb["emb_hash"])
+
+
+def test_autotune_keeps_results(small):
+    qs = []
+    for k in (3, 4, 6):
+        for q in gem.gen_queries(small, k, gem.ANY, 4, seed=7000 + k):
+            if oracle.count(small, q, want_hash=False, work_cap=100_000_000)[2]:
+                qs.append(q)
+    with gem.Context(time_cap_ms=30000) as c:
+        c.load_graph(small)
+        before = [c.run(q)["count"] for q in qs]
+        rep = c.autotune(qs, trial_cap_ms=5000)
+        assert rep and all(v[0] >= 1 and v[1] >= 1 for v in rep.values())
+        st, after = c.batch(qs)
+        assert st == 0 and [r["count"] for r in after] == before

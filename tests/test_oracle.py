@@ -81,3 +81,32 @@ def test_oracle_edge_table():
     off, vals = oracle.edge_table(g, np.array([0, 3], np.uint32), np.array([1, 2, 4], np.uint32))
     assert off.tolist() == [0, 2, 5]
     assert vals.tolist() == [1, 2, 1, 2, 4]
+
+
+REF_COUNTS = os.path.join(os.path.dirname(__file__), "golden", "ref_counts.json")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_COUNTS), reason="reference-binary fixture not generated")
+def test_oracle_matches_reference_binary():
+    """Counts printed by the reference's own in-core binary (uint32 print) on
+    seeded inputs equal the oracle's count mod 2^32."""
+    with open(REF_COUNTS) as f:
+        data = json.load(f)
+    graphs = {}
+    checked = 0
+    for c in data["cases"]:
+        if c["exit"] != 0 or len(c["printed"]) != 1:
+            continue
+        gd = c["graph"]
+        key = gd["name"]
+        if key not in graphs:
+            graphs[key] = gem.HostGraph.rmat(gd["scale"], gd["edge_factor"], seed=gd["seed"]).set_labels(
+                gd["labels"], gd["zipf_s"], seed=gd["seed"] ^ 0x4C)
+        q = gem.Query(c["labels"], c["edges"])
+        cnt, _, ok = oracle.count(graphs[key], q, want_hash=False, work_cap=2_000_000_000)
+        if not ok:
+            continue
+        assert cnt % (1 << 32) == c["printed"][0], (key, c["labels"], c["edges"], cnt, c["printed"])
+        assert c["et"][0] == "0" * (32 - len(c["edges"])) + "1" * len(c["edges"])
+        checked += 1
+    assert checked >= 10
