@@ -2,15 +2,21 @@
 """Benchmark: exact subgraph-matching throughput on one B200 (queries/s and
 embeddings/s, batched vs plain, p50/p99 latency).
 
-Workload (default `rmat22`): R-MAT scale 22 (4,194,304 vertices), edge
-factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), self loops and duplicates
-removed, uint32 CSR with sorted adjacency, 16 labels Zipf(s=1.0); four query
-sets of random-walk queries: 8 vertices sparse, 8 dense, 16 sparse, 16 dense
-(seeded synthetic stand-ins; the reference's datasets are not used).  A step
-is one gem_batch_run over a batch of queries drawn round-robin from the four
-sets (one persistent join launch per wave).  Every query runs under the same
-device time cap; a query that exceeds it is reported as capped, never as an
-exact count, and only exact queries enter `value`.
+Headline workload (default `rmat16`, the configuration whose every query
+completes exactly): R-MAT scale 16 (65,536 vertices), edge factor 8,
+(a,b,c,d) = (0.57,0.19,0.19,0.05), self loops and duplicates removed, uint32
+CSR with sorted adjacency, 8 uniform labels; 100 random-walk queries of 4
+vertices (seeded synthetic stand-ins; the reference's datasets are not used).
+A step is one gem_batch_run over the 100 queries (one persistent join launch
+per wave); `plain` runs the same queries one gem_query_run each.
+
+The scale-22 workload (`--workload rmat22`: 4,194,304 vertices, edge factor
+16, 16 labels Zipf(s=1.0), query sets 8 sparse / 8 dense / 16 sparse / 16
+dense) is reported in the `rmat22` section: its random-walk queries have
+10^13 to 10^17 embeddings each, so no exact method finishes them in a
+bounded step; the section reports, per query under a device time cap,
+whether it completed and the enumeration rate.  A query that exceeds the cap
+is reported as capped, never as an exact count.
 
 `value` is device-timed (CUDA events around each batch, inputs resident in
 HBM), `e2e` is wall time around the C-ABI call from host buffers (query
@@ -156,6 +162,7 @@ def run_gem(args):
     B = args.batch
     ctx = gem.Context(device=local, time_cap_ms=args.cap_ms)
     ctx.load_graph(g)
+    tuned = ctx.autotune(pool[: min(len(pool), 48)], trial_cap_ms=args.cap_ms) if args.autotune else {}
 
     def batch_of(step):
         i = (step * world + rank) * B
@@ -168,6 +175,7 @@ def run_gem(args):
     dev_ms, wall_ms, res_all = [], [], []
     h2d = d2h = launches = jbytes = 0
     jms = 0.0
+    phase = {"filter": 0.0, "tables": 0.0, "index": 0.0, "join": 0.0}
     with Clocks(local) as clk:
         for s in steps:
             qs = batch_of(s)
@@ -187,6 +195,8 @@ def run_gem(args):
             launches += sum(r["launches"] for r in waves.values())
             jbytes += sum(r["bytes_alg"][3] for r in waves.values())
             jms += sum(r["ms"]["join"] for r in waves.values())
+            for k in phase:
+                phase[k] += sum(r["ms"][k] for r in waves.values())
             res_all.append(rs)
             h2d += sum(4 * q.nv + 8 * q.ne for q in qs)
             d2h += 8 * 4 * len(qs)
@@ -206,11 +216,13 @@ def run_gem(args):
         dist.all_reduce(sm, op=dist.ReduceOp.SUM)
         tdev, twall = float(mx[0]), float(mx[1])
         exact, emb, capped = int(sm[0]), int(sm[1]), int(sm[2])
-    # plain mode: one query per call, latency distribution (rank 0, bounded sample)
+    # plain mode: the same queries, one gem_query_run each (rank 0)
     plain = {}
     if rank == 0 and args.plain > 0:
         lat, pe, pn, pdev = [], 0, 0, 0.0
-        for q in batch_of(args.warmup)[: args.plain]:
+        qs = batch_of(args.warmup)[: args.plain]
+        same = True
+        for q, rb in zip(qs, res_all[0]):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             r = ctx.run(q, raise_on_error=False)
@@ -220,9 +232,12 @@ def run_gem(args):
             if r["status"] == "OK":
                 pn += 1
                 pe += r["count"]
-        plain = {"queries": len(lat), "exact": pn, "queries_per_s": pn / (sum(lat) / 1e3) if lat else None,
-                 "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99)}
+                same &= rb["status"] != "OK" or rb["count"] == r["count"]
+        plain = {"queries": len(lat), "exact": pn, "queries_per_s": pn / pdev if pdev else None,
+                 "queries_per_s_wall": pn / (sum(lat) / 1e3) if lat else None,
+                 "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99), "counts_equal_batched": same}
     ctx.close()
+    c2 = rmat22_section(gem, args, local) if rank == 0 and args.c2_sample > 0 else None
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -251,7 +266,11 @@ def run_gem(args):
                        time_cap_ms=args.cap_ms, parallelism=f"replicas{world}", l2="flushed (256 MiB write)",
                        exact_queries=exact, capped_queries=capped, graph_gen_s=round(gen_s, 2)),
         "embeddings_per_s": emb / tdev if tdev > 0 else 0.0,
+        "batched_over_plain": (exact / tdev) / plain["queries_per_s"] if plain.get("queries_per_s") else None,
         "plain": plain,
+        "phase_ms": {k: round(v, 3) for k, v in phase.items()},
+        "autotune": tuned,
+        "rmat22": c2,
         "e2e": {"value": exact / twall if twall > 0 else 0.0, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -263,6 +282,30 @@ def run_gem(args):
     if args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(g, pool, args)
     print(json.dumps(line), flush=True)
+
+
+def rmat22_section(gem, args, local):
+    """Scale-22 R-MAT with 16 Zipf(1.0) labels and the 8s/8d/16s/16d query sets:
+    per query, plain run under a device time cap (status, count, nodes/s)."""
+    t = time.time()
+    g = gem.HostGraph.rmat(22, 16, seed=0x47454D00 + 22).set_labels(16, 1.0, seed=(0x47454D00 + 22) ^ 0x4C)
+    gen_s = time.time() - t
+    per = max(1, args.c2_sample // len(SETS))
+    out = {"workload": "rmat22-ef16-zipf16", "time_cap_ms": args.c2_cap_ms, "graph_gen_s": round(gen_s, 2),
+           "queries": []}
+    with gem.Context(device=local, time_cap_ms=args.c2_cap_ms) as c:
+        c.load_graph(g)
+        for i, (k, d) in enumerate(SETS):
+            for q in gem.gen_queries(g, k, d, per, seed=0x51000 + i):
+                r = c.run(q, raise_on_error=False)
+                js = r["ms"]["join"] / 1e3
+                out["queries"].append({"set": f"{k}{'s' if d == 1 else 'd'}", "edges": q.ne, "status": r["status"],
+                                       "count": r["count"] if r["status"] == "OK" else None,
+                                       "count_before_cap": r["count"] if r["status"] != "OK" else None,
+                                       "join_ms": round(r["ms"]["join"], 1),
+                                       "prefix_matches_per_s": r["nodes"] / js if js > 0 else None})
+    out["exact"] = sum(1 for x in out["queries"] if x["status"] == "OK")
+    return out
 
 
 def cpu_baseline(g, pool, args):
@@ -290,10 +333,10 @@ def run_reference(args):
     pool = query_pool(gem, g, sets, args.per_set)
     import oracle
     threads = os.cpu_count() or 1
-    B = min(args.batch, 4)
+    B = args.batch
     times, exact, emb = [], 0, 0
     for s in range(args.warmup + args.steps):
-        qs = [pool[(s * B + j) % len(pool)] for j in range(B)]
+        qs = [pool[(s * B + j) % len(pool)] for j in range(B)]  # the same batches as the GPU arm's steps
         t0 = time.perf_counter()
         for q in qs:
             c, h, ok = oracle.count(g, q, threads=threads, want_hash=False, work_cap=args.cpu_work_cap)
@@ -322,12 +365,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gem", choices=["gem", "reference"])
-    ap.add_argument("--workload", default="rmat22")
+    ap.add_argument("--workload", default="rmat16")
     ap.add_argument("--sets", default=None, help="query sets, e.g. '8s,8d,16s,16d' (s sparse, d dense, a any)")
-    ap.add_argument("--per-set", type=int, default=200)
-    ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--cap-ms", type=int, default=2000)
-    ap.add_argument("--plain", type=int, default=16)
+    ap.add_argument("--per-set", type=int, default=100)
+    ap.add_argument("--batch", type=int, default=100)
+    ap.add_argument("--cap-ms", type=int, default=20000)
+    ap.add_argument("--plain", type=int, default=100)
+    ap.add_argument("--autotune", type=int, default=1)
+    ap.add_argument("--c2-sample", type=int, default=8, help="scale-22 queries in the rmat22 section (0 = skip)")
+    ap.add_argument("--c2-cap-ms", type=int, default=1000)
     ap.add_argument("--cpu-sample", type=int, default=8)
     ap.add_argument("--cpu-work-cap", type=int, default=1_000_000_000)
     args = ap.parse_args()

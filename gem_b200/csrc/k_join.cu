@@ -213,8 +213,12 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
   }
 }
 
+// A lane intersects at most this many source entries by itself; longer
+// intersections are deferred to the whole warp (warp_suffix_count).
+constexpr uint64_t LANE_SCAN_MAX = 48;
+
 __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
-                                      uint32_t dup_mask, Stats &st) {
+                                      uint32_t dup_mask, Stats &st, bool &heavy) {
   uint32_t nl = 0;
   for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[(first + __ffs(m) - 1) & 31u].nback;
   uint32_t s = 0;
@@ -238,6 +242,10 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
     st.probes += __popc(dup_mask);
     return c;
   }
+  if (s_hi - s_lo > LANE_SCAN_MAX) {
+    heavy = true;
+    return 0;
+  }
   uint64_t c = 0;
   for (uint64_t e = s_lo; e < s_hi; ++e) {
     const uint32_t v = __ldg(a.values + e);
@@ -259,7 +267,9 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   return c;
 }
 
-__device__ uint64_t lane_suffix_count(const JoinArgs &a, const LaneCtx &x, Stats &st) {
+// Suffix completions of one lane's prefix match; sets `heavy` (and returns
+// 0) when an intersection is too long for one lane.
+__device__ uint64_t lane_suffix_count(const JoinArgs &a, const LaneCtx &x, Stats &st, bool &heavy) {
   const JQuery *Q = x.Q;
   uint64_t total = 1;
   const uint32_t ng = Q->n_groups < MAX_GROUPS ? Q->n_groups : MAX_GROUPS;
@@ -268,14 +278,110 @@ __device__ uint64_t lane_suffix_count(const JoinArgs &a, const LaneCtx &x, Stats
     const uint32_t gs = Q->grp_size[g] < MAX_GROUP ? Q->grp_size[g] : MAX_GROUP;
     const uint32_t dup_mask = Q->lv[first & 31u].dup_mask;
     if (gs == 1) {
-      total *= lane_subset_count(a, x, first, 1u, dup_mask, st);
+      total *= lane_subset_count(a, x, first, 1u, dup_mask, st, heavy);
+      if (heavy) return 0;
       continue;
     }
     uint64_t sv[1u << MAX_GROUP];
     for (uint32_t S = 0; S < (1u << MAX_GROUP); ++S) sv[S] = 0;
     for (uint32_t S = 1; S < (1u << gs); ++S) {
-      sv[S] = lane_subset_count(a, x, first, S, dup_mask, st);
+      sv[S] = lane_subset_count(a, x, first, S, dup_mask, st, heavy);
+      if (heavy) return 0;
       if (sv[S] == 0 && __popc(S) == 1) return 0;
+    }
+    uint64_t G = 0;
+    const uint32_t tb = Q->term_base[g], tc = Q->term_count[g];
+    for (uint32_t t = 0; t < tc; ++t) {
+      if (!inb(a, SITE_TERM, (uint64_t)tb + t, a.n_terms)) return 0;
+      const uint64_t term = __ldg(a.terms + tb + t);
+      uint64_t prod = (uint64_t)(int64_t)(int32_t)(uint32_t)(term >> 32);
+      const uint32_t blocks = (uint32_t)term;
+      for (uint32_t b = 0; b < MAX_GROUP; ++b) {
+        const uint32_t mk = (blocks >> (4 * b)) & 15u;
+        if (!mk) break;
+        prod *= sv[mk];
+      }
+      G += prod;
+    }
+    total *= G;
+  }
+  return total;
+}
+
+// Warp-cooperative form for one deferred (heavy) prefix match: every lane
+// receives the same context; lists are spread one per lane and the shortest
+// is scanned 32 entries at a time.
+__device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
+                                      uint32_t dup_mask, Stats &st) {
+  const uint32_t lane = lane_id();
+  uint32_t nl = 0;
+  for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[(first + __ffs(m) - 1) & 31u].nback;
+  nl = nl < 32 ? nl : 32;
+  uint64_t my_lo = 0, my_hi = 0;
+  if (lane < nl) lane_list(a, x, first, members, lane, my_lo, my_hi);
+  uint64_t best = lane < nl ? my_hi - my_lo : ~0ull;
+  uint32_t bl = lane;
+#pragma unroll
+  for (int d = 16; d; d >>= 1) {
+    const uint64_t ob = __shfl_xor_sync(FULL, best, d);
+    const uint32_t ol = __shfl_xor_sync(FULL, bl, d);
+    if (ob < best || (ob == best && ol < bl)) {
+      best = ob;
+      bl = ol;
+    }
+  }
+  const uint32_t src = bl;
+  const uint64_t s_lo = __shfl_sync(FULL, my_lo, src), s_hi = __shfl_sync(FULL, my_hi, src);
+  if (nl == 1) {
+    bool hit = false;
+    if ((dup_mask >> lane) & 1u) hit = contains_u32(a.values, s_lo, s_hi, lane == x.L ? x.w : x.sf[lane]);
+    return (s_hi - s_lo) - (uint64_t)__popc(__ballot_sync(FULL, hit));
+  }
+  uint64_t cnt = 0;
+  for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
+    const uint64_t e = cp + lane;
+    bool ok = e < s_hi;
+    const uint32_t v = ok ? __ldg(a.values + e) : 0u;
+    for (uint32_t i = 0; i < nl; ++i) {
+      const uint64_t lo = __shfl_sync(FULL, my_lo, i), hi = __shfl_sync(FULL, my_hi, i);
+      if (i == src) continue;
+      if (ok) ok = contains_u32(a.values, lo, hi, v);
+    }
+    for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
+      const uint32_t j = __ffs(dm) - 1;
+      ok = v != (j == x.L ? x.w : x.sf[j]);
+    }
+    cnt += __popc(__ballot_sync(FULL, ok));
+  }
+  if (lane == 0) {
+    st.scanned += s_hi - s_lo;
+    st.probes += (s_hi - s_lo) * (nl - 1);
+  }
+  return cnt;
+}
+
+__device__ uint64_t warp_suffix_count(const JoinArgs &a, const LaneCtx &x, Stats &st) {
+  const JQuery *Q = x.Q;
+  uint64_t total = 1;
+  const uint32_t ng = Q->n_groups < MAX_GROUPS ? Q->n_groups : MAX_GROUPS;
+  for (uint32_t g = 0; g < ng && total; ++g) {
+    const uint32_t first = Q->grp_first[g];
+    const uint32_t gs = Q->grp_size[g] < MAX_GROUP ? Q->grp_size[g] : MAX_GROUP;
+    const uint32_t dup_mask = Q->lv[first & 31u].dup_mask;
+    uint64_t sv[1u << MAX_GROUP];
+    for (uint32_t S = 0; S < (1u << MAX_GROUP); ++S) sv[S] = 0;
+    bool empty = false;
+    for (uint32_t S = 1; S < (1u << gs); ++S) {
+      sv[S] = warp_subset_count(a, x, first, S, dup_mask, st);
+      if (sv[S] == 0 && __popc(S) == 1) {
+        empty = true;
+        break;
+      }
+    }
+    if (empty) return 0;
+    if (gs == 1) {
+      total *= sv[1];
+      continue;
     }
     uint64_t G = 0;
     const uint32_t tb = Q->term_base[g], tc = Q->term_count[g];
@@ -480,6 +586,8 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         if (__shfl_sync(FULL, stop, 0)) break;
       }
       const uint64_t r = base + lane;
+      bool heavy = false;
+      uint32_t hq = 0, hw = 0, hidx = 0;
       if (r < a.lp_roots) {
         const uint32_t k = find_query(a.lp_prefix, a.lp_nq, r);
         const uint32_t q = a.lp_query[k];
@@ -504,12 +612,29 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
               x.widx = (uint32_t)rl;
               x.sf = sf;
               x.sidx = sidx;
-              cnt = lane_suffix_count(a, x, st);
+              cnt = lane_suffix_count(a, x, st, heavy);
+              hq = q;
+              hw = w0;
+              hidx = (uint32_t)rl;
             }
             if (cnt) atomicAdd(&a.out[q].count, (unsigned long long)cnt);
             if (h) atomicAdd(&a.out[q].hash, (unsigned long long)h);
           }
         }
+      }
+      // roots whose intersections are long: the whole warp, one at a time
+      for (uint32_t hm = __ballot_sync(FULL, heavy); hm; hm &= hm - 1) {
+        const uint32_t hl = __ffs(hm) - 1;
+        const uint32_t qh = __shfl_sync(FULL, hq, hl);
+        LaneCtx x;
+        x.Q = a.queries + qh;
+        x.L = 0;
+        x.w = __shfl_sync(FULL, hw, hl);
+        x.widx = __shfl_sync(FULL, hidx, hl);
+        x.sf = sf;
+        x.sidx = sidx;
+        const uint64_t k = warp_suffix_count(a, x, st);
+        if (lane == 0 && k) atomicAdd(&a.out[qh].count, (unsigned long long)k);
       }
       if (lane == 0) st.nodes += (a.lp_roots - base) < 32 ? (a.lp_roots - base) : 32;
     }
@@ -562,7 +687,8 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
           q = t.q;
           lvl = base_lvl = t.lvl;
           have = true;
-          if (!inb(a, SITE_QUERY, q, a.nquery) || !inb(a, SITE_LEVEL, lvl, a.queries[q].n) || lvl == 0) {
+          if (!inb(a, SITE_QUERY, q, a.nquery) || !inb(a, SITE_LEVEL, lvl, a.queries[q].n) || lvl == 0 ||
+              !inb(a, SITE_RANGE, t.end, a.n_values + 1) || !inb(a, SITE_RANGE, t.begin, t.end + 1)) {
             lvl = 0;  // unusable task: nothing to run (a failed check stops the grid)
             base_lvl = 1;
             q = 0;
@@ -690,15 +816,30 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
             sidx[lane] = c.idx;
           }
           __syncwarp();
+          bool heavy = false;
+          uint32_t widx = 0;
           if ((m >> lane) & 1u) {
             LaneCtx x;
             x.Q = Q;
             x.L = lvl;
             x.w = w;
-            x.widx = index_of(a, L, w);
+            x.widx = widx = index_of(a, L, w);
             x.sf = sf;
             x.sidx = sidx;
-            lane_cnt += lane_suffix_count(a, x, st);
+            lane_cnt += lane_suffix_count(a, x, st, heavy);
+          }
+          // candidates whose intersections are long: the whole warp, one at a time
+          for (uint32_t hm = __ballot_sync(FULL, heavy); hm; hm &= hm - 1) {
+            const uint32_t hl = __ffs(hm) - 1;
+            LaneCtx x;
+            x.Q = Q;
+            x.L = lvl;
+            x.w = __shfl_sync(FULL, w, hl);
+            x.widx = __shfl_sync(FULL, widx, hl);
+            x.sf = sf;
+            x.sidx = sidx;
+            const uint64_t k = warp_suffix_count(a, x, st);
+            if (lane == 0) lane_cnt += k;
           }
           __syncwarp();
           if (lane == 0) st.nodes += __popc(m);
