@@ -337,15 +337,49 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
     if ((dup_mask >> lane) & 1u) hit = contains_u32(a.values, s_lo, s_hi, lane == x.L ? x.w : x.sf[lane]);
     return (s_hi - s_lo) - (uint64_t)__popc(__ballot_sync(FULL, hit));
   }
+  // Merge intersection: 32 entries of the shortest list per step (one per
+  // lane) against coalesced 32-entry windows of every other list; list i's
+  // read cursor lives in lane i.  A window that ends below the step's first
+  // entry is skipped with one binary search (galloping for skewed lengths).
+  uint64_t cur = my_lo;
   uint64_t cnt = 0;
   for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
     const uint64_t e = cp + lane;
     bool ok = e < s_hi;
-    const uint32_t v = ok ? __ldg(a.values + e) : 0u;
+    const uint32_t v = ok ? __ldg(a.values + e) : 0xFFFFFFFFu;
+    const uint32_t last = (uint32_t)((s_hi - cp) < 32 ? (s_hi - cp - 1) : 31);
+    const uint32_t vmin = __shfl_sync(FULL, v, 0), vmax = __shfl_sync(FULL, v, last);
     for (uint32_t i = 0; i < nl; ++i) {
-      const uint64_t lo = __shfl_sync(FULL, my_lo, i), hi = __shfl_sync(FULL, my_hi, i);
       if (i == src) continue;
-      if (ok) ok = contains_u32(a.values, lo, hi, v);
+      uint64_t bp = __shfl_sync(FULL, cur, i);
+      const uint64_t be = __shfl_sync(FULL, my_hi, i);
+      bool found = false;
+      if (bp < be) {
+        const uint64_t probe = bp + 31 < be ? bp + 31 : be - 1;
+        if (__ldg(a.values + probe) < vmin) bp = lower_bound_u32(a.values, probe + 1, be, vmin);
+      }
+      while (bp < be) {
+        const uint64_t j = bp + lane;
+        const uint32_t b = j < be ? __ldg(a.values + j) : 0xFFFFFFFFu;
+        const uint32_t bl = (uint32_t)((be - bp) < 32 ? (be - bp - 1) : 31);
+        const uint32_t bmax = __shfl_sync(FULL, b, bl);
+        // lane-register binary search of v among the window's 32 values
+        uint32_t lo = 0, hi = bl + 1;
+#pragma unroll
+        for (int step = 0; step < 6; ++step) {
+          const uint32_t mid = (lo + hi) >> 1;
+          const uint32_t bm = __shfl_sync(FULL, b, mid & 31u);
+          if (lo < hi) {
+            if (bm < v) lo = mid + 1; else hi = mid;
+          }
+        }
+        const uint32_t bf = __shfl_sync(FULL, b, lo & 31u);
+        found |= lo <= bl && bf == v;
+        if (bmax >= vmax) break;  // entries > vmax may serve the next step
+        bp += 32;
+      }
+      ok = ok && found;
+      if (lane == i) cur = bp;
     }
     for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
