@@ -591,6 +591,11 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
   c.f = 0; c.idx = 0; c.hs = 0; c.pos = 0; c.end = 0; c.cbase = 0; c.mask = 0; c.src = 0;
   Stats st;
   bool idle_registered = false;
+  // Root batch held by this warp ([rb_cur, rb_end) of the ordinary pool); the
+  // warp counts as busy from the batch grab until its last root retires.
+  uint64_t rb_cur = 0, rb_end = 0;
+  const uint64_t total_warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  bool pushed = false;  // donated work since the last busy decrement
 
   // ---------------------------------------------------------------- lane-parallel roots
   // Queries whose only enumerated level is the root: one root per lane.
@@ -680,22 +685,38 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
     bool have = false, from_root = false;
     uint64_t r = 0;
     if (!idle_registered) {
-      unsigned long long rr = 0;
-      if (lane == 0) {
-        atomicAdd(&ctl->busy, 1u);
-        __threadfence();
-        rr = atomicAdd(&ctl->root_next, 1ull);
-        if (rr >= a.n_roots) atomicSub(&ctl->busy, 1u);
+      if (rb_cur >= rb_end) {
+        // guided batches: a quarter of the remaining roots per warp, 1..16
+        unsigned long long rr = 0, cnt = 1;
+        if (lane == 0) {
+          const unsigned long long seen = ld_vol(&ctl->root_next);
+          const unsigned long long left = seen < a.n_roots ? a.n_roots - seen : 0;
+          cnt = left / (4ull * total_warps);
+          cnt = cnt < 1 ? 1 : (cnt > 16 ? 16 : cnt);
+          atomicAdd(&ctl->busy, 1u);
+          __threadfence();
+          rr = atomicAdd(&ctl->root_next, cnt);
+          if (rr >= a.n_roots) atomicSub(&ctl->busy, 1u);
+        }
+        rb_cur = __shfl_sync(FULL, rr, 0);
+        cnt = __shfl_sync(FULL, cnt, 0);
+        rb_end = rb_cur < a.n_roots ? (rb_cur + cnt < a.n_roots ? rb_cur + cnt : a.n_roots) : rb_cur;
       }
-      r = __shfl_sync(FULL, rr, 0);
+      r = rb_cur < rb_end ? rb_cur++ : a.n_roots;
       // warp-uniform: lane 0 reads the error word for the whole warp
       const int err_set = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->err) != DERR_NONE) : 0, 0);
       if (r < a.n_roots && err_set) {
-        // past the deadline: this root is not processed
+        // past the deadline: this root and the rest of the batch are not processed
         if (lane == 0) {
-          abandon(a, find_query(a.root_prefix, a.nquery, r));
+          const uint32_t q0 = find_query(a.root_prefix, a.nquery, r);
+          const uint32_t q1 = find_query(a.root_prefix, a.nquery, rb_end - 1);
+          for (uint32_t k = q0; k <= q1; ++k) atomicOr(&a.out[k].pad[0], 1ull);
+          abandon(a, q0);
+          if (pushed) __threadfence();
           atomicSub(&ctl->busy, 1u);
         }
+        pushed = false;
+        rb_cur = rb_end;
         r = a.n_roots;
       }
       if (r < a.n_roots) {
@@ -832,17 +853,28 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
           continue;
         }
         uint64_t new_end = end;
-        // warp-uniform: lane 0 reads the idle count for the whole warp
-        const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->idle) > 0) : 0, 0);
-        if (lvl <= a.donate_max_level && end > pos + 32 + 64 && idle_now) {
-          const uint64_t rem = pos + 32;
-          const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
-          if (mid < end) {
-            const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
-            if (queue_push(ctl, a.queue, q, lvl, src, mid, end, hsp, c)) new_end = mid;
+        // Donate the unread half of this level when another warp is idle and
+        // the half is worth a queue round trip: >= 1024 candidates at the
+        // lane-parallel level (cheap per candidate), >= 128 where each
+        // candidate opens a subtree.
+        const bool lane_level = MODE == MODE_COUNT && lvl + 1 >= Q->n_enum;
+        const uint64_t min_half = lane_level ? 1024 : 128;
+        if (lvl <= a.donate_max_level && end >= pos + 32 + 2 * min_half) {
+          // warp-uniform: lane 0 reads the idle count for the whole warp
+          const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->idle) > 0) : 0, 0);
+          if (idle_now) {
+            const uint64_t rem = pos + 32;
+            const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
+            if (mid < end) {
+              const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
+              if (queue_push(ctl, a.queue, q, lvl, src, mid, end, hsp, c)) {
+                new_end = mid;
+                pushed = true;
+              }
+            }
           }
         }
-        if (MODE == MODE_COUNT && lvl + 1 >= Q->n_enum) {
+        if (lane_level) {
           // last enumerated level: each lane counts its own candidate's
           // suffix completions (32 prefix matches in flight per warp)
           if (lane < lvl) {
@@ -929,13 +961,23 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
       tc += __shfl_xor_sync(FULL, tc, d);
       th += __shfl_xor_sync(FULL, th, d);
     }
+    const bool release = abort || !from_root || rb_cur >= rb_end;
     if (lane == 0) {
-      if (abort) abandon(a, q);
+      if (abort) {
+        abandon(a, q);
+        if (from_root && rb_cur < rb_end) {
+          const uint32_t q1 = find_query(a.root_prefix, a.nquery, rb_end - 1);
+          for (uint32_t k = q; k <= q1; ++k) atomicOr(&a.out[k].pad[0], 1ull);
+        }
+      }
       if (tc) atomicAdd(&a.out[q].count, (unsigned long long)tc);
       if (MODE != MODE_COUNT && th) atomicAdd(&a.out[q].hash, (unsigned long long)th);
-      __threadfence();
-      atomicSub(&ctl->busy, 1u);
+      if (release) {
+        if (pushed) __threadfence();  // donated tasks are visible before quiescence can be observed
+        atomicSub(&ctl->busy, 1u);
+      }
     }
+    if (release) pushed = false;
     if (abort) break;
     if (!from_root && !idle_registered) {
       idle_registered = true;
