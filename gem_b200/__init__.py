@@ -368,7 +368,14 @@ class Context:
         rep = np.zeros(18, np.uint32)
         _check(lib().gem_autotune(self._h, arr, len(qs), mode, trial_cap_ms, _p32(rep)), self._h, "autotune")
         names = ("<=4", "<=8", "<=12", "<=16", "<=24", "<=32")
-        return {names[b]: tuple(int(x) for x in rep[3 * b:3 * b + 3]) for b in range(6) if rep[3 * b]}
+        out = {}
+        for b in range(6):
+            if rep[3 * b]:
+                sched = int(rep[3 * b + 1])
+                out[names[b]] = {"blocks_per_sm": int(rep[3 * b]), "donate_max_level": sched & 0xFF,
+                                 "donate_min_lane": (sched >> 8) & 0xFFF, "root_batch_max": sched >> 20,
+                                 "join_us": int(rep[3 * b + 2])}
+        return out
 
     def submit(self, q, mode=MODE_COUNT):
         """Serving: returns a ticket, or None when admission is busy (retry later)."""

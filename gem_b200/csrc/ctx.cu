@@ -837,6 +837,10 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   for (auto &J : jq) maxnv = std::max(maxnv, J.n);
   const Tune &tu = ctx->tune[size_bucket(maxnv)];
   a.donate_max_level = tu.donate_max_level ? tu.donate_max_level : ctx->donate_max_level;
+  a.donate_min_lane = tu.donate_min_lane ? tu.donate_min_lane : 32;
+  a.donate_min_desc = 32;
+  a.root_batch_max = tu.root_batch_max ? tu.root_batch_max : 1;
+  a.lane_scan_max = tu.lane_scan_max ? tu.lane_scan_max : 48;
   a.nv = ctx->g.nv;
   a.n_values = w.table_values;
   a.n_backs = (uint32_t)jb.size();
@@ -1189,13 +1193,17 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
     std::string e;
     if (make_host_query(&qs[i], h, e) != GEM_OK) continue;
     auto &v = byb[size_bucket(h.nv)];
-    if (v.size() < 8) v.push_back(h);
+    if (v.size() < 32) v.push_back(h);
   }
   const int occ = ctx->join_bps[mode];
   std::vector<uint32_t> bps_c = {(uint32_t)occ};
   if (occ > 1) bps_c.push_back((uint32_t)occ - 1);
   if (occ > 2) bps_c.push_back((uint32_t)(occ + 1) / 2);
-  const uint32_t don_c[3] = {2, 6, 30};
+  struct Sched {
+    uint32_t dm, dml, rb, lsm;
+  };
+  const Sched sched_c[8] = {{30, 32, 1, 48}, {6, 32, 1, 48}, {2, 32, 1, 48}, {30, 256, 1, 48},
+                            {30, 32, 4, 48}, {30, 32, 1, 8},  {30, 32, 1, 160}, {6, 96, 2, 16}};
   const uint32_t saved_cap = ctx->opts.time_cap_ms;
   ctx->opts.time_cap_ms = trial_cap_ms ? trial_cap_ms : 2000;
   gem_status st = GEM_OK;
@@ -1204,9 +1212,12 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
     Tune best;
     double best_cost = 1e300;
     for (uint32_t bps : bps_c)
-      for (uint32_t dm : don_c) {
+      for (const Sched &sc : sched_c) {
         ctx->tune[b].blocks_per_sm = bps;
-        ctx->tune[b].donate_max_level = dm;
+        ctx->tune[b].donate_max_level = sc.dm;
+        ctx->tune[b].donate_min_lane = sc.dml;
+        ctx->tune[b].root_batch_max = sc.rb;
+        ctx->tune[b].lane_scan_max = sc.lsm;
         Wave w;
         w.q = byb[b];
         ctx->arena.reset();
@@ -1218,7 +1229,10 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
         if (cost < best_cost) {
           best_cost = cost;
           best.blocks_per_sm = bps;
-          best.donate_max_level = dm;
+          best.donate_max_level = sc.dm;
+          best.donate_min_lane = sc.dml;
+          best.root_batch_max = sc.rb;
+          best.lane_scan_max = sc.lsm;
           best.best_ms = (float)cost;
         }
       }
@@ -1228,7 +1242,8 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
   if (report)
     for (uint32_t b = 0; b < 6; ++b) {
       report[3 * b] = ctx->tune[b].blocks_per_sm;
-      report[3 * b + 1] = ctx->tune[b].donate_max_level;
+      report[3 * b + 1] = ctx->tune[b].donate_max_level | (ctx->tune[b].donate_min_lane << 8) |
+                          (ctx->tune[b].root_batch_max << 20);
       report[3 * b + 2] = (uint32_t)(ctx->tune[b].best_ms * 1000.0f);
     }
   return st;

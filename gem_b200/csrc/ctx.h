@@ -84,6 +84,9 @@ struct Wave {
 struct Tune {
   uint32_t blocks_per_sm = 0;
   uint32_t donate_max_level = 0;
+  uint32_t donate_min_lane = 0;   // 0 = library default
+  uint32_t root_batch_max = 0;    // 0 = library default
+  uint32_t lane_scan_max = 0;     // 0 = library default
   float best_ms = 0;
 };
 // Buckets by query size: <=4, <=8, <=12, <=16, <=24, <=32 vertices.

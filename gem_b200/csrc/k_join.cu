@@ -213,9 +213,6 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
   }
 }
 
-// A lane intersects at most this many source entries by itself; longer
-// intersections are deferred to the whole warp (warp_suffix_count).
-constexpr uint64_t LANE_SCAN_MAX = 48;
 
 __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
                                       uint32_t dup_mask, Stats &st, bool &heavy) {
@@ -242,7 +239,9 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
     st.probes += __popc(dup_mask);
     return c;
   }
-  if (s_hi - s_lo > LANE_SCAN_MAX) {
+  // A lane intersects at most a.lane_scan_max source entries by itself;
+  // longer intersections are deferred to the whole warp (warp_suffix_count).
+  if (s_hi - s_lo > a.lane_scan_max) {
     heavy = true;
     return 0;
   }
@@ -692,7 +691,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
           const unsigned long long seen = ld_vol(&ctl->root_next);
           const unsigned long long left = seen < a.n_roots ? a.n_roots - seen : 0;
           cnt = left / (4ull * total_warps);
-          cnt = cnt < 1 ? 1 : (cnt > 16 ? 16 : cnt);
+          cnt = cnt < 1 ? 1 : (cnt > a.root_batch_max ? a.root_batch_max : cnt);
           atomicAdd(&ctl->busy, 1u);
           __threadfence();
           rr = atomicAdd(&ctl->root_next, cnt);
@@ -760,9 +759,8 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         }
         int leave = 0;
         if (lane == 0) {
-          __threadfence();
           const unsigned int b = ld_vol(&ctl->busy);
-          __threadfence();
+          __threadfence();  // the queue is read after `busy`
           const bool empty = ld_vol(&ctl->head) >= ld_vol(&ctl->tail);
           if (b == 0 && empty) leave = 1;
           if (ld_vol(&ctl->err) != DERR_NONE) leave = 1;
@@ -773,7 +771,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         }
         if (__shfl_sync(FULL, leave, 0)) break;
         __nanosleep(backoff);
-        backoff = backoff < 4096 ? backoff * 2 : 4096;
+        backoff = backoff < 16384 ? backoff * 2 : 16384;
       }
       if (!have) {
         if (lane == 0) atomicSub(&ctl->idle, 1u);
@@ -854,11 +852,11 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         }
         uint64_t new_end = end;
         // Donate the unread half of this level when another warp is idle and
-        // the half is worth a queue round trip: >= 1024 candidates at the
-        // lane-parallel level (cheap per candidate), >= 128 where each
-        // candidate opens a subtree.
+        // the half is at least the tuned minimum (separate minimums for the
+        // lane-parallel level, cheap per candidate, and for levels whose
+        // candidates open subtrees).
         const bool lane_level = MODE == MODE_COUNT && lvl + 1 >= Q->n_enum;
-        const uint64_t min_half = lane_level ? 1024 : 128;
+        const uint64_t min_half = lane_level ? a.donate_min_lane : a.donate_min_desc;
         if (lvl <= a.donate_max_level && end >= pos + 32 + 2 * min_half) {
           // warp-uniform: lane 0 reads the idle count for the whole warp
           const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->idle) > 0) : 0, 0);

@@ -244,6 +244,10 @@ struct JoinArgs {
   uint32_t *emb;             // ENUM: output buffer
   uint64_t emb_cap;          // embeddings that fit
   uint32_t donate_max_level; // donate candidates of levels <= this
+  uint32_t donate_min_lane;  // smallest donated half at the lane-parallel level
+  uint32_t donate_min_desc;  // smallest donated half at other levels
+  uint32_t root_batch_max;   // largest root batch a warp takes at once
+  uint32_t lane_scan_max;    // longest intersection one lane does alone
   uint32_t nv;               // data vertices (bounds of rank-bitmap probes)
   uint64_t n_values;         // entries of `values`
   uint32_t n_backs;          // entries of `backs`

@@ -200,11 +200,14 @@ gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n,
 
 /* Autotuner (no counterpart in the reference): for each query-size bucket
  * (<=4, <=8, <=12, <=16, <=24, <=32 vertices) present in qs, runs a sample of
- * up to 8 of its queries under each candidate join schedule (blocks per SM of
+ * up to 32 of its queries under each candidate join schedule (blocks per SM of
  * the persistent grid, deepest level that donates work), each trial capped at
  * trial_cap_ms, and keeps the fastest for later waves of this context.
+ * Candidate schedules combine blocks per SM with the deepest donating level,
+ * the smallest donated half at the lane-parallel level and the root batch.
  * report (optional, 18 entries): per bucket {blocks_per_sm,
- * donate_max_level, best join time in us}; zeros for untuned buckets. */
+ * donate_max_level | donate_min_lane << 8 | root_batch_max << 20, best join
+ * time in us}; zeros for untuned buckets. */
 gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode,
                         uint32_t trial_cap_ms, uint32_t *report);
 

@@ -323,6 +323,6 @@ def test_autotune_keeps_results(small):
         c.load_graph(small)
         before = [c.run(q)["count"] for q in qs]
         rep = c.autotune(qs, trial_cap_ms=5000)
-        assert rep and all(v[0] >= 1 and v[1] >= 1 for v in rep.values())
+        assert rep and all(v["blocks_per_sm"] >= 1 and v["donate_max_level"] >= 1 for v in rep.values())
         st, after = c.batch(qs)
         assert st == 0 and [r["count"] for r in after] == before
