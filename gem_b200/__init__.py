@@ -43,7 +43,7 @@ EXPORTS = (
     "gem_hgraph_destroy", "gem_query_read_text", "gem_query_write_text", "gem_gen_queries",
     "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
-    "gem_submit", "gem_poll", "gem_autotune",
+    "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static",
 )
 
 
@@ -115,6 +115,8 @@ def lib():
         L.gem_submit.argtypes = [vp, C.POINTER(_Query), C.c_int, u64p]
         L.gem_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Result), C.POINTER(C.c_int)]
         L.gem_autotune.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, C.c_uint32, u32p]
+        L.gem_filter_static.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(_Query), C.c_uint32, u32p, vp,
+                                        C.c_uint64, vp]
         _lib = L
     return _lib
 

@@ -250,6 +250,32 @@ gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t u,
                            uint32_t index_kind, const uint32_t *keys,
                            uint32_t n_keys, uint32_t *pos_out);
 
+/* Candidate filter that allocates nothing (no counterpart in the reference).
+ * For callers that cannot allocate device memory — code inside another
+ * framework's allocator or memory pool, which owns every device byte of the
+ * process, or a service whose memory is reserved up front and must not grow
+ * while it serves.  The caller passes the
+ * data graph as device arrays it owns (offsets nv+1, nbrs offsets[nv],
+ * labels nv) and a device output array d_cand of cand_cap entries; the
+ * C(u) lists are written back to back (u = 0 first) and counts[u] (host
+ * array, nv_q entries) receives |C(u)|, exactly as gem_filter does.  Scratch
+ * lives in a fixed device array of GEM_STATIC_SCRATCH_BYTES held by every
+ * GPU that loads libgem until exit; graphs above GEM_STATIC_MAX_VERTICES
+ * vertices return GEM_ERR_LIMIT; more candidates than cand_cap return
+ * GEM_ERR_OVERFLOW with exact counts.  All calls on a device share that
+ * array, so calls whose work overlaps on the GPU race: order them on one
+ * stream.  The first call on a device looks up the array's address (with
+ * that device current) and should come before any stream capture.  stream
+ * is a cudaStream_t (NULL = legacy default stream); the call returns after
+ * the stream has finished its work. */
+#define GEM_STATIC_SCRATCH_BYTES (4u << 20)
+#define GEM_STATIC_MAX_VERTICES 8000000u
+gem_status gem_filter_static(const uint64_t *d_offsets, const uint32_t *d_nbrs,
+                             const uint32_t *d_labels, uint32_t nv,
+                             const gem_query *q, uint32_t threshold,
+                             uint32_t *counts, uint32_t *d_cand,
+                             uint64_t cand_cap, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching with memory-based admission.                 */
 /* The first gem_submit starts a server thread on the context; from then on  */
