@@ -326,3 +326,33 @@ def test_autotune_keeps_results(small):
         assert rep and all(v["blocks_per_sm"] >= 1 and v["donate_max_level"] >= 1 for v in rep.values())
         st, after = c.batch(qs)
         assert st == 0 and [r["count"] for r in after] == before
+
+
+REF_COUNTS = os.path.join(os.path.dirname(__file__), "golden", "ref_counts.json")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_COUNTS), reason="reference-binary fixture not generated")
+def test_counts_match_reference_binary():
+    """Counts printed by the reference's own in-core binary (a uint32 print,
+    in-core/src/main.cu:233) equal the GPU count mod 2^32 on every recorded
+    case, including those too large for the oracle's work cap."""
+    with open(REF_COUNTS) as f:
+        data = json.load(f)
+    graphs, checked = {}, 0
+    for c in data["cases"]:
+        if c["exit"] != 0 or len(c["printed"]) != 1:
+            continue
+        gd = c["graph"]
+        if gd["name"] not in graphs:
+            g = gem.HostGraph.rmat(gd["scale"], gd["edge_factor"], seed=gd["seed"]).set_labels(
+                gd["labels"], gd["zipf_s"], seed=gd["seed"] ^ 0x4C)
+            ctx = gem.Context(time_cap_ms=60000)
+            ctx.load_graph(g)
+            graphs[gd["name"]] = ctx
+        r = graphs[gd["name"]].run(gem.Query(c["labels"], c["edges"]))
+        assert r["status"] == "OK"
+        assert r["count"] % (1 << 32) == c["printed"][0], (gd["name"], c["labels"], c["edges"], r["count"])
+        checked += 1
+    for ctx in graphs.values():
+        ctx.close()
+    assert checked >= 10
