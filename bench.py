@@ -173,7 +173,7 @@ def run_gem(args):
         ctx.batch(batch_of(s))
     steps = list(range(args.warmup, args.warmup + args.steps))
     dev_ms, wall_ms, res_all = [], [], []
-    h2d = d2h = launches = jbytes = 0
+    h2d = d2h = launches = jbytes = n_joins = 0
     jms = 0.0
     phase = {"filter": 0.0, "tables": 0.0, "index": 0.0, "join": 0.0}
     with Clocks(local) as clk:
@@ -194,6 +194,7 @@ def run_gem(args):
             dev_ms.append(sum(r["ms"]["total"] for r in waves.values()))
             launches += sum(r["launches"] for r in waves.values())
             jbytes += sum(r["bytes_alg"][3] for r in waves.values())
+            n_joins += len(waves)
             jms += sum(r["ms"]["join"] for r in waves.values())
             for k in phase:
                 phase[k] += sum(r["ms"][k] for r in waves.values())
@@ -249,6 +250,8 @@ def run_gem(args):
     except Exception:
         peak, peak_src = 6650.0, "fallback"
     achieved = (jb / jt / 1e9) if jt > 0 else 0.0
+    set_names = ",".join(f"{k}{'s' if d == 1 else 'd' if d == 2 else 'a'}" for k, d in sets)
+    traffic, traffic_src = profiled_traffic(f"{args.workload} {set_names} batch {B}")
     line = {
         "metric": METRIC,
         "value": exact / tdev if tdev > 0 else 0.0,
@@ -274,7 +277,8 @@ def run_gem(args):
         "e2e": {"value": exact / twall if twall > 0 else 0.0, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if peak else None, "traffic": None, "kernel": "join_kernel<COUNT>",
+                     "frac": achieved / peak if peak else None, "traffic": traffic, "traffic_source": traffic_src,
+                     "alg_bytes_per_launch": jb / n_joins if n_joins else None, "kernel": "join_kernel<COUNT>",
                      "peak_source": peak_src},
         "gpu_launches": launches,
         "clocks": clk.summary(),
@@ -282,6 +286,21 @@ def run_gem(args):
     if args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(g, pool, args)
     print(json.dumps(line), flush=True)
+
+
+def profiled_traffic(key):
+    """DRAM bytes (read + write) of one join launch of the workload `key`
+    ("<workload> <query sets> batch <B>"), from the committed ncu capture
+    summary whose `workload_key` line equals it, or None."""
+    import glob
+    import re
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "join_*.md"))):
+        text = open(path).read()
+        k = re.search(r"^workload_key: (.+)$", text, re.M)
+        m = re.search(r"^dram_bytes_per_launch: (\d+)$", text, re.M)
+        if k and m and k.group(1).strip() == key:
+            return int(m.group(1)), os.path.relpath(path, ROOT) + " (ncu, one launch)"
+    return None, None
 
 
 def rmat22_section(gem, args, local):
@@ -362,7 +381,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gem", choices=["gem", "reference"])
     ap.add_argument("--workload", default="rmat16")

@@ -148,9 +148,10 @@ extern "C" gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out) {
   // persistent small buffers
   CU(cudaMalloc(&ctx->d_ctl, sizeof(JControl)));
   CU(cudaMalloc(&ctx->d_queue, sizeof(JTask) * TASK_CAP));
+  CU(cudaMalloc(&ctx->d_qends, sizeof(JQueueEnds) * QUEUE_SUBQ));
   CU(cudaMalloc(&ctx->d_err, sizeof(uint32_t) * 4));
   CU(cudaHostAlloc(&ctx->h_small, 1 << 20, cudaHostAllocDefault));
-  ctx->device_bytes += sizeof(JControl) + sizeof(JTask) * TASK_CAP + 16;
+  ctx->device_bytes += sizeof(JControl) + sizeof(JTask) * TASK_CAP + sizeof(JQueueEnds) * QUEUE_SUBQ + 16;
   *out = c.release();
   return GEM_OK;
 }
@@ -180,6 +181,7 @@ extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
   destroy_join_graph(ctx->jgraph);
   if (ctx->d_ctl) cudaFree(ctx->d_ctl);
   if (ctx->d_queue) cudaFree(ctx->d_queue);
+  if (ctx->d_qends) cudaFree(ctx->d_qends);
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   for (auto &ev : ctx->ev)
@@ -830,6 +832,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   a.out = d_out;
   a.ctl = ctx->d_ctl;
   a.queue = ctx->d_queue;
+  a.qends = ctx->d_qends;
   a.emb = emb_dev;
   a.emb_cap = emb_cap;
   // schedule: tuned per query-size bucket (largest query of the wave)
@@ -838,7 +841,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   const Tune &tu = ctx->tune[size_bucket(maxnv)];
   a.donate_max_level = tu.donate_max_level ? tu.donate_max_level : ctx->donate_max_level;
   a.donate_min_lane = tu.donate_min_lane ? tu.donate_min_lane : 32;
-  a.donate_min_desc = 32;
+  a.donate_min_desc = tu.donate_min_desc ? tu.donate_min_desc : 1;
   a.root_batch_max = tu.root_batch_max ? tu.root_batch_max : 1;
   a.lane_scan_max = tu.lane_scan_max ? tu.lane_scan_max : 48;
   a.nv = ctx->g.nv;
@@ -859,12 +862,16 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   w.join_ms = ev_ms(ctx->ev[6], ctx->ev[7]);
   // Donated tasks still queued when the grid stopped (deadline) were never
   // run: their queries are incomplete.
-  if (hc.head < hc.tail) {
-    for (unsigned long long t = hc.head; t < hc.tail && t < hc.head + TASK_CAP; ++t) {
-      uint32_t qq = 0;
-      CU(cudaMemcpy(&qq, &ctx->d_queue[t & (TASK_CAP - 1)].q, 4, cudaMemcpyDeviceToHost));
-      if (qq < out.size()) out[qq].pad[0] = 1;
-    }
+  if (hc.pending) {
+    std::vector<JQueueEnds> ends(QUEUE_SUBQ);
+    CU(cudaMemcpy(ends.data(), ctx->d_qends, sizeof(JQueueEnds) * QUEUE_SUBQ, cudaMemcpyDeviceToHost));
+    for (uint32_t sq = 0; sq < QUEUE_SUBQ; ++sq)
+      for (unsigned long long t = ends[sq].head; t < ends[sq].tail && t < ends[sq].head + QUEUE_SUBQ_CAP; ++t) {
+        uint32_t qq = 0;
+        CU(cudaMemcpy(&qq, &ctx->d_queue[sq * QUEUE_SUBQ_CAP + (t & (QUEUE_SUBQ_CAP - 1))].q, 4,
+                      cudaMemcpyDeviceToHost));
+        if (qq < out.size()) out[qq].pad[0] = 1;
+      }
   }
   for (size_t qi = 0; qi < w.q.size(); ++qi)
     if (w.jq_index[qi] != UINT32_MAX) w.out[qi] = out[w.jq_index[qi]];
@@ -1200,10 +1207,10 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
   if (occ > 1) bps_c.push_back((uint32_t)occ - 1);
   if (occ > 2) bps_c.push_back((uint32_t)(occ + 1) / 2);
   struct Sched {
-    uint32_t dm, dml, rb, lsm;
+    uint32_t dm, dml, rb, lsm, dmd;
   };
-  const Sched sched_c[8] = {{30, 32, 1, 48}, {6, 32, 1, 48}, {2, 32, 1, 48}, {30, 256, 1, 48},
-                            {30, 32, 4, 48}, {30, 32, 1, 8},  {30, 32, 1, 160}, {6, 96, 2, 16}};
+  const Sched sched_c[8] = {{30, 32, 1, 48, 1},  {6, 32, 1, 48, 1},  {2, 32, 1, 48, 1},  {30, 256, 1, 48, 1},
+                            {30, 32, 4, 48, 1},  {30, 32, 1, 8, 1},  {30, 32, 1, 160, 1}, {30, 32, 1, 48, 32}};
   const uint32_t saved_cap = ctx->opts.time_cap_ms;
   ctx->opts.time_cap_ms = trial_cap_ms ? trial_cap_ms : 2000;
   gem_status st = GEM_OK;
@@ -1218,6 +1225,7 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
         ctx->tune[b].donate_min_lane = sc.dml;
         ctx->tune[b].root_batch_max = sc.rb;
         ctx->tune[b].lane_scan_max = sc.lsm;
+        ctx->tune[b].donate_min_desc = sc.dmd;
         Wave w;
         w.q = byb[b];
         ctx->arena.reset();
@@ -1233,6 +1241,7 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
           best.donate_min_lane = sc.dml;
           best.root_batch_max = sc.rb;
           best.lane_scan_max = sc.lsm;
+          best.donate_min_desc = sc.dmd;
           best.best_ms = (float)cost;
         }
       }

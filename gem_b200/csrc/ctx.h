@@ -87,6 +87,7 @@ struct Tune {
   uint32_t donate_min_lane = 0;   // 0 = library default
   uint32_t root_batch_max = 0;    // 0 = library default
   uint32_t lane_scan_max = 0;     // 0 = library default
+  uint32_t donate_min_desc = 0;   // 0 = library default
   float best_ms = 0;
 };
 // Buckets by query size: <=4, <=8, <=12, <=16, <=24, <=32 vertices.
@@ -115,6 +116,7 @@ struct gem_ctx {
   Arena arena;
   gem::JControl *d_ctl = nullptr;
   gem::JTask *d_queue = nullptr;
+  gem::JQueueEnds *d_qends = nullptr;
   uint32_t *d_err = nullptr;
   void *h_small = nullptr;
   // join schedule: CUDA graph and per-size-bucket tuning (gem_autotune)

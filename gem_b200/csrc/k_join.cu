@@ -173,6 +173,110 @@ __device__ __forceinline__ uint32_t index_of(const JoinArgs &a, const JLevel *__
 }
 
 // ---------------------------------------------------------------------------
+// Per-warp list cache in shared memory.  A suffix list keyed by an earlier
+// level than the last enumerated one is the same for all 32 lanes of a chunk
+// and usually for every chunk of the same prefix, so the warp copies the two
+// longest of them (up to LIST_CACHE_CAP entries each) into shared memory and
+// membership tests against them become shared-memory binary searches instead
+// of chains of dependent L2 loads.  A slot is tagged by the list's absolute
+// range in the values array, which identifies the list for the whole launch.
+// ---------------------------------------------------------------------------
+struct ListCache {
+  uint32_t *buf;            // LIST_CACHE_SLOTS * LIST_CACHE_CAP entries
+  unsigned long long *tag;  // {lo, hi} per slot
+};
+
+__device__ __forceinline__ int cache_slot(const ListCache &lc, uint64_t lo, uint64_t hi) {
+  if (hi <= lo) return -1;
+#pragma unroll
+  for (int k = 0; k < (int)LIST_CACHE_SLOTS; ++k)
+    if (lc.tag[2 * k] == lo && lc.tag[2 * k + 1] == hi) return k;
+  return -1;
+}
+
+__device__ __forceinline__ bool smem_contains(const uint32_t *b, uint32_t n, uint32_t x) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (b[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo < n && b[lo] == x;
+}
+
+// x in list [lo, hi): from the cache slot when there is one, else by binary
+// search of the values array from *cur (lists are probed in ascending x, so
+// the search start only moves forward).
+__device__ __forceinline__ bool list_member(const JoinArgs &a, const ListCache &lc, int slot, uint64_t lo,
+                                            uint64_t hi, uint64_t &cur, uint32_t x) {
+  if (slot >= 0) return smem_contains(lc.buf + slot * LIST_CACHE_CAP, (uint32_t)(hi - lo), x);
+  const uint64_t p = lower_bound_u32(a.values, cur, hi, x);
+  cur = p;
+  return p < hi && __ldg(a.values + p) == x;
+}
+
+// Warp-collective: caches the longest suffix lists keyed by levels below L
+// (the prefix is sf/sidx).  Lists already cached stay in their slots.
+__device__ void cache_suffix_lists(const JoinArgs &a, const JQuery *__restrict__ Q, uint32_t L,
+                                   const uint32_t *sidx, const ListCache &lc) {
+  const uint32_t lane = lane_id();
+  const uint32_t n = Q->n, ne = Q->n_enum;
+  if (ne >= n || n > QV) return;
+  const uint32_t b0 = Q->lv[ne].back_base, b1 = Q->lv[n - 1].back_base + Q->lv[n - 1].nback;
+  uint64_t my_lo = 0, my_hi = 0, my_len = 0;
+  if (b1 > b0 && lane < b1 - b0 && inb(a, SITE_BACK, (uint64_t)b0 + lane, a.n_backs)) {
+    const JBack *b = a.backs + b0 + lane;
+    const uint32_t kl = b->lvl;
+    if (kl < L) {
+      table_range(a, b, sidx[kl], my_lo, my_hi);
+      const uint64_t len = my_hi - my_lo;
+      if (len >= 4 && len <= LIST_CACHE_CAP) my_len = len;
+    }
+  }
+  uint64_t pick_lo[LIST_CACHE_SLOTS], pick_hi[LIST_CACHE_SLOTS];
+#pragma unroll
+  for (int k = 0; k < (int)LIST_CACHE_SLOTS; ++k) {
+    uint64_t best = my_len;
+    uint32_t bl = lane;
+#pragma unroll
+    for (int d = 16; d; d >>= 1) {
+      const uint64_t ob = __shfl_xor_sync(FULL, best, d);
+      const uint32_t ol = __shfl_xor_sync(FULL, bl, d);
+      if (ob > best || (ob == best && ol < bl)) {
+        best = ob;
+        bl = ol;
+      }
+    }
+    pick_lo[k] = __shfl_sync(FULL, my_lo, bl);
+    pick_hi[k] = best ? __shfl_sync(FULL, my_hi, bl) : pick_lo[k];
+    if (lane == bl) my_len = 0;  // the next round picks another list
+  }
+  // keep what is cached already; fill the other picks into the free slots
+  uint32_t used = 0;
+#pragma unroll
+  for (int k = 0; k < (int)LIST_CACHE_SLOTS; ++k) {
+    const int s = cache_slot(lc, pick_lo[k], pick_hi[k]);
+    if (s >= 0) used |= 1u << s;
+  }
+#pragma unroll
+  for (int k = 0; k < (int)LIST_CACHE_SLOTS; ++k) {
+    if (pick_hi[k] <= pick_lo[k] || cache_slot(lc, pick_lo[k], pick_hi[k]) >= 0) continue;
+    const uint32_t free_slots = ~used & ((1u << LIST_CACHE_SLOTS) - 1u);
+    if (!free_slots) break;
+    const uint32_t s = __ffs(free_slots) - 1;
+    used |= 1u << s;
+    uint32_t *dst = lc.buf + s * LIST_CACHE_CAP;
+    const uint32_t len = (uint32_t)(pick_hi[k] - pick_lo[k]);
+    for (uint32_t j = lane; j < len; j += 32) dst[j] = __ldg(a.values + pick_lo[k] + j);
+    __syncwarp();
+    if (lane == 0) {
+      lc.tag[2 * s] = pick_lo[k];
+      lc.tag[2 * s + 1] = pick_hi[k];
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Count mode, closed-form suffix.  The suffix levels form an independent set
 // of the query graph, so once the prefix is matched each suffix level's
 // candidates are fixed: A_i = intersection of its backward lists minus the
@@ -192,6 +296,7 @@ struct LaneCtx {
   const JQuery *Q;
   uint32_t L, w, widx;
   const uint32_t *sf, *sidx;
+  ListCache lc;
 };
 
 __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
@@ -214,10 +319,76 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
 }
 
 
+// Lists of one subset, at most three: ranges computed once, cached lists read
+// from shared memory, the others searched from a moving start.
+__device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
+                                       uint32_t nl, uint32_t dup_mask, Stats &st, bool &heavy) {
+  uint64_t lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0, lo2 = 0, hi2 = 0;
+  lane_list(a, x, first, members, 0, lo0, hi0);
+  if (nl > 1) lane_list(a, x, first, members, 1, lo1, hi1);
+  if (nl > 2) lane_list(a, x, first, members, 2, lo2, hi2);
+  // the shortest list is scanned; the other two (oa, ob) are probed
+  uint64_t slo = lo0, shi = hi0, alo = lo1, ahi = hi1, blo = lo2, bhi = hi2;
+  if (nl > 1 && hi1 - lo1 < shi - slo) {
+    slo = lo1; shi = hi1; alo = lo0; ahi = hi0;
+  }
+  if (nl > 2 && hi2 - lo2 < shi - slo) {
+    blo = slo; bhi = shi; slo = lo2; shi = hi2;
+  }
+  const uint64_t len = shi - slo;
+  const int ss = cache_slot(x.lc, slo, shi);
+  if (nl == 1) {
+    uint64_t c = len, cur = slo;
+    for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
+      const uint32_t j = __ffs(dm) - 1;
+      const uint32_t v = j == x.L ? x.w : x.sf[j];
+      cur = slo;
+      if (list_member(a, x.lc, ss, slo, shi, cur, v)) --c;
+    }
+    st.probes += __popc(dup_mask);
+    return c;
+  }
+  const int sa = cache_slot(x.lc, alo, ahi), sb = nl > 2 ? cache_slot(x.lc, blo, bhi) : 0;
+  // A lane intersects at most lane_scan_max entries by itself (8x that when
+  // the scanned and the probed lists are all in shared memory); longer
+  // intersections are deferred to the whole warp (warp_suffix_count).
+  const bool all_shared = ss >= 0 && sa >= 0 && sb >= 0;
+  if (len > (all_shared ? 8ull * a.lane_scan_max : (uint64_t)a.lane_scan_max)) {
+    heavy = true;
+    return 0;
+  }
+  uint64_t c = 0, ca = alo, cb = blo;
+  const uint32_t *sbuf = ss >= 0 ? x.lc.buf + ss * LIST_CACHE_CAP : nullptr;
+  for (uint64_t e0 = 0; e0 < len; e0 += 4) {
+    // four entries of the scanned list per step: their loads overlap
+    uint32_t vv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      vv[k] = e0 + k >= len ? 0u : sbuf ? sbuf[e0 + k] : __ldg(a.values + slo + e0 + k);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (e0 + k >= len) break;
+      const uint32_t v = vv[k];
+      bool ok = true;
+      for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
+        const uint32_t j = __ffs(dm) - 1;
+        ok = v != (j == x.L ? x.w : x.sf[j]);
+      }
+      if (ok) ok = list_member(a, x.lc, sa, alo, ahi, ca, v);
+      if (ok && nl > 2) ok = list_member(a, x.lc, sb, blo, bhi, cb, v);
+      c += ok;
+    }
+  }
+  st.scanned += len;
+  st.probes += len * (nl - 1);
+  return c;
+}
+
 __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
                                       uint32_t dup_mask, Stats &st, bool &heavy) {
   uint32_t nl = 0;
   for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[(first + __ffs(m) - 1) & 31u].nback;
+  if (nl <= 3) return lane_subset_count3(a, x, first, members, nl, dup_mask, st, heavy);
   uint32_t s = 0;
   uint64_t s_lo = 0, s_hi = 0;
   for (uint32_t i = 0; i < nl; ++i) {
@@ -228,16 +399,6 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
       s_lo = lo;
       s_hi = hi;
     }
-  }
-  if (nl == 1) {
-    uint64_t c = s_hi - s_lo;
-    for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
-      const uint32_t j = __ffs(dm) - 1;
-      const uint32_t v = j == x.L ? x.w : x.sf[j];
-      if (contains_u32(a.values, s_lo, s_hi, v)) --c;
-    }
-    st.probes += __popc(dup_mask);
-    return c;
   }
   // A lane intersects at most a.lane_scan_max source entries by itself;
   // longer intersections are deferred to the whole warp (warp_suffix_count).
@@ -257,7 +418,8 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
       if (i == s) continue;
       uint64_t lo, hi;
       lane_list(a, x, first, members, i, lo, hi);
-      ok = contains_u32(a.values, lo, hi, v);
+      uint64_t cur = lo;
+      ok = list_member(a, x.lc, cache_slot(x.lc, lo, hi), lo, hi, cur, v);
     }
     c += ok;
   }
@@ -333,9 +495,14 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   const uint64_t s_lo = __shfl_sync(FULL, my_lo, src), s_hi = __shfl_sync(FULL, my_hi, src);
   if (nl == 1) {
     bool hit = false;
-    if ((dup_mask >> lane) & 1u) hit = contains_u32(a.values, s_lo, s_hi, lane == x.L ? x.w : x.sf[lane]);
+    uint64_t cur = s_lo;
+    if ((dup_mask >> lane) & 1u)
+      hit = list_member(a, x.lc, cache_slot(x.lc, s_lo, s_hi), s_lo, s_hi, cur, lane == x.L ? x.w : x.sf[lane]);
     return (s_hi - s_lo) - (uint64_t)__popc(__ballot_sync(FULL, hit));
   }
+  // cached lists: the scanned one is read from, the probed ones searched in, shared memory
+  const int my_slot = lane < nl ? cache_slot(x.lc, my_lo, my_hi) : -1;
+  const int s_slot = __shfl_sync(FULL, my_slot, src);
   // Merge intersection: 32 entries of the shortest list per step (one per
   // lane) against coalesced 32-entry windows of every other list; list i's
   // read cursor lives in lane i.  A window that ends below the step's first
@@ -345,11 +512,19 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
     const uint64_t e = cp + lane;
     bool ok = e < s_hi;
-    const uint32_t v = ok ? __ldg(a.values + e) : 0xFFFFFFFFu;
+    const uint32_t v = !ok ? 0xFFFFFFFFu
+                           : s_slot >= 0 ? x.lc.buf[s_slot * LIST_CACHE_CAP + (uint32_t)(e - s_lo)]
+                                         : __ldg(a.values + e);
     const uint32_t last = (uint32_t)((s_hi - cp) < 32 ? (s_hi - cp - 1) : 31);
     const uint32_t vmin = __shfl_sync(FULL, v, 0), vmax = __shfl_sync(FULL, v, last);
     for (uint32_t i = 0; i < nl; ++i) {
       if (i == src) continue;
+      const int sl = __shfl_sync(FULL, my_slot, i);
+      if (sl >= 0) {
+        const uint32_t ln = (uint32_t)(__shfl_sync(FULL, my_hi, i) - __shfl_sync(FULL, my_lo, i));
+        ok = ok && smem_contains(x.lc.buf + sl * LIST_CACHE_CAP, ln, v);
+        continue;
+      }
       uint64_t bp = __shfl_sync(FULL, cur, i);
       const uint64_t be = __shfl_sync(FULL, my_hi, i);
       bool found = false;
@@ -436,38 +611,58 @@ __device__ uint64_t warp_suffix_count(const JoinArgs &a, const LaneCtx &x, Stats
 }
 
 // ---------------------------------------------------------------------------
-// Bounded MPMC queue (sequence-numbered cells).  Called by a whole warp;
-// lane 0 reserves, every lane writes its share, lane 0 publishes.
+// Donation queue: QUEUE_SUBQ bounded MPMC sub-queues of sequence-numbered
+// cells.  A push reserves a position with an atomic add on one sub-queue's
+// tail (a reservation cannot lose a race), writes the cell and publishes it;
+// a pop scans the sub-queues with all 32 lanes and takes a published cell
+// with a CAS on that sub-queue's head.  `pending` counts published tasks not
+// yet taken.  Called by a whole warp; lane 0 does the atomics.
 // ---------------------------------------------------------------------------
-__device__ bool queue_push(JControl *ctl, JTask *cells, uint32_t q, uint32_t lvl, uint32_t src, uint64_t begin,
-                           uint64_t end, uint64_t hs, const LaneState &c) {
+__device__ __forceinline__ uint32_t warp_global_id() {
+  return blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+}
+
+__device__ __forceinline__ JTask *queue_cell(const JoinArgs &a, uint32_t sq, unsigned long long pos) {
+  return a.queue + sq * QUEUE_SUBQ_CAP + (pos & (QUEUE_SUBQ_CAP - 1));
+}
+
+__device__ bool queue_push(const JoinArgs &a, uint32_t q, uint32_t lvl, uint32_t src, uint64_t begin, uint64_t end,
+                           uint64_t hs, const LaneState &c) {
   const uint32_t lane = lane_id();
+  JControl *ctl = a.ctl;
   unsigned long long slot = 0;
+  uint32_t sq = 0;
   int ok = 0;
   if (lane == 0) {
-    unsigned long long pos = ld_vol(&ctl->tail);
-    for (int tries = 0; tries < 32; ++tries) {
-      JTask *cell = cells + (pos & (TASK_CAP - 1));
-      const unsigned long long seq = ld_vol(&cell->seq);
-      const long long dif = (long long)seq - (long long)pos;
-      if (dif == 0) {
-        if (atomicCAS(&ctl->tail, pos, pos + 1) == pos) {
-          ok = 1;
-          slot = pos;
+    const uint32_t q0 = warp_global_id() % QUEUE_SUBQ;
+    for (uint32_t k = 0; k < 4; ++k) {
+      sq = (q0 + 37u * k) % QUEUE_SUBQ;
+      // head first: the tail read after it is never smaller
+      const unsigned long long h = ld_vol(&a.qends[sq].head), t = ld_vol(&a.qends[sq].tail);
+      if (t - h >= QUEUE_SUBQ_FILL) continue;
+      // A reserved position is never given back.  Its cell is free once the
+      // pop of the previous lap released it, which has happened unless more
+      // than QUEUE_SUBQ_CAP - QUEUE_SUBQ_FILL warps passed the check together;
+      // a wait that runs out stops the grid with an overflow error.
+      slot = atomicAdd(&a.qends[sq].tail, 1ull);
+      const JTask *cell = queue_cell(a, sq, slot);
+      ok = 1;
+      for (uint32_t spin = 0; ld_vol(&cell->seq) != slot; ++spin) {
+        if (spin >= 4096) {
+          set_error(&ctl->err, DERR_OVERFLOW);
+          ok = 0;
           break;
         }
-        pos = ld_vol(&ctl->tail);
-      } else if (dif < 0) {
-        break;  // full
-      } else {
-        pos = ld_vol(&ctl->tail);
+        __nanosleep(64);
       }
+      break;
     }
   }
   ok = __shfl_sync(FULL, ok, 0);
-  slot = __shfl_sync(FULL, slot, 0);
   if (!ok) return false;
-  JTask *cell = cells + (slot & (TASK_CAP - 1));
+  slot = __shfl_sync(FULL, slot, 0);
+  sq = __shfl_sync(FULL, sq, 0);
+  JTask *cell = queue_cell(a, sq, slot);
   if (lane < lvl) {
     cell->f[lane] = c.f;
     cell->idx[lane] = c.idx;
@@ -482,7 +677,10 @@ __device__ bool queue_push(JControl *ctl, JTask *cells, uint32_t q, uint32_t lvl
   }
   __threadfence();
   __syncwarp();
-  if (lane == 0) *reinterpret_cast<volatile unsigned long long *>(&cell->seq) = slot + 1;
+  if (lane == 0) {
+    *reinterpret_cast<volatile unsigned long long *>(&cell->seq) = slot + 1;
+    atomicAdd(&ctl->pending, 1ull);  // after publishing, before this warp's busy release
+  }
   return true;
 }
 
@@ -491,35 +689,57 @@ struct PoppedTask {
   uint64_t begin, end, hs;
 };
 
-__device__ bool queue_pop(JControl *ctl, JTask *cells, PoppedTask &t, LaneState &c) {
+// Takes one published task.  The caller raises `busy` and then lowers
+// `pending`, so that a task is always counted by one of the two.
+__device__ bool queue_pop(const JoinArgs &a, PoppedTask &t, LaneState &c) {
   const uint32_t lane = lane_id();
+  JControl *ctl = a.ctl;
+  const unsigned long long pend = __shfl_sync(FULL, lane == 0 ? ld_vol(&ctl->pending) : 0ull, 0);
+  if (!pend) return false;
+  // one bit per sub-queue that holds tasks, rotated to start at this warp's own
+  const uint32_t q0 = warp_global_id() % QUEUE_SUBQ;
+  uint32_t nonempty[QUEUE_SUBQ / 32];
+#pragma unroll
+  for (uint32_t r = 0; r < QUEUE_SUBQ / 32; ++r) {
+    const uint32_t sq = (q0 + 32 * r + lane) % QUEUE_SUBQ;
+    const unsigned long long h = ld_vol(&a.qends[sq].head), tl = ld_vol(&a.qends[sq].tail);
+    nonempty[r] = __ballot_sync(FULL, h < tl);
+  }
   unsigned long long slot = 0;
+  uint32_t sq_got = 0;
   int ok = 0;
   if (lane == 0) {
-    unsigned long long pos = ld_vol(&ctl->head);
-    for (int tries = 0; tries < 32; ++tries) {
-      JTask *cell = cells + (pos & (TASK_CAP - 1));
-      const unsigned long long seq = ld_vol(&cell->seq);
-      const long long dif = (long long)seq - (long long)(pos + 1);
-      if (dif == 0) {
-        if (atomicCAS(&ctl->head, pos, pos + 1) == pos) {
-          ok = 1;
-          slot = pos;
-          break;
+    uint32_t attempts = 0;
+    for (uint32_t r = 0; r < QUEUE_SUBQ / 32 && !ok && attempts < 8; ++r)
+      for (uint32_t bits = nonempty[r]; bits && !ok && attempts < 8; bits &= bits - 1, ++attempts) {
+        const uint32_t sq = (q0 + 32 * r + __ffs(bits) - 1) % QUEUE_SUBQ;
+        unsigned long long pos = ld_vol(&a.qends[sq].head);
+        for (int tries = 0; tries < 4; ++tries) {
+          const unsigned long long seq = ld_vol(&queue_cell(a, sq, pos)->seq);
+          const long long dif = (long long)seq - (long long)(pos + 1);
+          if (dif == 0) {
+            const unsigned long long prev = atomicCAS(&a.qends[sq].head, pos, pos + 1);
+            if (prev == pos) {
+              ok = 1;
+              slot = pos;
+              sq_got = sq;
+              break;
+            }
+            pos = prev;  // another warp took it: try the position after
+          } else if (dif < 0) {
+            break;  // empty, or the task at the head is not published yet
+          } else {
+            pos = ld_vol(&a.qends[sq].head);
+          }
         }
-        pos = ld_vol(&ctl->head);
-      } else if (dif < 0) {
-        break;  // empty
-      } else {
-        pos = ld_vol(&ctl->head);
       }
-    }
   }
   ok = __shfl_sync(FULL, ok, 0);
-  slot = __shfl_sync(FULL, slot, 0);
   if (!ok) return false;
+  slot = __shfl_sync(FULL, slot, 0);
+  sq_got = __shfl_sync(FULL, sq_got, 0);
   __threadfence();
-  JTask *cell = cells + (slot & (TASK_CAP - 1));
+  JTask *cell = queue_cell(a, sq_got, slot);
   t.q = __ldcg(&cell->q);
   t.lvl = __ldcg(&cell->lvl);
   t.src = __ldcg(&cell->src);
@@ -532,7 +752,7 @@ __device__ bool queue_pop(JControl *ctl, JTask *cells, PoppedTask &t, LaneState 
   }
   __syncwarp();
   __threadfence();
-  if (lane == 0) *reinterpret_cast<volatile unsigned long long *>(&cell->seq) = slot + TASK_CAP;
+  if (lane == 0) *reinterpret_cast<volatile unsigned long long *>(&cell->seq) = slot + QUEUE_SUBQ_CAP;
   return true;
 }
 
@@ -584,8 +804,15 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
   const uint32_t lane = lane_id();
   JControl *ctl = a.ctl;
   const uint64_t deadline = ctl->deadline_ns;
-  __shared__ uint32_t s_pref[8][2][QV];  // per warp: f and idx of the enumerated prefix
+  __shared__ uint32_t s_pref[JOIN_WARPS_PER_BLOCK][2][QV];  // per warp: f and idx of the enumerated prefix
+  __shared__ unsigned long long s_ctag[JOIN_WARPS_PER_BLOCK][2 * LIST_CACHE_SLOTS];
+  extern __shared__ uint32_t s_lcache[];  // JOIN_DYN_SMEM bytes: per warp LIST_CACHE_SLOTS lists
   uint32_t *sf = s_pref[threadIdx.x >> 5][0], *sidx = s_pref[threadIdx.x >> 5][1];
+  ListCache lc;
+  lc.buf = s_lcache + (threadIdx.x >> 5) * (LIST_CACHE_SLOTS * LIST_CACHE_CAP);
+  lc.tag = s_ctag[threadIdx.x >> 5];
+  if (lane < 2 * LIST_CACHE_SLOTS) lc.tag[lane] = 0ull;  // empty: no list has lo == hi == 0 and hi > lo
+  __syncwarp();
   LaneState c;
   c.f = 0; c.idx = 0; c.hs = 0; c.pos = 0; c.end = 0; c.cbase = 0; c.mask = 0; c.src = 0;
   Stats st;
@@ -650,6 +877,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
               x.widx = (uint32_t)rl;
               x.sf = sf;
               x.sidx = sidx;
+              x.lc = lc;
               cnt = lane_suffix_count(a, x, st, heavy);
               hq = q;
               hw = w0;
@@ -671,6 +899,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         x.widx = __shfl_sync(FULL, hidx, hl);
         x.sf = sf;
         x.sidx = sidx;
+        x.lc = lc;
         const uint64_t k = warp_suffix_count(a, x, st);
         if (lane == 0 && k) atomicAdd(&a.out[qh].count, (unsigned long long)k);
       }
@@ -732,10 +961,12 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
         // Only a warp that holds work counts as busy: pollers must not keep
         // `busy` above zero, or no poller could ever observe quiescence.
         PoppedTask t;
-        if (queue_pop(ctl, a.queue, t, c)) {
+        if (queue_pop(a, t, c)) {
           if (lane == 0) {
             atomicAdd(&ctl->busy, 1u);
             atomicSub(&ctl->idle, 1u);
+            __threadfence();  // busy is raised before pending drops
+            atomicAdd(&ctl->pending, ~0ull);
           }
           idle_registered = false;  // a finished donated task re-registers as idle below
           q = t.q;
@@ -757,11 +988,12 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
           }
           break;
         }
-        int leave = 0;
+        int leave = 0, pending = 0;
         if (lane == 0) {
           const unsigned int b = ld_vol(&ctl->busy);
-          __threadfence();  // the queue is read after `busy`
-          const bool empty = ld_vol(&ctl->head) >= ld_vol(&ctl->tail);
+          __threadfence();  // `pending` is read after `busy`
+          const bool empty = ld_vol(&ctl->pending) == 0;
+          pending = !empty;
           if (b == 0 && empty) leave = 1;
           if (ld_vol(&ctl->err) != DERR_NONE) leave = 1;
           if (globaltimer_ns() > deadline) {
@@ -770,6 +1002,8 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
           }
         }
         if (__shfl_sync(FULL, leave, 0)) break;
+        // tasks are published but other warps won them: retry soon
+        if (__shfl_sync(FULL, pending, 0)) backoff = 256;
         __nanosleep(backoff);
         backoff = backoff < 16384 ? backoff * 2 : 16384;
       }
@@ -865,7 +1099,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
             const uint64_t mid = rem + ((((end - rem) >> 1) + 31) & ~31ull);
             if (mid < end) {
               const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
-              if (queue_push(ctl, a.queue, q, lvl, src, mid, end, hsp, c)) {
+              if (queue_push(a, q, lvl, src, mid, end, hsp, c)) {
                 new_end = mid;
                 pushed = true;
               }
@@ -880,6 +1114,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
             sidx[lane] = c.idx;
           }
           __syncwarp();
+          if (lvl > 0) cache_suffix_lists(a, Q, lvl, sidx, lc);
           bool heavy = false;
           uint32_t widx = 0;
           if ((m >> lane) & 1u) {
@@ -890,10 +1125,23 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
             x.widx = widx = index_of(a, L, w);
             x.sf = sf;
             x.sidx = sidx;
+            x.lc = lc;
             lane_cnt += lane_suffix_count(a, x, st, heavy);
           }
-          // candidates whose intersections are long: the whole warp, one at a time
-          for (uint32_t hm = __ballot_sync(FULL, heavy); hm; hm &= hm - 1) {
+          // candidates whose intersections are long: the whole warp, one at a
+          // time, after handing all but one of them to idle warps (one task
+          // per candidate: the one-entry source range that holds it)
+          uint32_t hm = __ballot_sync(FULL, heavy);
+          if (hm & (hm - 1)) {
+            uint32_t give = __shfl_sync(FULL, lane == 0 ? ld_vol(&ctl->idle) : 0u, 0);
+            for (uint32_t left = __popc(hm) - 1; give && left; --give, --left) {
+              const uint32_t hl = 31 - __clz(hm);
+              if (!queue_push(a, q, lvl, src, pos + hl, pos + hl + 1, 0ull, c)) break;
+              hm &= ~(1u << hl);
+              pushed = true;
+            }
+          }
+          for (; hm; hm &= hm - 1) {
             const uint32_t hl = __ffs(hm) - 1;
             LaneCtx x;
             x.Q = Q;
@@ -902,6 +1150,7 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
             x.widx = __shfl_sync(FULL, widx, hl);
             x.sf = sf;
             x.sidx = sidx;
+            x.lc = lc;
             const uint64_t k = warp_suffix_count(a, x, st);
             if (lane == 0) lane_cnt += k;
           }
@@ -922,7 +1171,26 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
       // descend into the lowest remaining candidate
       const uint32_t b = __ffs(mask) - 1;
       const uint64_t cb = __shfl_sync(FULL, c.cbase, lvl);
-      if (lane == lvl) c.mask = mask & (mask - 1);
+      uint32_t rest = mask & (mask - 1);
+      // Each survivor of the chunk opens a subtree of its own: when another
+      // warp is idle, the upper half of the remaining survivors goes to the
+      // queue as the source range that holds them (the recipient evaluates
+      // that range again and finds the same survivors).
+      if (rest && lvl <= a.donate_max_level) {
+        const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->idle) > 0) : 0, 0);
+        if (idle_now) {
+          uint32_t upper = rest;
+          for (uint32_t k = __popc(rest) >> 1; k; --k) upper &= upper - 1;  // drop the lower half
+          const uint32_t s = __ffs(upper) - 1, hb = 31 - __clz(rest);
+          const uint32_t src = __shfl_sync(FULL, c.src, lvl);
+          const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
+          if (queue_push(a, q, lvl, src, cb + s, cb + hb + 1, hsp, c)) {
+            rest &= (1u << s) - 1u;
+            pushed = true;
+          }
+        }
+      }
+      if (lane == lvl) c.mask = rest;
       const uint32_t w = __ldg(a.values + cb + b);
       const uint32_t widx = index_of(a, L, w);
       const uint64_t hsp = MODE == MODE_COUNT ? 0ull : __shfl_sync(FULL, c.hs, lvl - 1);
@@ -991,9 +1259,14 @@ __global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
 
 // Zeroes the control block and the per-query outputs, resets the task queue
 // and sets the deadline; runs right before the join in the same graph.
-__global__ void join_prepare_kernel(JControl *ctl, JOut *out, uint32_t nquery, JTask *cells, uint64_t cap_ns) {
+__global__ void join_prepare_kernel(JControl *ctl, JOut *out, uint32_t nquery, JTask *cells, JQueueEnds *qends,
+                                    uint64_t cap_ns) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
-  for (uint32_t i = t; i < TASK_CAP; i += nt) cells[i].seq = i;
+  for (uint32_t i = t; i < TASK_CAP; i += nt) cells[i].seq = i & (QUEUE_SUBQ_CAP - 1);
+  for (uint32_t i = t; i < QUEUE_SUBQ; i += nt) {
+    qends[i].head = 0;
+    qends[i].tail = 0;
+  }
   unsigned long long *o = reinterpret_cast<unsigned long long *>(out);
   const uint32_t words = nquery * (uint32_t)(sizeof(JOut) / 8);
   for (uint32_t i = t; i < words; i += nt) o[i] = 0ull;
@@ -1005,20 +1278,36 @@ __global__ void join_prepare_kernel(JControl *ctl, JOut *out, uint32_t nquery, J
   }
 }
 
-int join_blocks_per_sm(uint32_t mode) {
-  int n = 0;
-  cudaError_t e;
-  if (mode == MODE_COUNT) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, join_kernel<MODE_COUNT>, 256, 0);
-  else if (mode == MODE_HASH) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, join_kernel<MODE_HASH>, 256, 0);
-  else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, join_kernel<MODE_ENUM>, 256, 0);
-  if (e != cudaSuccess || n <= 0) n = 1;
-  return n;
-}
-
 static void *join_fn(uint32_t mode) {
   if (mode == MODE_COUNT) return (void *)join_kernel<MODE_COUNT>;
   if (mode == MODE_HASH) return (void *)join_kernel<MODE_HASH>;
   return (void *)join_kernel<MODE_ENUM>;
+}
+
+// The list cache takes JOIN_DYN_SMEM of dynamic shared memory per block,
+// above the default 48 KiB limit: every join instance opts in once.
+static cudaError_t join_smem_optin() {
+  static cudaError_t done = [] {
+    for (uint32_t m : {MODE_COUNT, MODE_HASH, MODE_ENUM}) {
+      const cudaError_t e =
+          cudaFuncSetAttribute(join_fn(m), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JOIN_DYN_SMEM);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }();
+  return done;
+}
+
+int join_blocks_per_sm(uint32_t mode) {
+  int n = 0;
+  if (join_smem_optin() != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, join_fn(mode), JOIN_WARPS_PER_BLOCK * 32, JOIN_DYN_SMEM) !=
+          cudaSuccess ||
+      n <= 0) {
+    cudaGetLastError();
+    n = 1;
+  }
+  return n;
 }
 
 void destroy_join_graph(JoinGraph &jg) {
@@ -1033,8 +1322,9 @@ cudaError_t launch_join_graph(JoinGraph &jg, const JoinArgs &a, uint64_t cap_ns,
   JOut *out = a.out;
   uint32_t nq = a.nquery;
   JTask *cells = a.queue;
+  JQueueEnds *qends = a.qends;
   uint64_t cap = cap_ns;
-  void *prep_params[] = {&ctl, &out, &nq, &cells, &cap};
+  void *prep_params[] = {&ctl, &out, &nq, &cells, &qends, &cap};
   void *join_params[] = {&args};
   cudaKernelNodeParams pp = {};
   pp.func = (void *)join_prepare_kernel;
@@ -1044,9 +1334,11 @@ cudaError_t launch_join_graph(JoinGraph &jg, const JoinArgs &a, uint64_t cap_ns,
   cudaKernelNodeParams jp = {};
   jp.func = join_fn(a.mode);
   jp.gridDim = dim3(grid);
-  jp.blockDim = dim3(256);
+  jp.blockDim = dim3(JOIN_WARPS_PER_BLOCK * 32);
+  jp.sharedMemBytes = JOIN_DYN_SMEM;
   jp.kernelParams = join_params;
   cudaError_t e;
+  if ((e = join_smem_optin()) != cudaSuccess) return e;
   if (!jg.exec || jg.mode != a.mode || jg.grid != grid) {
     destroy_join_graph(jg);
     if ((e = cudaGraphCreate(&jg.graph, 0)) != cudaSuccess) return e;

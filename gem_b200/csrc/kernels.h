@@ -164,6 +164,11 @@ struct JBack {
   uint32_t nkeys;            // keys of the table (offsets has nkeys + 1 entries)
   const uint64_t *off;       // table offsets (absolute into the values array)
 };
+// Join: per-warp shared-memory cache of suffix lists (slots x entries).
+constexpr uint32_t LIST_CACHE_SLOTS = 2;
+constexpr uint32_t LIST_CACHE_CAP = 1024;
+constexpr uint32_t JOIN_WARPS_PER_BLOCK = 8;
+constexpr uint32_t JOIN_DYN_SMEM = JOIN_WARPS_PER_BLOCK * LIST_CACHE_SLOTS * LIST_CACHE_CAP * 4;
 constexpr uint32_t MAX_GROUPS = 16;   // label groups of a closed-form suffix
 constexpr uint32_t MAX_GROUP = 4;     // members of one group (15 subsets, 15 partitions)
 // Inclusion-exclusion term: coefficient in the high 32 bits (two's
@@ -196,7 +201,18 @@ struct JOut {                // per query, accumulated with atomics
   unsigned long long probes;     // binary-search and index probes
   unsigned long long pad[2];     // pad[0] != 0: some work of this query was abandoned
 };
-constexpr uint32_t TASK_CAP = 8192;  // donation queue cells
+// Donation queue: QUEUE_SUBQ sub-queues of QUEUE_SUBQ_CAP cells each, so
+// that thousands of polling warps spread their atomics over many lines.
+constexpr uint32_t QUEUE_SUBQ = 128;
+constexpr uint32_t QUEUE_SUBQ_CAP = 256;                    // power of two
+constexpr uint32_t TASK_CAP = QUEUE_SUBQ * QUEUE_SUBQ_CAP;  // donation queue cells
+// A push skips a sub-queue holding this many tasks; the other half of the
+// cells is room for the warps that passed the check at the same time.
+constexpr uint32_t QUEUE_SUBQ_FILL = QUEUE_SUBQ_CAP / 2;
+struct JQueueEnds {  // one sub-queue; head and tail on lines of their own
+  alignas(128) unsigned long long head;  // next position to take
+  alignas(128) unsigned long long tail;  // next position to reserve
+};
 struct JTask {
   unsigned long long seq;
   uint32_t q, lvl, src;      // query, level whose candidates are donated, source back entry
@@ -206,27 +222,31 @@ struct JTask {
   uint32_t f[QV];
   uint32_t idx[QV];
 };
-struct JControl {            // zeroed before every launch (except queue seq init)
-  unsigned long long lp_next;    // next root of the lane-parallel pool
-  unsigned long long root_next;
-  unsigned long long tail;
-  unsigned long long head;
-  unsigned int busy;
-  unsigned int idle;
-  unsigned int err;
+// Zeroed before every launch (except the queue cells' sequence numbers).
+// Every counter that many warps update or poll sits on a 128-byte line of
+// its own, so the atomics on one do not queue behind traffic to the others.
+struct JControl {
+  alignas(128) unsigned long long lp_next;    // next root of the lane-parallel pool
+  alignas(128) unsigned long long root_next;  // next root of the ordinary pool
+  alignas(128) unsigned long long pending;    // tasks published and not yet taken
+  alignas(128) unsigned int busy;             // warps holding work
+  alignas(128) unsigned int idle;             // warps waiting for donated work
+  alignas(128) unsigned long long emb_next;   // enumerate cursor
+  alignas(128) unsigned int err;              // read-mostly: error word, then cold fields
   unsigned int pad;
   unsigned long long deadline_ns;
-  unsigned long long emb_next;   // enumerate cursor
   unsigned long long bad_site;   // first failed bounds check: site id
   unsigned long long bad_value;  // ... the offending index
   unsigned long long bad_limit;  // ... and its limit
 };
+
 enum : uint32_t { MODE_COUNT = 0, MODE_HASH = 1, MODE_ENUM = 2 };
 struct JoinArgs {
   const JQuery *queries;
   uint32_t nquery;
   uint32_t mode;
   const JBack *backs;
+  JQueueEnds *qends;          // QUEUE_SUBQ sub-queue ends (cells in `queue`)
   const uint32_t *values;     // edge-table values of the whole wave
   const uint64_t *root_prefix; // nquery + 1 global root offsets
   // Lane-parallel root pool: queries whose only enumerated level is the root
