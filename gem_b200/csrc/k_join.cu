@@ -214,6 +214,38 @@ __device__ __forceinline__ bool list_member(const JoinArgs &a, const ListCache &
   return p < hi && __ldg(a.values + p) == x;
 }
 
+// Membership of up to 8 ascending keys in the sorted list [lo, hi) of the
+// values array: eight binary searches advance together, so every step issues
+// eight independent loads instead of one.  Returns a bit per key found
+// (bit k for key k, among the `n` valid keys); *cur moves to the lower bound
+// of the last key, where the next block of larger keys starts.
+__device__ __forceinline__ uint32_t list_member8(const JoinArgs &a, uint64_t &cur, uint64_t hi, const uint32_t (&v)[8],
+                                                 uint32_t n) {
+  const uint32_t *__restrict__ base = a.values + cur;
+  const uint32_t len = (uint32_t)(hi - cur);
+  uint32_t l[8], h[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    l[k] = 0;
+    h[k] = (uint32_t)k < n ? len : 0;
+  }
+  for (uint32_t span = len; span; span >>= 1) {  // ceil(log2(len + 1)) rounds
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (l[k] < h[k]) {
+        const uint32_t mid = (l[k] + h[k]) >> 1;
+        if (__ldg(base + mid) < v[k]) l[k] = mid + 1; else h[k] = mid;
+      }
+    }
+  }
+  uint32_t found = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if ((uint32_t)k < n && l[k] < len && __ldg(base + l[k]) == v[k]) found |= 1u << k;
+  if (n) cur += l[n - 1 < 8 ? n - 1 : 7];
+  return found;
+}
+
 // Warp-collective: caches the longest suffix lists keyed by levels below L
 // (the prefix is sf/sidx).  Lists already cached stay in their slots.
 __device__ void cache_suffix_lists(const JoinArgs &a, const JQuery *__restrict__ Q, uint32_t L,
@@ -359,25 +391,43 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
   }
   uint64_t c = 0, ca = alo, cb = blo;
   const uint32_t *sbuf = ss >= 0 ? x.lc.buf + ss * LIST_CACHE_CAP : nullptr;
-  for (uint64_t e0 = 0; e0 < len; e0 += 4) {
-    // four entries of the scanned list per step: their loads overlap
-    uint32_t vv[4];
+  for (uint64_t e0 = 0; e0 < len; e0 += 8) {
+    // eight entries of the scanned list per step; their loads, and the
+    // binary searches for them in global lists, overlap
+    const uint32_t n = len - e0 < 8 ? (uint32_t)(len - e0) : 8u;
+    uint32_t vv[8];
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      vv[k] = e0 + k >= len ? 0u : sbuf ? sbuf[e0 + k] : __ldg(a.values + slo + e0 + k);
+    for (int k = 0; k < 8; ++k)
+      vv[k] = (uint32_t)k >= n ? 0xFFFFFFFFu : sbuf ? sbuf[e0 + k] : __ldg(a.values + slo + e0 + k);
+    uint32_t okm = (1u << n) - 1u;
+    for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
+      const uint32_t j = __ffs(dm) - 1;
+      const uint32_t d = j == x.L ? x.w : x.sf[j];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (e0 + k >= len) break;
-      const uint32_t v = vv[k];
-      bool ok = true;
-      for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
-        const uint32_t j = __ffs(dm) - 1;
-        ok = v != (j == x.L ? x.w : x.sf[j]);
-      }
-      if (ok) ok = list_member(a, x.lc, sa, alo, ahi, ca, v);
-      if (ok && nl > 2) ok = list_member(a, x.lc, sb, blo, bhi, cb, v);
-      c += ok;
+      for (int k = 0; k < 8; ++k)
+        if (vv[k] == d) okm &= ~(1u << k);
     }
+    if (okm) {
+      if (sa >= 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (((okm >> k) & 1u) && !smem_contains(x.lc.buf + sa * LIST_CACHE_CAP, (uint32_t)(ahi - alo), vv[k]))
+            okm &= ~(1u << k);
+      } else {
+        okm &= list_member8(a, ca, ahi, vv, n);
+      }
+    }
+    if (okm && nl > 2) {
+      if (sb >= 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (((okm >> k) & 1u) && !smem_contains(x.lc.buf + sb * LIST_CACHE_CAP, (uint32_t)(bhi - blo), vv[k]))
+            okm &= ~(1u << k);
+      } else {
+        okm &= list_member8(a, cb, bhi, vv, n);
+      }
+    }
+    c += __popc(okm);
   }
   st.scanned += len;
   st.probes += len * (nl - 1);
@@ -800,7 +850,7 @@ __device__ __forceinline__ void emit_last(const JoinArgs &a, const JQuery *__res
 }
 
 template <uint32_t MODE>
-__global__ void __launch_bounds__(256, 3) join_kernel(JoinArgs a) {
+__global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
   const uint32_t lane = lane_id();
   JControl *ctl = a.ctl;
   const uint64_t deadline = ctl->deadline_ns;
