@@ -43,7 +43,7 @@ EXPORTS = (
     "gem_hgraph_destroy", "gem_query_read_text", "gem_query_write_text", "gem_gen_queries",
     "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
-    "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static",
+    "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static", "gem_set_schedule", "gem_get_schedule",
 )
 
 
@@ -62,6 +62,16 @@ class _Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("device_budget_bytes", C.c_uint64), ("pinned_budget_bytes", C.c_uint64),
                 ("ooc", C.c_int), ("time_cap_ms", C.c_uint32), ("index_kind", C.c_uint32),
                 ("admit_gb", C.c_uint32), ("reserved", C.c_uint32 * 5)]
+
+
+class _Schedule(C.Structure):
+    _fields_ = [("blocks_per_sm", C.c_uint32), ("donate_max_level", C.c_uint32), ("donate_min_lane", C.c_uint32),
+                ("donate_min_desc", C.c_uint32), ("root_batch_max", C.c_uint32), ("lane_scan_max", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
+
+
+SCHEDULE_FIELDS = ("blocks_per_sm", "donate_max_level", "donate_min_lane", "donate_min_desc", "root_batch_max",
+                   "lane_scan_max")
 
 
 class _Result(C.Structure):
@@ -115,6 +125,8 @@ def lib():
         L.gem_submit.argtypes = [vp, C.POINTER(_Query), C.c_int, u64p]
         L.gem_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Result), C.POINTER(C.c_int)]
         L.gem_autotune.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, C.c_uint32, u32p]
+        L.gem_set_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
+        L.gem_get_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
         L.gem_filter_static.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(_Query), C.c_uint32, u32p, vp,
                                         C.c_uint64, vp]
         _lib = L
@@ -378,6 +390,20 @@ class Context:
                                  "donate_min_lane": (sched >> 8) & 0xFFF, "root_batch_max": sched >> 20,
                                  "join_us": int(rep[3 * b + 2])}
         return out
+
+    def set_schedule(self, query_vertices, **fields):
+        """Pin the join schedule of a query-size bucket (fields of gem_schedule; 0 = default)."""
+        sc = _Schedule()
+        for k, v in fields.items():
+            if k not in SCHEDULE_FIELDS:
+                raise ValueError(f"unknown schedule field {k}")
+            setattr(sc, k, int(v))
+        _check(lib().gem_set_schedule(self._h, query_vertices, C.byref(sc)), self._h, "set_schedule")
+
+    def get_schedule(self, query_vertices):
+        sc = _Schedule()
+        _check(lib().gem_get_schedule(self._h, query_vertices, C.byref(sc)), self._h, "get_schedule")
+        return {k: int(getattr(sc, k)) for k in SCHEDULE_FIELDS}
 
     def submit(self, q, mode=MODE_COUNT):
         """Serving: returns a ticket, or None when admission is busy (retry later)."""

@@ -165,6 +165,14 @@ static void free_graph(gem_ctx *ctx) {
     cudaFree(ctx->graph_mem);
     ctx->device_bytes -= ctx->graph_bytes;
   }
+  if (ctx->vnh_mem) {
+    cudaFree(ctx->vnh_mem);
+    ctx->device_bytes -= ctx->vnh_bytes;
+  }
+  ctx->vnh_mem = nullptr;
+  ctx->vnh_bytes = 0;
+  ctx->vnh_off = nullptr;
+  ctx->vnh_slots = nullptr;
   ctx->graph_mem = nullptr;
   ctx->graph_bytes = 0;
   ctx->g = DevGraph();
@@ -258,6 +266,40 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   if (stride) launch_nlc(g, d_nlc, stride, ctx->s);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(ctx->s));
+  // Neighbourhood hash for arc tests in the join: in-core graphs only (it
+  // is read at random), and only when it fits the budget with a quarter of
+  // the remaining budget left for the waves; otherwise the join searches
+  // the sorted adjacency instead.
+  if (!ooc && na) {
+    std::vector<uint64_t> hoff(nv + 1);
+    uint64_t n_slots = 0;
+    for (uint32_t v = 0; v < nv; ++v) {
+      hoff[v] = n_slots;
+      const uint64_t d = hg->off[v + 1] - hg->off[v];
+      if (d) {
+        uint64_t size = 2;
+        while (size < 2 * d) size <<= 1;
+        n_slots += size;
+      }
+    }
+    hoff[nv] = n_slots;
+    const uint64_t b_hoff = al(8ull * (nv + 1)), b_slots = al(4ull * n_slots);
+    const uint64_t left = ctx->budget > ctx->device_bytes ? ctx->budget - ctx->device_bytes : 0;
+    char *hp = nullptr;
+    if (b_hoff + b_slots <= left - left / 4 && cudaMalloc(&hp, b_hoff + b_slots) == cudaSuccess) {
+      ctx->vnh_mem = hp;
+      ctx->vnh_bytes = b_hoff + b_slots;
+      ctx->device_bytes += ctx->vnh_bytes;
+      ctx->vnh_off = (const uint64_t *)hp;
+      ctx->vnh_slots = (const uint32_t *)(hp + b_hoff);
+      CU(cudaMemcpyAsync(hp, hoff.data(), 8ull * (nv + 1), cudaMemcpyHostToDevice, ctx->s));
+      launch_vnh_build(g, (const uint64_t *)hp, (uint32_t *)(hp + b_hoff), n_slots, ctx->s);
+      CU(cudaGetLastError());
+      CU(cudaStreamSynchronize(ctx->s));
+    } else {
+      cudaGetLastError();
+    }
+  }
   ctx->g = g;
   ctx->loaded = true;
   ctx->label_freq.assign(L, 0);
@@ -845,6 +887,8 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   a.root_batch_max = tu.root_batch_max ? tu.root_batch_max : 1;
   a.lane_scan_max = tu.lane_scan_max ? tu.lane_scan_max : 48;
   a.nv = ctx->g.nv;
+  a.vnh_off = ctx->vnh_off;
+  a.vnh_slots = ctx->vnh_slots;
   a.n_values = w.table_values;
   a.n_backs = (uint32_t)jb.size();
   a.n_terms = (uint32_t)terms.size();
@@ -1189,6 +1233,33 @@ extern "C" gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t
 // persistent grid, deepest level that donates work) with the lowest join
 // time on a sample of the caller's queries.
 // ---------------------------------------------------------------------------
+extern "C" gem_status gem_set_schedule(gem_ctx *ctx, uint32_t query_vertices, const gem_schedule *sched) {
+  if (!ctx || !sched || query_vertices == 0 || query_vertices > QV) return GEM_ERR_ARG;
+  if (ctx->server) return GEM_ERR_STATE;
+  Tune &t = ctx->tune[size_bucket(query_vertices)];
+  t = Tune();
+  t.blocks_per_sm = sched->blocks_per_sm;
+  t.donate_max_level = sched->donate_max_level;
+  t.donate_min_lane = sched->donate_min_lane;
+  t.donate_min_desc = sched->donate_min_desc;
+  t.root_batch_max = sched->root_batch_max;
+  t.lane_scan_max = sched->lane_scan_max;
+  return GEM_OK;
+}
+
+extern "C" gem_status gem_get_schedule(gem_ctx *ctx, uint32_t query_vertices, gem_schedule *sched) {
+  if (!ctx || !sched || query_vertices == 0 || query_vertices > QV) return GEM_ERR_ARG;
+  const Tune &t = ctx->tune[size_bucket(query_vertices)];
+  *sched = gem_schedule{};
+  sched->blocks_per_sm = t.blocks_per_sm;
+  sched->donate_max_level = t.donate_max_level;
+  sched->donate_min_lane = t.donate_min_lane;
+  sched->donate_min_desc = t.donate_min_desc;
+  sched->root_batch_max = t.root_batch_max;
+  sched->lane_scan_max = t.lane_scan_max;
+  return GEM_OK;
+}
+
 extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode, uint32_t trial_cap_ms,
                                    uint32_t *report) {
   if (!ctx || (n && !qs)) return GEM_ERR_ARG;

@@ -107,6 +107,10 @@ struct gem_ctx {
   bool loaded = false;
   gem::DevGraph g;
   char *graph_mem = nullptr;
+  char *vnh_mem = nullptr;           // neighbourhood hash (in-core graphs that fit)
+  uint64_t vnh_bytes = 0;
+  const uint64_t *vnh_off = nullptr;
+  const uint32_t *vnh_slots = nullptr;
   void *pinned_nbr = nullptr;        // out-of-core: mapped pinned adjacency
   uint64_t graph_bytes = 0;
   std::vector<uint64_t> label_freq;  // vertices per label

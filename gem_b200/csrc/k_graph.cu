@@ -67,6 +67,38 @@ void launch_nlc(const DevGraph &g, uint8_t *nlc, uint32_t stride, cudaStream_t s
 // ---------------------------------------------------------------------------
 // Exclusive scan: 2048 items per block (256 threads x 8 consecutive items).
 // ---------------------------------------------------------------------------
+// One warp per vertex inserts its neighbours into the vertex's table.
+__global__ void __launch_bounds__(256) vnh_build_kernel(const uint64_t *__restrict__ off,
+                                                        const uint32_t *__restrict__ nbr, uint32_t nv,
+                                                        const uint64_t *__restrict__ hoff, uint32_t *slots) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t u = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); u < nv; u += nw) {
+    const uint64_t b = hoff[u], size = hoff[u + 1] - b;
+    if (!size) continue;
+    const uint32_t lg = 63 - __clzll(size);
+    for (uint64_t i = off[u] + lane; i < off[u + 1]; i += 32) {
+      const uint32_t v = nbr[i];
+      uint64_t pos = (v * VNH_MULT) >> (64 - lg);
+      for (uint64_t k = 0; k < size; ++k) {  // size >= 2 deg: a free slot exists
+        const uint32_t prev = atomicCAS(slots + b + pos, VNH_EMPTY, v);
+        if (prev == VNH_EMPTY || prev == v) break;
+        pos = (pos + 1) & (size - 1);
+      }
+    }
+  }
+}
+
+void launch_vnh_build(const DevGraph &g, const uint64_t *hoff, uint32_t *slots, uint64_t n_slots,
+                      cudaStream_t s) {
+  if (!g.nv || !n_slots) return;
+  cudaMemsetAsync(slots, 0xFF, n_slots * 4, s);
+  uint64_t blocks = ((uint64_t)g.nv + 7) / 8;
+  if (blocks > 148ull * 32) blocks = 148ull * 32;
+  count_launch();
+  vnh_build_kernel<<<(uint32_t)blocks, 256, 0, s>>>(g.off, g.nbr, g.nv, hoff, slots);
+}
+
 constexpr uint32_t SCAN_T = 256, SCAN_I = 8, SCAN_B = SCAN_T * SCAN_I;
 
 template <ScanInput K>

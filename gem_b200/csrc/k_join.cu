@@ -98,7 +98,8 @@ __device__ __forceinline__ void table_range(const JoinArgs &a, const JBack *b, u
 // Per back entry i (lane i < nback): the list T(u_j -> u_L)[idx_j] as the
 // absolute range [lo, hi) of the values array.
 __device__ __forceinline__ void level_ranges(const JoinArgs &a, const JLevel *__restrict__ L, const LaneState &c,
-                                             uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi) {
+                                             uint32_t &nback, uint64_t &my_lo, uint64_t &my_hi,
+                                             uint32_t *my_kv = nullptr) {
   const uint32_t lane = lane_id();
   nback = L->nback;
   uint32_t klvl = 0;
@@ -108,6 +109,8 @@ __device__ __forceinline__ void level_ranges(const JoinArgs &a, const JLevel *__
     klvl = b->lvl & 31u;
   }
   const uint32_t kidx = __shfl_sync(FULL, c.idx, klvl);
+  const uint32_t kv = __shfl_sync(FULL, c.f, klvl);  // the list's key vertex f(u_j)
+  if (my_kv) *my_kv = kv;
   my_lo = my_hi = 0;
   if (b) table_range(a, b, kidx, my_lo, my_hi);
 }
@@ -138,17 +141,80 @@ __device__ __forceinline__ void level_lists(const JoinArgs &a, const JLevel *__r
 // Evaluates the chunk [cpos, min(cpos + 32, end)) of the source list: a lane's
 // candidate survives if every other backward list contains it and no earlier
 // same-label level holds it.  Returns the ballot; *w receives the lane's value.
+// ---------------------------------------------------------------------------
+// Arc tests through the neighbourhood hash.  A list T(u_j -> u_s)[f_j] is
+// N(f_j) restricted to C(u_s), so a value already known to be in C(u_s) is
+// in the list exactly when (f_j, value) is an arc.
+// ---------------------------------------------------------------------------
+struct VnhRow {
+  uint64_t b, mask;  // first slot and size - 1 of the vertex's table (mask ~0: no neighbours)
+  uint32_t shift;    // 64 - log2(size)
+};
+
+__device__ __forceinline__ VnhRow vnh_row(const JoinArgs &a, uint32_t u) {
+  VnhRow r;
+  r.b = __ldg(a.vnh_off + u);
+  const uint64_t size = __ldg(a.vnh_off + u + 1) - r.b;
+  r.mask = size ? size - 1 : ~0ull;
+  r.shift = size ? 1 + __clzll(size) : 0;
+  return r;
+}
+
+__device__ __forceinline__ bool vnh_has(const JoinArgs &a, const VnhRow &r, uint32_t v) {
+  if (r.mask == ~0ull) return false;
+  uint64_t pos = (v * VNH_MULT) >> r.shift;
+  for (uint64_t k = 0; k <= r.mask; ++k) {
+    const uint32_t x = __ldg(a.vnh_slots + r.b + pos);
+    if (x == v) return true;
+    if (x == VNH_EMPTY) return false;
+    pos = (pos + 1) & r.mask;
+  }
+  return false;
+}
+
+// Arc tests of up to 8 keys (the bits of `want`) against one vertex's
+// table; the probes of all keys are issued together.  Returns the keys found.
+__device__ __forceinline__ uint32_t vnh_has8(const JoinArgs &a, const VnhRow &r, const uint32_t (&v)[8],
+                                             uint32_t want) {
+  if (r.mask == ~0ull) return 0;
+  uint64_t pos[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) pos[k] = (v[k] * VNH_MULT) >> r.shift;
+  uint32_t found = 0, open = want;
+  for (uint64_t step = 0; open && step <= r.mask; ++step) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if ((open >> k) & 1u) {
+        const uint32_t x = __ldg(a.vnh_slots + r.b + pos[k]);
+        if (x == v[k]) {
+          found |= 1u << k;
+          open &= ~(1u << k);
+        } else if (x == VNH_EMPTY) {
+          open &= ~(1u << k);
+        } else {
+          pos[k] = (pos[k] + 1) & r.mask;
+        }
+      }
+    }
+  }
+  return found;
+}
+
+// The source list and the probed lists all lie in C(u_L), so with the
+// neighbourhood hash a probe of list T(u_j -> u_L)[f_j] is the arc test
+// (f_j, w); without it, a binary search of the list.
 __device__ __forceinline__ uint32_t eval_chunk(const JoinArgs &a, uint64_t cpos, uint64_t end, uint32_t nback,
-                                               uint32_t src, uint64_t my_lo, uint64_t my_hi, uint32_t dup_mask,
-                                               const LaneState &c, uint32_t *w_out, Stats &st) {
+                                               uint32_t src, uint64_t my_lo, uint64_t my_hi, uint32_t my_kv,
+                                               uint32_t dup_mask, const LaneState &c, uint32_t *w_out, Stats &st) {
   const uint32_t lane = lane_id();
   const uint64_t e = cpos + lane;
   bool ok = e < end;
   uint32_t w = ok ? __ldg(a.values + e) : 0u;
   for (uint32_t i = 0; i < nback; ++i) {
     const uint64_t lo = __shfl_sync(FULL, my_lo, i), hi = __shfl_sync(FULL, my_hi, i);
+    const uint32_t kv = __shfl_sync(FULL, my_kv, i);
     if (i == src) continue;
-    if (ok) ok = contains_u32(a.values, lo, hi, w);
+    if (ok) ok = a.vnh_off ? vnh_has(a, vnh_row(a, kv), w) : contains_u32(a.values, lo, hi, w);
   }
   for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
     const uint32_t j = __ffs(dm) - 1;
@@ -329,13 +395,19 @@ struct LaneCtx {
   uint32_t L, w, widx;
   const uint32_t *sf, *sidx;
   ListCache lc;
+  uint64_t deadline;  // device time cap (%globaltimer ns)
 };
 
+// List li of the subset `members` of a suffix group: its range, its key
+// vertex (f of the key level) and the level of the member it belongs to.
 __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
-                                          uint32_t li, uint64_t &lo, uint64_t &hi) {
+                                          uint32_t li, uint64_t &lo, uint64_t &hi, uint32_t &kv, uint32_t &mlvl) {
   lo = hi = 0;
+  kv = 0;
+  mlvl = first;
   for (uint32_t m = members; m; m &= m - 1) {
-    const JLevel *M = &x.Q->lv[(first + __ffs(m) - 1) & 31u];
+    mlvl = (first + __ffs(m) - 1) & 31u;
+    const JLevel *M = &x.Q->lv[mlvl];
     const uint32_t nb = M->nback;
     if (li < nb) {
       if (!inb(a, SITE_BACK, (uint64_t)M->back_base + li, a.n_backs)) return;
@@ -343,6 +415,7 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
       const uint32_t kl = b->lvl;
       if (!inb(a, SITE_KEYLVL, kl, (uint64_t)x.L + 1)) return;
       const uint32_t kidx = kl == x.L ? x.widx : x.sidx[kl];
+      kv = kl == x.L ? x.w : x.sf[kl];
       table_range(a, b, kidx, lo, hi);
       return;
     }
@@ -350,50 +423,73 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
   }
 }
 
+// v in list (range [lo, hi), key vertex kv, member level ml) when v is known
+// to be in C(u of level vl): an arc test, plus a candidate test when the
+// list belongs to another member.
+__device__ __forceinline__ bool vnh_list_has(const JoinArgs &a, const JQuery *Q, uint32_t kv, uint32_t ml,
+                                             uint32_t vl, uint32_t v) {
+  if (!vnh_has(a, vnh_row(a, kv), v)) return false;
+  return ml == vl || (v < a.nv && rank_member(Q->lv[ml].rb, v));
+}
+
 
 // Lists of one subset, at most three: ranges computed once, cached lists read
-// from shared memory, the others searched from a moving start.
+// from shared memory, the others probed through the neighbourhood hash (or
+// searched from a moving start without it).
 __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint32_t first, uint32_t members,
                                        uint32_t nl, uint32_t dup_mask, Stats &st, bool &heavy) {
   uint64_t lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0, lo2 = 0, hi2 = 0;
-  lane_list(a, x, first, members, 0, lo0, hi0);
-  if (nl > 1) lane_list(a, x, first, members, 1, lo1, hi1);
-  if (nl > 2) lane_list(a, x, first, members, 2, lo2, hi2);
-  // the shortest list is scanned; the other two (oa, ob) are probed
+  uint32_t kv0 = 0, kv1 = 0, kv2 = 0, ml0 = 0, ml1 = 0, ml2 = 0;
+  lane_list(a, x, first, members, 0, lo0, hi0, kv0, ml0);
+  if (nl > 1) lane_list(a, x, first, members, 1, lo1, hi1, kv1, ml1);
+  if (nl > 2) lane_list(a, x, first, members, 2, lo2, hi2, kv2, ml2);
+  // the shortest list (s) is scanned; the other two (a, b) are probed
   uint64_t slo = lo0, shi = hi0, alo = lo1, ahi = hi1, blo = lo2, bhi = hi2;
+  uint32_t skv = kv0, sml = ml0, akv = kv1, aml = ml1, bkv = kv2, bml = ml2;
   if (nl > 1 && hi1 - lo1 < shi - slo) {
-    slo = lo1; shi = hi1; alo = lo0; ahi = hi0;
+    slo = lo1; shi = hi1; skv = kv1; sml = ml1;
+    alo = lo0; ahi = hi0; akv = kv0; aml = ml0;
   }
   if (nl > 2 && hi2 - lo2 < shi - slo) {
-    blo = slo; bhi = shi; slo = lo2; shi = hi2;
+    blo = slo; bhi = shi; bkv = skv; bml = sml;
+    slo = lo2; shi = hi2; skv = kv2; sml = ml2;
   }
   const uint64_t len = shi - slo;
   const int ss = cache_slot(x.lc, slo, shi);
+  const bool hash = a.vnh_off != nullptr;
   if (nl == 1) {
     uint64_t c = len, cur = slo;
     for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
-      const uint32_t v = j == x.L ? x.w : x.sf[j];
+      const uint32_t v = j == x.L ? x.w : x.sf[j];  // a prefix vertex: not known to be in C(u_s)
       cur = slo;
-      if (list_member(a, x.lc, ss, slo, shi, cur, v)) --c;
+      const bool in = ss >= 0 || !hash ? list_member(a, x.lc, ss, slo, shi, cur, v)
+                                       : vnh_list_has(a, x.Q, skv, sml, ~0u, v);
+      if (in) --c;
     }
     st.probes += __popc(dup_mask);
     return c;
   }
   const int sa = cache_slot(x.lc, alo, ahi), sb = nl > 2 ? cache_slot(x.lc, blo, bhi) : 0;
-  // A lane intersects at most lane_scan_max entries by itself (8x that when
-  // the scanned and the probed lists are all in shared memory); longer
-  // intersections are deferred to the whole warp (warp_suffix_count).
+  // A lane intersects at most lane_scan_max entries by itself (2x that with
+  // the neighbourhood hash, 8x when the scanned and the probed lists are all
+  // in shared memory); longer intersections are deferred to the whole warp
+  // (warp_suffix_count).
   const bool all_shared = ss >= 0 && sa >= 0 && sb >= 0;
-  if (len > (all_shared ? 8ull * a.lane_scan_max : (uint64_t)a.lane_scan_max)) {
+  const uint64_t lim = all_shared ? 8ull * a.lane_scan_max : hash ? 2ull * a.lane_scan_max : a.lane_scan_max;
+  if (len > lim) {
     heavy = true;
     return 0;
   }
+  VnhRow ra = {}, rb = {};
+  if (hash && sa < 0) ra = vnh_row(a, akv);
+  if (hash && nl > 2 && sb < 0) rb = vnh_row(a, bkv);
+  const uint64_t *rba = x.Q->lv[aml & 31u].rb, *rbb = x.Q->lv[bml & 31u].rb;
   uint64_t c = 0, ca = alo, cb = blo;
   const uint32_t *sbuf = ss >= 0 ? x.lc.buf + ss * LIST_CACHE_CAP : nullptr;
   for (uint64_t e0 = 0; e0 < len; e0 += 8) {
-    // eight entries of the scanned list per step; their loads, and the
-    // binary searches for them in global lists, overlap
+    // eight entries of the scanned list per step; their loads, and their
+    // probes of the other lists, overlap
     const uint32_t n = len - e0 < 8 ? (uint32_t)(len - e0) : 8u;
     uint32_t vv[8];
 #pragma unroll
@@ -413,6 +509,13 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
         for (int k = 0; k < 8; ++k)
           if (((okm >> k) & 1u) && !smem_contains(x.lc.buf + sa * LIST_CACHE_CAP, (uint32_t)(ahi - alo), vv[k]))
             okm &= ~(1u << k);
+      } else if (hash) {
+        okm &= vnh_has8(a, ra, vv, okm);
+        if (aml != sml) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if (((okm >> k) & 1u) && !(vv[k] < a.nv && rank_member(rba, vv[k]))) okm &= ~(1u << k);
+        }
       } else {
         okm &= list_member8(a, ca, ahi, vv, n);
       }
@@ -423,6 +526,13 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
         for (int k = 0; k < 8; ++k)
           if (((okm >> k) & 1u) && !smem_contains(x.lc.buf + sb * LIST_CACHE_CAP, (uint32_t)(bhi - blo), vv[k]))
             okm &= ~(1u << k);
+      } else if (hash) {
+        okm &= vnh_has8(a, rb, vv, okm);
+        if (bml != sml) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if (((okm >> k) & 1u) && !(vv[k] < a.nv && rank_member(rbb, vv[k]))) okm &= ~(1u << k);
+        }
       } else {
         okm &= list_member8(a, cb, bhi, vv, n);
       }
@@ -439,15 +549,17 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   uint32_t nl = 0;
   for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[(first + __ffs(m) - 1) & 31u].nback;
   if (nl <= 3) return lane_subset_count3(a, x, first, members, nl, dup_mask, st, heavy);
-  uint32_t s = 0;
+  uint32_t s = 0, s_ml = 0;
   uint64_t s_lo = 0, s_hi = 0;
   for (uint32_t i = 0; i < nl; ++i) {
     uint64_t lo, hi;
-    lane_list(a, x, first, members, i, lo, hi);
+    uint32_t kv, ml;
+    lane_list(a, x, first, members, i, lo, hi, kv, ml);
     if (i == 0 || hi - lo < s_hi - s_lo) {
       s = i;
       s_lo = lo;
       s_hi = hi;
+      s_ml = ml;
     }
   }
   // A lane intersects at most a.lane_scan_max source entries by itself;
@@ -467,9 +579,12 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
     for (uint32_t i = 0; i < nl && ok; ++i) {
       if (i == s) continue;
       uint64_t lo, hi;
-      lane_list(a, x, first, members, i, lo, hi);
+      uint32_t kv, ml;
+      lane_list(a, x, first, members, i, lo, hi, kv, ml);
+      const int slot = cache_slot(x.lc, lo, hi);
       uint64_t cur = lo;
-      ok = list_member(a, x.lc, cache_slot(x.lc, lo, hi), lo, hi, cur, v);
+      ok = slot >= 0 || !a.vnh_off ? list_member(a, x.lc, slot, lo, hi, cur, v)
+                                   : vnh_list_has(a, x.Q, kv, ml, s_ml, v);
     }
     c += ok;
   }
@@ -529,7 +644,8 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   for (uint32_t m = members; m; m &= m - 1) nl += x.Q->lv[(first + __ffs(m) - 1) & 31u].nback;
   nl = nl < 32 ? nl : 32;
   uint64_t my_lo = 0, my_hi = 0;
-  if (lane < nl) lane_list(a, x, first, members, lane, my_lo, my_hi);
+  uint32_t my_kv = 0, my_ml = 0;
+  if (lane < nl) lane_list(a, x, first, members, lane, my_lo, my_hi, my_kv, my_ml);
   uint64_t best = lane < nl ? my_hi - my_lo : ~0ull;
   uint32_t bl = lane;
 #pragma unroll
@@ -543,11 +659,17 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   }
   const uint32_t src = bl;
   const uint64_t s_lo = __shfl_sync(FULL, my_lo, src), s_hi = __shfl_sync(FULL, my_hi, src);
+  const uint32_t s_kv = __shfl_sync(FULL, my_kv, src), s_ml = __shfl_sync(FULL, my_ml, src);
+  const bool hash = a.vnh_off != nullptr;
   if (nl == 1) {
     bool hit = false;
     uint64_t cur = s_lo;
-    if ((dup_mask >> lane) & 1u)
-      hit = list_member(a, x.lc, cache_slot(x.lc, s_lo, s_hi), s_lo, s_hi, cur, lane == x.L ? x.w : x.sf[lane]);
+    if ((dup_mask >> lane) & 1u) {
+      const uint32_t v = lane == x.L ? x.w : x.sf[lane];  // a prefix vertex: not known to be in C(u_s)
+      const int slot = cache_slot(x.lc, s_lo, s_hi);
+      hit = slot >= 0 || !hash ? list_member(a, x.lc, slot, s_lo, s_hi, cur, v)
+                               : vnh_list_has(a, x.Q, s_kv, s_ml, ~0u, v);
+    }
     return (s_hi - s_lo) - (uint64_t)__popc(__ballot_sync(FULL, hit));
   }
   // cached lists: the scanned one is read from, the probed ones searched in, shared memory
@@ -559,7 +681,17 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   // entry is skipped with one binary search (galloping for skewed lengths).
   uint64_t cur = my_lo;
   uint64_t cnt = 0;
+  uint32_t step = 0;
   for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
+    // long merges look at the time cap every 64 steps; past it, the partial
+    // count is dropped with the query (the error word marks it incomplete)
+    if ((++step & 63u) == 0) {
+      const int late = __shfl_sync(FULL, lane == 0 ? (int)(globaltimer_ns() > x.deadline) : 0, 0);
+      if (late) {
+        if (lane == 0) set_error(&a.ctl->err, DERR_TIMEOUT);
+        break;
+      }
+    }
     const uint64_t e = cp + lane;
     bool ok = e < s_hi;
     const uint32_t v = !ok ? 0xFFFFFFFFu
@@ -573,6 +705,11 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
       if (sl >= 0) {
         const uint32_t ln = (uint32_t)(__shfl_sync(FULL, my_hi, i) - __shfl_sync(FULL, my_lo, i));
         ok = ok && smem_contains(x.lc.buf + sl * LIST_CACHE_CAP, ln, v);
+        continue;
+      }
+      if (hash) {  // v is in C(u of the scanned list's member)
+        const uint32_t kv = __shfl_sync(FULL, my_kv, i), ml = __shfl_sync(FULL, my_ml, i);
+        ok = ok && vnh_list_has(a, x.Q, kv, ml, s_ml, v);
         continue;
       }
       uint64_t bp = __shfl_sync(FULL, cur, i);
@@ -928,6 +1065,7 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
               x.sf = sf;
               x.sidx = sidx;
               x.lc = lc;
+              x.deadline = deadline;
               cnt = lane_suffix_count(a, x, st, heavy);
               hq = q;
               hw = w0;
@@ -950,6 +1088,7 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
         x.sf = sf;
         x.sidx = sidx;
         x.lc = lc;
+        x.deadline = deadline;
         const uint64_t k = warp_suffix_count(a, x, st);
         if (lane == 0 && k) atomicAdd(&a.out[qh].count, (unsigned long long)k);
       }
@@ -1109,7 +1248,7 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
           --lvl;
           continue;
         }
-        if ((++iter & 63u) == 0) {
+        if ((++iter & 3u) == 0) {
           int stop = 0;
           if (lane == 0) {
             if (ld_vol(&ctl->err) != DERR_NONE) stop = 1;
@@ -1123,12 +1262,12 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
             break;
           }
         }
-        uint32_t nb;
+        uint32_t nb, kv;
         uint64_t lo, hi;
-        level_ranges(a, L, c, nb, lo, hi);
+        level_ranges(a, L, c, nb, lo, hi, &kv);
         const uint32_t src = __shfl_sync(FULL, c.src, lvl);
         uint32_t w;
-        const uint32_t m = eval_chunk(a, pos, end, nb, src, lo, hi, L->dup_mask, c, &w, st);
+        const uint32_t m = eval_chunk(a, pos, end, nb, src, lo, hi, kv, L->dup_mask, c, &w, st);
         if (MODE != MODE_COUNT && lvl == n - 1) {
           emit_last<MODE>(a, Q, lvl, m, w, c, lane_cnt, lane_hash);
           if (lane == lvl) c.pos = pos + 32;
@@ -1167,6 +1306,7 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
           if (lvl > 0) cache_suffix_lists(a, Q, lvl, sidx, lc);
           bool heavy = false;
           uint32_t widx = 0;
+          uint64_t my_cnt = 0;
           if ((m >> lane) & 1u) {
             LaneCtx x;
             x.Q = Q;
@@ -1176,21 +1316,29 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
             x.sf = sf;
             x.sidx = sidx;
             x.lc = lc;
-            lane_cnt += lane_suffix_count(a, x, st, heavy);
+            x.deadline = deadline;
+            my_cnt = lane_suffix_count(a, x, st, heavy);
           }
-          // candidates whose intersections are long: the whole warp, one at a
-          // time, after handing all but one of them to idle warps (one task
-          // per candidate: the one-entry source range that holds it)
+          // Candidates whose intersections are long are counted by the whole
+          // warp, one at a time.  When another warp is idle, the chunk's
+          // positions from the first of the upper half of them on go to the
+          // queue as one task; the recipient evaluates them all again, so
+          // their counts here are dropped.
           uint32_t hm = __ballot_sync(FULL, heavy);
-          if (hm & (hm - 1)) {
-            uint32_t give = __shfl_sync(FULL, lane == 0 ? ld_vol(&ctl->idle) : 0u, 0);
-            for (uint32_t left = __popc(hm) - 1; give && left; --give, --left) {
-              const uint32_t hl = 31 - __clz(hm);
-              if (!queue_push(a, q, lvl, src, pos + hl, pos + hl + 1, 0ull, c)) break;
-              hm &= ~(1u << hl);
-              pushed = true;
-            }
+          uint64_t give_end = end < pos + 32 ? end : pos + 32;  // chunk positions not yet given away
+          while (hm & (hm - 1)) {
+            const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&ctl->idle) > 0) : 0, 0);
+            if (!idle_now) break;
+            uint32_t upper = hm;
+            for (uint32_t k = __popc(hm) >> 1; k; --k) upper &= upper - 1;
+            const uint32_t s0 = __ffs(upper) - 1;
+            if (!queue_push(a, q, lvl, src, pos + s0, give_end, 0ull, c)) break;
+            hm &= (1u << s0) - 1u;
+            if (lane >= s0 && pos + lane < give_end) my_cnt = 0;
+            give_end = pos + s0;
+            pushed = true;
           }
+          lane_cnt += my_cnt;
           for (; hm; hm &= hm - 1) {
             const uint32_t hl = __ffs(hm) - 1;
             LaneCtx x;
@@ -1201,6 +1349,7 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
             x.sf = sf;
             x.sidx = sidx;
             x.lc = lc;
+            x.deadline = deadline;
             const uint64_t k = warp_suffix_count(a, x, st);
             if (lane == 0) lane_cnt += k;
           }

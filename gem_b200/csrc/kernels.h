@@ -37,6 +37,17 @@ struct DevGraph {
 void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s);
 void launch_nlc(const DevGraph &g, uint8_t *nlc, uint32_t stride, cudaStream_t s);
 
+// Neighbourhood hash: per vertex u an open-addressed table of its neighbours
+// (u32, empty = VNH_EMPTY) of a power of two >= 2 deg(u) slots, at
+// [hoff[u], hoff[u+1]) of `slots`; a neighbour v starts probing at the top
+// log2(size) bits of v * VNH_MULT and moves to the next slot (mod size).
+// It answers "is (u, v) an arc" in about one load, where a binary search of
+// a hub's sorted adjacency takes a dozen dependent loads.
+constexpr uint32_t VNH_EMPTY = 0xFFFFFFFFu;
+constexpr uint64_t VNH_MULT = 0x9E3779B97F4A7C15ull;
+void launch_vnh_build(const DevGraph &g, const uint64_t *hoff, uint32_t *slots, uint64_t n_slots,
+                      cudaStream_t s);
+
 // ---------------------------------------------------------------------------
 // Generic exclusive scan (u64 results, n + 1 entries: out[n] = total)
 // ---------------------------------------------------------------------------
@@ -269,6 +280,8 @@ struct JoinArgs {
   uint32_t root_batch_max;   // largest root batch a warp takes at once
   uint32_t lane_scan_max;    // longest intersection one lane does alone
   uint32_t nv;               // data vertices (bounds of rank-bitmap probes)
+  const uint64_t *vnh_off;   // neighbourhood hash offsets (nv + 1), or null: binary search
+  const uint32_t *vnh_slots;
   uint64_t n_values;         // entries of `values`
   uint32_t n_backs;          // entries of `backs`
   uint32_t n_terms;          // entries of `terms`

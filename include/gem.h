@@ -211,6 +211,30 @@ gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n,
 gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode,
                         uint32_t trial_cap_ms, uint32_t *report);
 
+/* Join schedule of one query-size bucket (no counterpart in the reference).
+ * Every field 0 means the library default.  blocks_per_sm caps the
+ * persistent grid; donate_max_level is the deepest level that hands work to
+ * idle warps; donate_min_lane / donate_min_desc are the smallest halves of a
+ * level's unread candidates worth handing over (last enumerated level /
+ * other levels); root_batch_max caps the roots a warp takes at once;
+ * lane_scan_max is the longest intersection a single lane works through
+ * before the whole warp takes it over. */
+typedef struct gem_schedule {
+  uint32_t blocks_per_sm;
+  uint32_t donate_max_level;
+  uint32_t donate_min_lane;
+  uint32_t donate_min_desc;
+  uint32_t root_batch_max;
+  uint32_t lane_scan_max;
+  uint32_t reserved[2];
+} gem_schedule;
+
+/* Set / read the schedule used for waves whose largest query has
+ * query_vertices vertices (its bucket: <=4, <=8, <=12, <=16, <=24, <=32).
+ * gem_autotune overwrites the schedules of the buckets it tunes. */
+gem_status gem_set_schedule(gem_ctx *ctx, uint32_t query_vertices, const gem_schedule *sched);
+gem_status gem_get_schedule(gem_ctx *ctx, uint32_t query_vertices, gem_schedule *sched);
+
 /* Embedding hash of one embedding f (f[u] = data vertex of query vertex u):
  * h = mix(sum_u mix(f[u] | u << 32)) with mix the splitmix64 finaliser of
  * (x + 0x9E3779B97F4A7C15); GEM_MODE_HASH reports the sum of h over all
