@@ -67,11 +67,11 @@ class _Opts(C.Structure):
 class _Schedule(C.Structure):
     _fields_ = [("blocks_per_sm", C.c_uint32), ("donate_max_level", C.c_uint32), ("donate_min_lane", C.c_uint32),
                 ("donate_min_desc", C.c_uint32), ("root_batch_max", C.c_uint32), ("lane_scan_max", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("split_blocks", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 SCHEDULE_FIELDS = ("blocks_per_sm", "donate_max_level", "donate_min_lane", "donate_min_desc", "root_batch_max",
-                   "lane_scan_max")
+                   "lane_scan_max", "split_blocks")
 
 
 class _Result(C.Structure):

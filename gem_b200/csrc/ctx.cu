@@ -791,6 +791,24 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
       J.term_count[gi] = (uint32_t)p.groups[gi].terms.size();
       terms.insert(terms.end(), p.groups[gi].terms.begin(), p.groups[gi].terms.end());
     }
+    // balanced lane-level counting: at most FLAT_MAX_VALUES subset values per
+    // prefix match, each an intersection of at most three lists
+    {
+      uint32_t nval = 0, nscan = 0;
+      bool ok = mode == GEM_MODE_COUNT && J.n_groups > 0;
+      for (uint32_t gi = 0; ok && gi < J.n_groups; ++gi) {
+        const uint32_t first = J.grp_first[gi], gs = J.grp_size[gi];
+        for (uint32_t S = 1; ok && S < (1u << gs); ++S) {
+          uint32_t nl = 0;
+          for (uint32_t b = 0; b < gs; ++b)
+            if (S & (1u << b)) nl += (uint32_t)p.back[first + b].size();
+          ok = nl >= 1 && nl <= 3;
+          ++nval;
+          nscan += nl >= 2;
+        }
+      }
+      J.flat = ok && nval <= FLAT_MAX_VALUES ? nval | (nscan << 8) : 0;
+    }
     J.root_u = p.order[0];
     const uint32_t r0 = w.row_base[qi] + p.order[0];
     J.root_cand = w.d_cand + w.c_base[r0];
@@ -886,6 +904,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   a.donate_min_desc = tu.donate_min_desc ? tu.donate_min_desc : 1;
   a.root_batch_max = tu.root_batch_max ? tu.root_batch_max : 1;
   a.lane_scan_max = tu.lane_scan_max ? tu.lane_scan_max : 48;
+  a.flat_donate_blocks = tu.split_blocks ? tu.split_blocks : 32;
   a.nv = ctx->g.nv;
   a.vnh_off = ctx->vnh_off;
   a.vnh_slots = ctx->vnh_slots;
@@ -1244,6 +1263,7 @@ extern "C" gem_status gem_set_schedule(gem_ctx *ctx, uint32_t query_vertices, co
   t.donate_min_desc = sched->donate_min_desc;
   t.root_batch_max = sched->root_batch_max;
   t.lane_scan_max = sched->lane_scan_max;
+  t.split_blocks = sched->split_blocks;
   return GEM_OK;
 }
 
@@ -1257,6 +1277,7 @@ extern "C" gem_status gem_get_schedule(gem_ctx *ctx, uint32_t query_vertices, ge
   sched->donate_min_desc = t.donate_min_desc;
   sched->root_batch_max = t.root_batch_max;
   sched->lane_scan_max = t.lane_scan_max;
+  sched->split_blocks = t.split_blocks;
   return GEM_OK;
 }
 
@@ -1278,10 +1299,11 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
   if (occ > 1) bps_c.push_back((uint32_t)occ - 1);
   if (occ > 2) bps_c.push_back((uint32_t)(occ + 1) / 2);
   struct Sched {
-    uint32_t dm, dml, rb, lsm, dmd;
+    uint32_t dm, dml, rb, lsm, dmd, split;
   };
-  const Sched sched_c[8] = {{30, 32, 1, 48, 1},  {6, 32, 1, 48, 1},  {2, 32, 1, 48, 1},  {30, 256, 1, 48, 1},
-                            {30, 32, 4, 48, 1},  {30, 32, 1, 8, 1},  {30, 32, 1, 160, 1}, {30, 32, 1, 48, 32}};
+  const Sched sched_c[8] = {{30, 32, 1, 48, 1, 32}, {6, 32, 1, 48, 1, 32},  {2, 32, 1, 48, 1, 32},
+                            {30, 256, 1, 48, 1, 32}, {30, 32, 4, 48, 1, 32}, {30, 32, 1, 8, 1, 32},
+                            {30, 32, 1, 160, 1, 32}, {30, 32, 1, 48, 1, 64}};
   const uint32_t saved_cap = ctx->opts.time_cap_ms;
   ctx->opts.time_cap_ms = trial_cap_ms ? trial_cap_ms : 2000;
   gem_status st = GEM_OK;
@@ -1297,6 +1319,7 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
         ctx->tune[b].root_batch_max = sc.rb;
         ctx->tune[b].lane_scan_max = sc.lsm;
         ctx->tune[b].donate_min_desc = sc.dmd;
+        ctx->tune[b].split_blocks = sc.split;
         Wave w;
         w.q = byb[b];
         ctx->arena.reset();
@@ -1313,6 +1336,7 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
           best.root_batch_max = sc.rb;
           best.lane_scan_max = sc.lsm;
           best.donate_min_desc = sc.dmd;
+          best.split_blocks = sc.split;
           best.best_ms = (float)cost;
         }
       }

@@ -88,6 +88,7 @@ struct Tune {
   uint32_t root_batch_max = 0;    // 0 = library default
   uint32_t lane_scan_max = 0;     // 0 = library default
   uint32_t donate_min_desc = 0;   // 0 = library default
+  uint32_t split_blocks = 0;      // 0 = library default
   float best_ms = 0;
 };
 // Buckets by query size: <=4, <=8, <=12, <=16, <=24, <=32 vertices.

@@ -269,6 +269,32 @@ __device__ __forceinline__ bool smem_contains(const uint32_t *b, uint32_t n, uin
   return lo < n && b[lo] == x;
 }
 
+// Membership of up to 8 keys (the bits of `want`) in the sorted shared-memory
+// list b[0, n): the eight binary searches advance together.
+__device__ __forceinline__ uint32_t smem_member8(const uint32_t *b, uint32_t n, const uint32_t (&v)[8],
+                                                 uint32_t want) {
+  uint32_t l[8], h[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    l[k] = 0;
+    h[k] = ((want >> k) & 1u) ? n : 0;
+  }
+  for (uint32_t span = n; span; span >>= 1) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (l[k] < h[k]) {
+        const uint32_t mid = (l[k] + h[k]) >> 1;
+        if (b[mid] < v[k]) l[k] = mid + 1; else h[k] = mid;
+      }
+    }
+  }
+  uint32_t found = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (((want >> k) & 1u) && l[k] < n && b[l[k]] == v[k]) found |= 1u << k;
+  return found;
+}
+
 // x in list [lo, hi): from the cache slot when there is one, else by binary
 // search of the values array from *cur (lists are probed in ascending x, so
 // the search start only moves forward).
@@ -505,10 +531,7 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
     }
     if (okm) {
       if (sa >= 0) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-          if (((okm >> k) & 1u) && !smem_contains(x.lc.buf + sa * LIST_CACHE_CAP, (uint32_t)(ahi - alo), vv[k]))
-            okm &= ~(1u << k);
+        okm &= smem_member8(x.lc.buf + sa * LIST_CACHE_CAP, (uint32_t)(ahi - alo), vv, okm);
       } else if (hash) {
         okm &= vnh_has8(a, ra, vv, okm);
         if (aml != sml) {
@@ -522,10 +545,7 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
     }
     if (okm && nl > 2) {
       if (sb >= 0) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-          if (((okm >> k) & 1u) && !smem_contains(x.lc.buf + sb * LIST_CACHE_CAP, (uint32_t)(bhi - blo), vv[k]))
-            okm &= ~(1u << k);
+        okm &= smem_member8(x.lc.buf + sb * LIST_CACHE_CAP, (uint32_t)(bhi - blo), vv, okm);
       } else if (hash) {
         okm &= vnh_has8(a, rb, vv, okm);
         if (bml != sml) {
@@ -591,6 +611,276 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   st.scanned += s_hi - s_lo;
   st.probes += (s_hi - s_lo) * (nl - 1);
   return c;
+}
+
+// ---------------------------------------------------------------------------
+// Balanced lane-level counting.  The per-lane form above makes a chunk last as
+// long as its longest intersection; here every intersection of the chunk
+// (one per prefix match and subset with two or more lists) becomes a job in
+// the warp's shared memory, the jobs' blocks of 8 scanned entries are dealt
+// round-robin to all 32 lanes, and each lane then assembles its own prefix
+// match's inclusion-exclusion from the job results.  Used when the
+// neighbourhood hash exists and the query's suffix has at most
+// FLAT_MAX_VALUES subset values of at most three lists each.
+// ---------------------------------------------------------------------------
+struct FJob {
+  uint64_t s;     // scanned list: start in the values array, or offset in its cache slot
+  uint64_t ra;    // probe a: cached list length, or hash row start | log2(size) << 58 (63: no neighbours)
+  uint64_t rb;    // probe b (three-list subsets)
+  uint32_t len;   // scanned entries
+  uint32_t w;     // the prefix match's vertex at level L (a duplicate candidate)
+  uint32_t dup;   // earlier same-label levels
+  uint32_t meta;  // bit 0: three lists; bits 1-2 / 3-4 / 5-6: cache slot + 1 (0: none) of the
+                  // scanned list and of probes a, b; bits 7-11 / 12-16 / 17-21: their member levels
+};
+static_assert(sizeof(FJob) == FLAT_JOB_BYTES, "job record size");
+
+__device__ __forceinline__ uint64_t flat_probe_word(const JoinArgs &a, int slot, uint64_t lo, uint64_t hi,
+                                                    uint32_t kv) {
+  if (slot >= 0) return hi - lo;
+  const uint64_t b = __ldg(a.vnh_off + kv), size = __ldg(a.vnh_off + kv + 1) - b;
+  const uint64_t lg = size ? 63 - __clzll(size) : 63;
+  return b | (lg << 58);
+}
+
+// Keys among `want` that are in the probed list (word from flat_probe_word,
+// slot1 = cache slot + 1 or 0); keys come from a list of member level sml.
+__device__ __forceinline__ uint32_t flat_probe8(const JoinArgs &a, const JQuery *Q, const ListCache &lc,
+                                                uint32_t slot1, uint64_t word, uint32_t ml, uint32_t sml,
+                                                const uint32_t (&vv)[8], uint32_t want) {
+  if (!want) return 0;
+  if (slot1) return smem_member8(lc.buf + (slot1 - 1) * LIST_CACHE_CAP, (uint32_t)word, vv, want);
+  const uint64_t lg = word >> 58;
+  if (lg == 63) return 0;
+  VnhRow r;
+  r.b = word & ((1ull << 58) - 1);
+  r.mask = (1ull << lg) - 1;
+  r.shift = 64 - (uint32_t)lg;
+  uint32_t f = vnh_has8(a, r, vv, want);
+  if (ml != sml) {
+    const uint64_t *rbm = Q->lv[ml & 31u].rb;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (((f >> k) & 1u) && !(vv[k] < a.nv && rank_member(rbm, vv[k]))) f &= ~(1u << k);
+  }
+  return f;
+}
+
+__device__ bool queue_push(const JoinArgs &a, uint32_t q, uint32_t lvl, uint32_t src, uint64_t begin, uint64_t end,
+                           uint64_t hs, const LaneState &c);
+
+// Where the chunk came from, for handing part of it to idle warps.
+struct FlatOrigin {
+  uint32_t q, src;
+  uint64_t pos, end;  // the chunk's positions [pos, end) in the source list
+};
+
+// Counts the suffix completions of the chunk's prefix matches (lanes in m);
+// *my_cnt receives this lane's.  While the chunk holds more than
+// a.flat_donate_blocks blocks and other warps are idle, the positions of the
+// upper half of its work go to the queue (the recipient evaluates them
+// again) and their lanes count nothing here.  Returns false, having done
+// nothing, when the chunk's jobs do not fit the job table.
+__device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx &x, uint32_t m, char *fbase,
+                                                const FlatOrigin &org, const LaneState &c, bool &pushed,
+                                                Stats &st, uint64_t &my_cnt) {
+  const uint32_t lane = lane_id();
+  const JQuery *Q = x.Q;
+  const uint32_t nscan = (Q->flat >> 8) & 0xFFu;
+  const uint32_t nact = __popc(m);
+  if (nact * nscan > FLAT_MAX_JOBS) return false;
+  FJob *jobs = reinterpret_cast<FJob *>(fbase);
+  uint32_t *res = reinterpret_cast<uint32_t *>(fbase + FLAT_MAX_JOBS * FLAT_JOB_BYTES);
+  uint32_t *start = res + FLAT_MAX_JOBS;
+  bool act = (m >> lane) & 1u;
+  const uint32_t jbase = __popc(m & ((1u << lane) - 1u)) * nscan;
+  const uint32_t ng = Q->n_groups < MAX_GROUPS ? Q->n_groups : MAX_GROUPS;
+  uint64_t val[FLAT_MAX_VALUES] = {0, 0, 0, 0};
+  uint32_t my_blocks = 0;
+  // ---- stage 1: this lane's subsets: one-list values directly, the others as jobs
+  if (act) {
+    uint32_t k = 0, jn = 0;
+    for (uint32_t g = 0; g < ng; ++g) {
+      const uint32_t first = Q->grp_first[g], gs = Q->grp_size[g] < MAX_GROUP ? Q->grp_size[g] : MAX_GROUP;
+      const uint32_t dup = Q->lv[first & 31u].dup_mask;
+      for (uint32_t S = 1; S < (1u << gs) && k < FLAT_MAX_VALUES; ++S, ++k) {
+        uint32_t nl = 0;
+        for (uint32_t mm = S; mm; mm &= mm - 1) nl += Q->lv[(first + __ffs(mm) - 1) & 31u].nback;
+        uint64_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        uint32_t kv[3] = {0, 0, 0}, ml[3] = {0, 0, 0};
+#pragma unroll
+        for (uint32_t i = 0; i < 3; ++i)
+          if (i < nl) lane_list(a, x, first, S, i, lo[i], hi[i], kv[i], ml[i]);
+        uint32_t s = 0;
+        uint64_t best = hi[0] - lo[0];
+        if (nl > 1 && hi[1] - lo[1] < best) {
+          s = 1;
+          best = hi[1] - lo[1];
+        }
+        if (nl > 2 && hi[2] - lo[2] < best) s = 2;
+        const uint64_t slo = s == 0 ? lo[0] : s == 1 ? lo[1] : lo[2];
+        const uint64_t shi = s == 0 ? hi[0] : s == 1 ? hi[1] : hi[2];
+        const uint32_t skv = s == 0 ? kv[0] : s == 1 ? kv[1] : kv[2];
+        const uint32_t sml = s == 0 ? ml[0] : s == 1 ? ml[1] : ml[2];
+        const int ss = cache_slot(x.lc, slo, shi);
+        if (nl == 1) {
+          uint64_t cnt = shi - slo, cur = slo;
+          for (uint32_t dm = dup; dm; dm &= dm - 1) {
+            const uint32_t j = __ffs(dm) - 1;
+            const uint32_t v = j == x.L ? x.w : x.sf[j];
+            cur = slo;
+            const bool in = ss >= 0 ? list_member(a, x.lc, ss, slo, shi, cur, v)
+                                    : vnh_list_has(a, Q, skv, sml, ~0u, v);
+            if (in) --cnt;
+          }
+          val[k] = cnt;
+          continue;
+        }
+        // the probed lists: the two (or one) other than s
+        const uint32_t ia = s == 0 ? 1 : 0, ib = s == 2 ? 1 : 2;
+        const uint64_t alo = ia == 0 ? lo[0] : lo[1], ahi = ia == 0 ? hi[0] : hi[1];
+        const uint64_t blo = ib == 1 ? lo[1] : lo[2], bhi = ib == 1 ? hi[1] : hi[2];
+        const uint32_t akv = ia == 0 ? kv[0] : kv[1], bkv = ib == 1 ? kv[1] : kv[2];
+        const uint32_t aml = ia == 0 ? ml[0] : ml[1], bml = ib == 1 ? ml[1] : ml[2];
+        const int sa = cache_slot(x.lc, alo, ahi), sb = nl > 2 ? cache_slot(x.lc, blo, bhi) : -1;
+        FJob jb;
+        jb.s = ss >= 0 ? 0 : slo;
+        jb.len = (uint32_t)(shi - slo);
+        jb.ra = flat_probe_word(a, sa, alo, ahi, akv);
+        jb.rb = nl > 2 ? flat_probe_word(a, sb, blo, bhi, bkv) : 0;
+        jb.w = x.w;
+        jb.dup = dup;
+        jb.meta = (nl > 2 ? 1u : 0u) | ((uint32_t)(ss + 1) << 1) | ((uint32_t)(sa + 1) << 3) |
+                  ((uint32_t)(sb + 1) << 5) | ((sml & 31u) << 7) | ((aml & 31u) << 12) | ((bml & 31u) << 17);
+        jobs[jbase + jn] = jb;
+        res[jbase + jn] = 0;
+        my_blocks += (jb.len + 7) >> 3;
+        st.scanned += jb.len;
+        st.probes += (uint64_t)jb.len * (nl - 1);
+        ++jn;
+      }
+    }
+  }
+  // ---- job starts (in blocks of 8 entries): lanes in order, jobs in order
+  uint32_t incl = my_blocks;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(FULL, incl, d);
+    if (lane >= (uint32_t)d) incl += o;
+  }
+  uint32_t total = __shfl_sync(FULL, incl, 31);
+  // hand the upper half of the work to idle warps while the chunk is large
+  uint32_t keep = m;  // lanes whose prefix matches stay here
+  uint64_t give_end = org.end;
+  while (total > a.flat_donate_blocks) {
+    const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&a.ctl->idle) > 0) : 0, 0);
+    if (!idle_now) break;
+    // first lane whose work starts at or after half of the remaining blocks
+    const uint32_t cut = __ballot_sync(FULL, ((keep >> lane) & 1u) && incl - my_blocks >= total / 2);
+    if (!cut) break;
+    const uint32_t s0 = __ffs(cut) - 1;
+    if (!queue_push(a, org.q, x.L, org.src, org.pos + s0, give_end, 0ull, c)) break;
+    pushed = true;
+    give_end = org.pos + s0;
+    keep &= (1u << s0) - 1u;
+    total = __shfl_sync(FULL, incl - my_blocks, s0);
+  }
+  act = act && ((keep >> lane) & 1u);
+  if (act) {
+    uint32_t b = incl - my_blocks;
+    for (uint32_t i = 0; i < nscan; ++i) {
+      start[jbase + i] = b;
+      b += (jobs[jbase + i].len + 7) >> 3;
+    }
+  }
+  const uint32_t njobs = __popc(keep) * nscan;
+  if (lane == 0) start[njobs] = total;
+  __syncwarp();
+  // ---- stage 2: blocks dealt round-robin; partial counts summed per job
+  uint32_t cur_j = 0, cur_c = 0;
+  for (uint32_t base = 0; base < total; base += 32) {
+    if (((base >> 5) & 63u) == 63u) {
+      const int late = __shfl_sync(FULL, lane == 0 ? (int)(globaltimer_ns() > x.deadline) : 0, 0);
+      if (late) {
+        if (lane == 0) set_error(&a.ctl->err, DERR_TIMEOUT);
+        break;
+      }
+    }
+    const uint32_t bid = base + lane;
+    if (bid < total) {
+      uint32_t lo = cur_j, hi = njobs;  // last job whose start <= bid (jobs only move forward)
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (start[mid] <= bid) lo = mid; else hi = mid;
+      }
+      if (lo != cur_j && cur_c) {
+        atomicAdd(res + cur_j, cur_c);
+        cur_c = 0;
+      }
+      cur_j = lo;
+      const FJob jb = jobs[lo];
+      const uint32_t off = (bid - start[lo]) << 3;
+      const uint32_t n = jb.len - off < 8 ? jb.len - off : 8u;
+      const uint32_t ss1 = (jb.meta >> 1) & 3u, sa1 = (jb.meta >> 3) & 3u, sb1 = (jb.meta >> 5) & 3u;
+      const uint32_t sml = (jb.meta >> 7) & 31u, aml = (jb.meta >> 12) & 31u, bml = (jb.meta >> 17) & 31u;
+      uint32_t vv[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        vv[k] = (uint32_t)k >= n ? 0xFFFFFFFFu
+                : ss1 ? x.lc.buf[(ss1 - 1) * LIST_CACHE_CAP + off + k]
+                      : __ldg(a.values + jb.s + off + k);
+      uint32_t okm = (1u << n) - 1u;
+      for (uint32_t dm = jb.dup; dm; dm &= dm - 1) {
+        const uint32_t j = __ffs(dm) - 1;
+        const uint32_t d = j == x.L ? jb.w : x.sf[j];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (vv[k] == d) okm &= ~(1u << k);
+      }
+      okm &= flat_probe8(a, Q, x.lc, sa1, jb.ra, aml, sml, vv, okm);
+      if (jb.meta & 1u) okm &= flat_probe8(a, Q, x.lc, sb1, jb.rb, bml, sml, vv, okm);
+      cur_c += __popc(okm);
+    }
+  }
+  if (cur_c) atomicAdd(res + cur_j, cur_c);
+  __syncwarp();
+  // ---- stage 3: this lane's inclusion-exclusion
+  my_cnt = 0;
+  if (act) {
+    uint64_t total_c = 1;
+    uint32_t k = 0, jn = 0;
+    for (uint32_t g = 0; g < ng && k < FLAT_MAX_VALUES; ++g) {
+      const uint32_t first = Q->grp_first[g], gs = Q->grp_size[g] < MAX_GROUP ? Q->grp_size[g] : MAX_GROUP;
+      uint64_t sv[4] = {0, 0, 0, 0};
+      for (uint32_t S = 1; S < (1u << gs) && k < FLAT_MAX_VALUES; ++S, ++k) {
+        uint32_t nl = 0;
+        for (uint32_t mm = S; mm; mm &= mm - 1) nl += Q->lv[(first + __ffs(mm) - 1) & 31u].nback;
+        const uint64_t v = nl == 1 ? val[k] : (uint64_t)res[jbase + jn++];
+        if (S < 4) sv[S] = v;
+      }
+      if (gs == 1) {
+        total_c *= sv[1];
+        continue;
+      }
+      uint64_t G = 0;
+      const uint32_t tb = Q->term_base[g], tc = Q->term_count[g];
+      for (uint32_t t = 0; t < tc; ++t) {
+        if (!inb(a, SITE_TERM, (uint64_t)tb + t, a.n_terms)) break;
+        const uint64_t term = __ldg(a.terms + tb + t);
+        uint64_t prod = (uint64_t)(int64_t)(int32_t)(uint32_t)(term >> 32);
+        const uint32_t blocks = (uint32_t)term;
+        for (uint32_t b = 0; b < MAX_GROUP; ++b) {
+          const uint32_t mk = (blocks >> (4 * b)) & 15u;
+          if (!mk) break;
+          prod *= mk < 4 ? sv[mk] : 0ull;
+        }
+        G += prod;
+      }
+      total_c *= G;
+    }
+    my_cnt = total_c;
+  }
+  return true;
 }
 
 // Suffix completions of one lane's prefix match; sets `heavy` (and returns
@@ -996,7 +1286,9 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
   extern __shared__ uint32_t s_lcache[];  // JOIN_DYN_SMEM bytes: per warp LIST_CACHE_SLOTS lists
   uint32_t *sf = s_pref[threadIdx.x >> 5][0], *sidx = s_pref[threadIdx.x >> 5][1];
   ListCache lc;
-  lc.buf = s_lcache + (threadIdx.x >> 5) * (LIST_CACHE_SLOTS * LIST_CACHE_CAP);
+  // per warp: the list cache, then the balanced-counting job table
+  lc.buf = s_lcache + (threadIdx.x >> 5) * (LIST_CACHE_SLOTS * LIST_CACHE_CAP + FLAT_WARP_BYTES / 4);
+  char *fbuf = reinterpret_cast<char *>(lc.buf + LIST_CACHE_SLOTS * LIST_CACHE_CAP);
   lc.tag = s_ctag[threadIdx.x >> 5];
   if (lane < 2 * LIST_CACHE_SLOTS) lc.tag[lane] = 0ull;  // empty: no list has lo == hi == 0 and hi > lo
   __syncwarp();
@@ -1304,10 +1596,30 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
           }
           __syncwarp();
           if (lvl > 0) cache_suffix_lists(a, Q, lvl, sidx, lc);
+          bool flat_done = false;
+          if (Q->flat && a.vnh_off) {
+            LaneCtx x;
+            x.Q = Q;
+            x.L = lvl;
+            x.w = w;
+            x.widx = ((m >> lane) & 1u) ? index_of(a, L, w) : 0u;
+            x.sf = sf;
+            x.sidx = sidx;
+            x.lc = lc;
+            x.deadline = deadline;
+            FlatOrigin org;
+            org.q = q;
+            org.src = src;
+            org.pos = pos;
+            org.end = end < pos + 32 ? end : pos + 32;
+            uint64_t fc = 0;
+            flat_done = flat_lane_chunk(a, x, m, fbuf, org, c, pushed, st, fc);
+            if (flat_done) lane_cnt += fc;
+          }
           bool heavy = false;
           uint32_t widx = 0;
           uint64_t my_cnt = 0;
-          if ((m >> lane) & 1u) {
+          if (!flat_done && ((m >> lane) & 1u)) {
             LaneCtx x;
             x.Q = Q;
             x.L = lvl;

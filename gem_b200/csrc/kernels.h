@@ -179,7 +179,14 @@ struct JBack {
 constexpr uint32_t LIST_CACHE_SLOTS = 2;
 constexpr uint32_t LIST_CACHE_CAP = 1024;
 constexpr uint32_t JOIN_WARPS_PER_BLOCK = 8;
-constexpr uint32_t JOIN_DYN_SMEM = JOIN_WARPS_PER_BLOCK * LIST_CACHE_SLOTS * LIST_CACHE_CAP * 4;
+// Balanced lane-level counting: per warp, up to FLAT_MAX_JOBS intersections
+// (one per subset of a prefix match) shared out in blocks of 8 entries.
+constexpr uint32_t FLAT_MAX_VALUES = 4;  // subset values per prefix match
+constexpr uint32_t FLAT_MAX_JOBS = 96;
+constexpr uint32_t FLAT_JOB_BYTES = 40;
+constexpr uint32_t FLAT_WARP_BYTES = FLAT_MAX_JOBS * (FLAT_JOB_BYTES + 8) + 16;
+constexpr uint32_t JOIN_DYN_SMEM =
+    JOIN_WARPS_PER_BLOCK * (LIST_CACHE_SLOTS * LIST_CACHE_CAP * 4 + FLAT_WARP_BYTES);
 constexpr uint32_t MAX_GROUPS = 16;   // label groups of a closed-form suffix
 constexpr uint32_t MAX_GROUP = 4;     // members of one group (15 subsets, 15 partitions)
 // Inclusion-exclusion term: coefficient in the high 32 bits (two's
@@ -196,7 +203,8 @@ struct JQuery {
   uint32_t n_enum;           // levels enumerated; levels n_enum..n-1 are counted in closed form
   uint64_t root_base;        // first global root index of this query
   uint32_t n_groups;         // label groups of the suffix
-  uint32_t pad2;
+  uint32_t flat;             // balanced lane-level counting: subset values per prefix match
+                             // (bits 0-7; 0 = not eligible) and those needing a scan (bits 8-15)
   uint32_t grp_first[MAX_GROUPS];
   uint32_t grp_size[MAX_GROUPS];
   uint32_t term_base[MAX_GROUPS];
@@ -280,6 +288,7 @@ struct JoinArgs {
   uint32_t root_batch_max;   // largest root batch a warp takes at once
   uint32_t lane_scan_max;    // longest intersection one lane does alone
   uint32_t nv;               // data vertices (bounds of rank-bitmap probes)
+  uint32_t flat_donate_blocks; // balanced counting: chunks above this many blocks are split with idle warps
   const uint64_t *vnh_off;   // neighbourhood hash offsets (nv + 1), or null: binary search
   const uint32_t *vnh_slots;
   uint64_t n_values;         // entries of `values`

@@ -218,7 +218,9 @@ gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode,
  * level's unread candidates worth handing over (last enumerated level /
  * other levels); root_batch_max caps the roots a warp takes at once;
  * lane_scan_max is the longest intersection a single lane works through
- * before the whole warp takes it over. */
+ * before the whole warp takes it over; split_blocks is the work (in blocks
+ * of 8 scanned entries) above which a warp's chunk of last-level matches is
+ * split with idle warps. */
 typedef struct gem_schedule {
   uint32_t blocks_per_sm;
   uint32_t donate_max_level;
@@ -226,7 +228,8 @@ typedef struct gem_schedule {
   uint32_t donate_min_desc;
   uint32_t root_batch_max;
   uint32_t lane_scan_max;
-  uint32_t reserved[2];
+  uint32_t split_blocks;
+  uint32_t reserved;
 } gem_schedule;
 
 /* Set / read the schedule used for waves whose largest query has
