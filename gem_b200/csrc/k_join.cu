@@ -250,6 +250,7 @@ __device__ __forceinline__ uint32_t index_of(const JoinArgs &a, const JLevel *__
 struct ListCache {
   uint32_t *buf;            // LIST_CACHE_SLOTS * LIST_CACHE_CAP entries
   unsigned long long *tag;  // {lo, hi} per slot
+  unsigned long long *rng;  // {lo, hi} of suffix back entries b0 + i (lo ~0: not keyed by the prefix); rng[64] = b0
 };
 
 __device__ __forceinline__ int cache_slot(const ListCache &lc, uint64_t lo, uint64_t hi) {
@@ -344,7 +345,11 @@ __device__ void cache_suffix_lists(const JoinArgs &a, const JQuery *__restrict__
                                    const uint32_t *sidx, const ListCache &lc) {
   const uint32_t lane = lane_id();
   const uint32_t n = Q->n, ne = Q->n_enum;
-  if (ne >= n || n > QV) return;
+  if (ne >= n || n > QV) {
+    lc.rng[2 * lane] = ~0ull;
+    __syncwarp();
+    return;
+  }
   const uint32_t b0 = Q->lv[ne].back_base, b1 = Q->lv[n - 1].back_base + Q->lv[n - 1].nback;
   uint64_t my_lo = 0, my_hi = 0, my_len = 0;
   if (b1 > b0 && lane < b1 - b0 && inb(a, SITE_BACK, (uint64_t)b0 + lane, a.n_backs)) {
@@ -354,8 +359,15 @@ __device__ void cache_suffix_lists(const JoinArgs &a, const JQuery *__restrict__
       table_range(a, b, sidx[kl], my_lo, my_hi);
       const uint64_t len = my_hi - my_lo;
       if (len >= 4 && len <= LIST_CACHE_CAP) my_len = len;
+      lc.rng[2 * lane] = my_lo;
+      lc.rng[2 * lane + 1] = my_hi;
+    } else {
+      lc.rng[2 * lane] = ~0ull;
     }
+  } else {
+    lc.rng[2 * lane] = ~0ull;
   }
+  if (lane == 0) lc.rng[64] = b0;
   uint64_t pick_lo[LIST_CACHE_SLOTS], pick_hi[LIST_CACHE_SLOTS];
 #pragma unroll
   for (int k = 0; k < (int)LIST_CACHE_SLOTS; ++k) {
@@ -440,8 +452,16 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
       const JBack *b = a.backs + M->back_base + li;
       const uint32_t kl = b->lvl;
       if (!inb(a, SITE_KEYLVL, kl, (uint64_t)x.L + 1)) return;
-      const uint32_t kidx = kl == x.L ? x.widx : x.sidx[kl];
       kv = kl == x.L ? x.w : x.sf[kl];
+      if (kl < x.L) {  // keyed by the prefix: the warp's range table has it
+        const uint32_t ti = M->back_base + li - (uint32_t)x.lc.rng[64];
+        if (ti < 32 && x.lc.rng[2 * ti] != ~0ull) {
+          lo = x.lc.rng[2 * ti];
+          hi = x.lc.rng[2 * ti + 1];
+          return;
+        }
+      }
+      const uint32_t kidx = kl == x.L ? x.widx : x.sidx[kl];
       table_range(a, b, kidx, lo, hi);
       return;
     }
@@ -1287,8 +1307,11 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
   uint32_t *sf = s_pref[threadIdx.x >> 5][0], *sidx = s_pref[threadIdx.x >> 5][1];
   ListCache lc;
   // per warp: the list cache, then the balanced-counting job table
-  lc.buf = s_lcache + (threadIdx.x >> 5) * (LIST_CACHE_SLOTS * LIST_CACHE_CAP + FLAT_WARP_BYTES / 4);
+  lc.buf = s_lcache + (threadIdx.x >> 5) * (JOIN_WARP_SMEM / 4);
   char *fbuf = reinterpret_cast<char *>(lc.buf + LIST_CACHE_SLOTS * LIST_CACHE_CAP);
+  lc.rng = reinterpret_cast<unsigned long long *>(fbuf + FLAT_WARP_BYTES);
+  lc.rng[2 * lane] = ~0ull;
+  if (lane == 0) lc.rng[64] = 0;
   lc.tag = s_ctag[threadIdx.x >> 5];
   if (lane < 2 * LIST_CACHE_SLOTS) lc.tag[lane] = 0ull;  // empty: no list has lo == hi == 0 and hi > lo
   __syncwarp();
@@ -1301,6 +1324,9 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
   uint64_t rb_cur = 0, rb_end = 0;
   const uint64_t total_warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   bool pushed = false;  // donated work since the last busy decrement
+  // The prefix changes only with a new task or a descent: the suffix lists
+  // keyed by it are looked up once per prefix (epoch), not once per chunk.
+  uint32_t epoch = 0, filled_epoch = 0xFFFFFFFFu;
 
   // ---------------------------------------------------------------- lane-parallel roots
   // Queries whose only enumerated level is the root: one root per lane.
@@ -1495,6 +1521,7 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
     }
 
     // ------------------------------------------------------------ set up
+    ++epoch;
     uint64_t lane_cnt = 0, lane_hash = 0;
     const JQuery *__restrict__ Q = a.queries + q;
     if (from_root) {
@@ -1595,7 +1622,10 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
             sidx[lane] = c.idx;
           }
           __syncwarp();
-          if (lvl > 0) cache_suffix_lists(a, Q, lvl, sidx, lc);
+          if (lvl > 0 && filled_epoch != epoch) {
+            cache_suffix_lists(a, Q, lvl, sidx, lc);
+            filled_epoch = epoch;
+          }
           bool flat_done = false;
           if (Q->flat && a.vnh_off) {
             LaneCtx x;
@@ -1715,6 +1745,7 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
         st.probes += L->idx_kind != IDX_NONE;
       }
       const uint32_t nxt = lvl + 1;
+      ++epoch;
       if (!inb(a, SITE_LEVEL, nxt, n)) {
         abort = true;
         break;

@@ -185,8 +185,11 @@ constexpr uint32_t FLAT_MAX_VALUES = 4;  // subset values per prefix match
 constexpr uint32_t FLAT_MAX_JOBS = 96;
 constexpr uint32_t FLAT_JOB_BYTES = 40;
 constexpr uint32_t FLAT_WARP_BYTES = FLAT_MAX_JOBS * (FLAT_JOB_BYTES + 8) + 16;
-constexpr uint32_t JOIN_DYN_SMEM =
-    JOIN_WARPS_PER_BLOCK * (LIST_CACHE_SLOTS * LIST_CACHE_CAP * 4 + FLAT_WARP_BYTES);
+// Ranges of the suffix lists keyed by prefix levels, per warp: 32 {lo, hi}
+// pairs and a header (the first suffix back entry).
+constexpr uint32_t SUFFIX_RANGE_BYTES = 32 * 16 + 16;
+constexpr uint32_t JOIN_WARP_SMEM = LIST_CACHE_SLOTS * LIST_CACHE_CAP * 4 + FLAT_WARP_BYTES + SUFFIX_RANGE_BYTES;
+constexpr uint32_t JOIN_DYN_SMEM = JOIN_WARPS_PER_BLOCK * JOIN_WARP_SMEM;
 constexpr uint32_t MAX_GROUPS = 16;   // label groups of a closed-form suffix
 constexpr uint32_t MAX_GROUP = 4;     // members of one group (15 subsets, 15 partitions)
 // Inclusion-exclusion term: coefficient in the high 32 bits (two's
