@@ -183,10 +183,8 @@ def run_gem(args):
             if dist:
                 dist.barrier()
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
             st, rs = ctx.batch(qs)
             torch.cuda.synchronize()
-            wall_ms.append((time.perf_counter() - t0) * 1e3)
             # device time of the batch: sum over its waves (first kernel .. last kernel, CUDA events)
             waves = {}
             for r in rs:
@@ -199,8 +197,24 @@ def run_gem(args):
             for k in phase:
                 phase[k] += sum(r["ms"][k] for r in waves.values())
             res_all.append(rs)
-            h2d += sum(4 * q.nv + 8 * q.ne for q in qs)
-            d2h += 8 * 4 * len(qs)
+    # end to end through the public API: query arrays in host memory, the
+    # counts and statuses read back, timed on the host (a separate pass over
+    # the same steps, so the device-timed pass keeps its per-wave records)
+    e2e_same, e2e_exact = True, 0
+    for i, s in enumerate(steps):
+        qs = batch_of(s)
+        flush_l2(dev)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, counts, status = ctx.batch_counts(qs)
+        torch.cuda.synchronize()
+        wall_ms.append((time.perf_counter() - t0) * 1e3)
+        e2e_same &= all(int(c) == r["count"] for c, r in zip(counts, res_all[i]) if r["status"] == "OK")
+        e2e_exact += int((status == 0).sum())
+        h2d += sum(4 * q.nv + 8 * q.ne for q in qs)  # the queries' label and edge arrays
+        d2h += 64 * len(qs) + 1024  # per-query counters and the control block
     exact = sum(1 for rs in res_all for r in rs if r["status"] == "OK")
     capped = sum(1 for rs in res_all for r in rs if r["status"] == "ERR_TIMEOUT")
     emb = sum(r["count"] for rs in res_all for r in rs if r["status"] == "OK")
@@ -210,13 +224,13 @@ def run_gem(args):
     jb = jbytes
     jt = jms / 1e3
     if dist:
-        t = torch.tensor([tdev, twall, float(exact), float(emb), float(capped)], dtype=torch.float64)
+        t = torch.tensor([tdev, twall, float(exact), float(emb), float(capped), float(e2e_exact)], dtype=torch.float64)
         mx = t.clone()
         dist.all_reduce(mx[:2], op=dist.ReduceOp.MAX)
         sm = t[2:].clone()
         dist.all_reduce(sm, op=dist.ReduceOp.SUM)
         tdev, twall = float(mx[0]), float(mx[1])
-        exact, emb, capped = int(sm[0]), int(sm[1]), int(sm[2])
+        exact, emb, capped, e2e_exact = int(sm[0]), int(sm[1]), int(sm[2]), int(sm[3])
     # plain mode: the same queries, one gem_query_run each (rank 0)
     plain = {}
     if rank == 0 and args.plain > 0:
@@ -274,7 +288,8 @@ def run_gem(args):
         "phase_ms": {k: round(v, 3) for k, v in phase.items()},
         "autotune": tuned,
         "rmat22": c2,
-        "e2e": {"value": exact / twall if twall > 0 else 0.0, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
+        "e2e": {"value": e2e_exact / twall if twall > 0 else 0.0, "unit": "queries/s", "counts_equal": e2e_same,
+                "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic, "traffic_source": traffic_src,

@@ -168,9 +168,13 @@ class Query:
         return int(self.edges.shape[0])
 
     def _c(self):
-        q = _Query(self.nv, self.ne, _p32(self.labels), _p32(self.edges.reshape(-1)))
-        q._keep = (self.labels, self.edges)
-        return q
+        # built once: the pointers refer to this object's arrays, which it keeps
+        cq = self.__dict__.get("_cq")
+        if cq is None:
+            self._flat_edges = self.edges.reshape(-1)
+            cq = _Query(self.nv, self.ne, _p32(self.labels), _p32(self._flat_edges))
+            self._cq = cq
+        return cq
 
     @staticmethod
     def read_text(path):
@@ -373,6 +377,19 @@ class Context:
             for r in out:
                 r["error"] = m.decode() if m else ""
         return st, out
+
+    def batch_counts(self, qs, mode=MODE_COUNT):
+        """gem_batch_run without per-query dicts: (status, counts u64[n], statuses i32[n])."""
+        n = len(qs)
+        arr = (_Query * n)()
+        for i, q in enumerate(qs):
+            arr[i] = q._c()
+        rs = (_Result * n)()
+        st = lib().gem_batch_run(self._h, arr, n, mode, rs)
+        raw = np.frombuffer(rs, dtype=np.uint8).reshape(n, C.sizeof(_Result))
+        counts = raw[:, _Result.count.offset:_Result.count.offset + 8].copy().view(np.uint64).reshape(n)
+        status = raw[:, _Result.status.offset:_Result.status.offset + 4].copy().view(np.int32).reshape(n)
+        return st, counts, status
 
     def autotune(self, qs, mode=MODE_COUNT, trial_cap_ms=2000):
         """Tune the join schedule per query-size bucket; returns {bucket: (blocks/SM, donate level, us)}."""

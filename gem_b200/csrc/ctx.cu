@@ -150,7 +150,7 @@ extern "C" gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out) {
   CU(cudaMalloc(&ctx->d_queue, sizeof(JTask) * TASK_CAP));
   CU(cudaMalloc(&ctx->d_qends, sizeof(JQueueEnds) * QUEUE_SUBQ));
   CU(cudaMalloc(&ctx->d_err, sizeof(uint32_t) * 4));
-  CU(cudaHostAlloc(&ctx->h_small, 1 << 20, cudaHostAllocDefault));
+  CU(cudaHostAlloc(&ctx->h_small, H_SMALL_BYTES, cudaHostAllocDefault));
   ctx->device_bytes += sizeof(JControl) + sizeof(JTask) * TASK_CAP + sizeof(JQueueEnds) * QUEUE_SUBQ + 16;
   *out = c.release();
   return GEM_OK;
@@ -543,6 +543,35 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 }
 
 // Runs the filter for every query of the wave; fills w.rows / counts / lists.
+// A slice of the pinned staging buffer for one copy of the current wave, or
+// null when it is used up (the copy then goes through pageable memory).
+static void *stage(gem_ctx *ctx, size_t bytes) {
+  const size_t at = (ctx->h_used + 255) & ~(size_t)255;
+  if (!ctx->h_small || at + bytes > H_SMALL_BYTES) return nullptr;
+  ctx->h_used = at + bytes;
+  return static_cast<char *>(ctx->h_small) + at;
+}
+
+// Host-to-device copy on the context's stream through pinned staging: the
+// source may be reused as soon as this returns.
+static cudaError_t h2d(gem_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  if (!bytes) return cudaSuccess;
+  void *st = stage(ctx, bytes);
+  if (!st) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->s);
+  std::memcpy(st, src, bytes);
+  return cudaMemcpyAsync(dst, st, bytes, cudaMemcpyHostToDevice, ctx->s);
+}
+
+// Device-to-host copy that completes with a stream synchronisation.
+static cudaError_t d2h_sync(gem_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  if (!bytes) return cudaSuccess;
+  void *st = stage(ctx, bytes);
+  cudaError_t e = cudaMemcpyAsync(st ? st : dst, src, bytes, cudaMemcpyDeviceToHost, ctx->s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->s);
+  if (e == cudaSuccess && st) std::memcpy(dst, st, bytes);
+  return e;
+}
+
 static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   const uint32_t nwords = (ctx->g.nv + 31) / 32;
   w.nwords = nwords;
@@ -556,7 +585,7 @@ static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   w.nrows = rows;
   FilterDesc *d_fd;
   ST(aalloc(ctx, fd.size(), &d_fd));
-  CU(cudaMemcpyAsync(d_fd, fd.data(), fd.size() * sizeof(FilterDesc), cudaMemcpyHostToDevice, ctx->s));
+  CU(h2d(ctx, d_fd, fd.data(), fd.size() * sizeof(FilterDesc)));
   const uint64_t nbits = (uint64_t)rows * nwords;
   ST(aalloc(ctx, nbits, &w.d_rb));
   uint64_t *d_ex, *d_tmp, *d_rows;
@@ -567,8 +596,7 @@ static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   launch_scan(w.d_rb, SCAN_POPC_U64LO, nbits, d_ex, d_tmp, ctx->s);
   launch_gather_strided(d_ex, nwords, rows + 1, d_rows, ctx->s);
   std::vector<uint64_t> rs(rows + 1);
-  CU(cudaMemcpyAsync(rs.data(), d_rows, 8ull * (rows + 1), cudaMemcpyDeviceToHost, ctx->s));
-  CU(cudaStreamSynchronize(ctx->s));
+  CU(d2h_sync(ctx, rs.data(), d_rows, 8ull * (rows + 1)));
   CU(cudaGetLastError());
   w.cnt.resize(rows);
   w.c_base.resize(rows + 1);
@@ -577,7 +605,7 @@ static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   const uint64_t total = w.c_base[rows];
   uint64_t *d_cbase;
   ST(aalloc(ctx, rows + 1, &d_cbase));
-  CU(cudaMemcpyAsync(d_cbase, w.c_base.data(), 8ull * (rows + 1), cudaMemcpyHostToDevice, ctx->s));
+  CU(h2d(ctx, d_cbase, w.c_base.data(), 8ull * (rows + 1)));
   ST(aalloc(ctx, total ? total : 1, &w.d_cand));
   launch_compact(w.d_rb, d_ex, rows, nwords, d_cbase, w.d_cand, ctx->s);
   CU(cudaGetLastError());
@@ -627,7 +655,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   if (src.empty()) return GEM_OK;
   TabSource *d_src;
   ST(aalloc(ctx, src.size(), &d_src));
-  CU(cudaMemcpyAsync(d_src, src.data(), src.size() * sizeof(TabSource), cudaMemcpyHostToDevice, ctx->s));
+  CU(h2d(ctx, d_src, src.data(), src.size() * sizeof(TabSource)));
   uint32_t *d_tiles;
   uint64_t *d_tp, *d_tmp, *d_stb;
   ST(aalloc(ctx, nkeys ? nkeys : 1, &d_tiles));
@@ -638,8 +666,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   launch_scan(d_tiles, SCAN_U32, nkeys, d_tp, d_tmp, ctx->s);
   launch_source_tile_bases(d_src, (uint32_t)src.size(), nkeys, d_tp, d_stb, ctx->s);
   std::vector<uint64_t> stb(src.size() + 1);
-  CU(cudaMemcpyAsync(stb.data(), d_stb, 8 * stb.size(), cudaMemcpyDeviceToHost, ctx->s));
-  CU(cudaStreamSynchronize(ctx->s));
+  CU(d2h_sync(ctx, stb.data(), d_stb, 8 * stb.size()));
   CU(cudaGetLastError());
   // edges
   uint64_t tiles = 0, offs = 0;
@@ -671,7 +698,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   for (auto &e : edge) e.offsets = d_offs + e.off_base;
   TabEdge *d_edge;
   ST(aalloc(ctx, edge.size(), &d_edge));
-  CU(cudaMemcpyAsync(d_edge, edge.data(), edge.size() * sizeof(TabEdge), cudaMemcpyHostToDevice, ctx->s));
+  CU(h2d(ctx, d_edge, edge.data(), edge.size() * sizeof(TabEdge)));
   uint32_t *d_mask;
   uint64_t *d_vp, *d_tmp2;
   ST(aalloc(ctx, tiles ? tiles : 1, &d_mask));
@@ -680,8 +707,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   launch_table_count(ctx->g, d_src, d_edge, (uint32_t)edge.size(), d_tp, tiles, d_mask, ctx->s);
   launch_scan(d_mask, SCAN_POPC_U32, tiles, d_vp, d_tmp2, ctx->s);
   uint64_t nvals = 0;
-  CU(cudaMemcpyAsync(&nvals, d_vp + tiles, 8, cudaMemcpyDeviceToHost, ctx->s));
-  CU(cudaStreamSynchronize(ctx->s));
+  CU(d2h_sync(ctx, &nvals, d_vp + tiles, 8));
   CU(cudaGetLastError());
   ST(aalloc(ctx, nvals ? nvals : 1, &w.d_values));
   launch_table_offsets(d_src, d_edge, (uint32_t)edge.size(), d_tp, d_vp, offs, ctx->s);
@@ -751,13 +777,12 @@ static gem_status wave_index(gem_ctx *ctx, Wave &w) {
   void *dv;
   ST(ctx->arena.alloc(ctx, tabs.size() * sizeof(CuckooTable) + tabs.size() * 4 + 16, &dv));
   CuckooTable *d_tabs = (CuckooTable *)dv;
-  CU(cudaMemcpyAsync(d_tabs, tabs.data(), tabs.size() * sizeof(CuckooTable), cudaMemcpyHostToDevice, ctx->s));
+  CU(h2d(ctx, d_tabs, tabs.data(), tabs.size() * sizeof(CuckooTable)));
   CU(cudaMemsetAsync(ctx->d_err, 0, 4, ctx->s));
   launch_cuckoo_build(d_tabs, tabs.data(), (uint32_t)tabs.size(), ctx->d_err, ctx->s);
   CU(cudaGetLastError());
   uint32_t herr = 0;
-  CU(cudaMemcpyAsync(&herr, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->s));
-  CU(cudaStreamSynchronize(ctx->s));
+  CU(d2h_sync(ctx, &herr, ctx->d_err, 4));
   if (herr) {
     ctx->err = "cuckoo stash overflow";
     return GEM_ERR_OVERFLOW;
@@ -863,17 +888,17 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   uint64_t *d_lpp;
   ST(aalloc(ctx, lpq.size() ? lpq.size() : 1, &d_lpq));
   ST(aalloc(ctx, lpp.size(), &d_lpp));
-  if (!lpq.empty()) CU(cudaMemcpyAsync(d_lpq, lpq.data(), lpq.size() * 4, cudaMemcpyHostToDevice, ctx->s));
-  CU(cudaMemcpyAsync(d_lpp, lpp.data(), lpp.size() * 8, cudaMemcpyHostToDevice, ctx->s));
+  if (!lpq.empty()) CU(h2d(ctx, d_lpq, lpq.data(), lpq.size() * 4));
+  CU(h2d(ctx, d_lpp, lpp.data(), lpp.size() * 8));
   if (!terms.empty())
-    CU(cudaMemcpyAsync(d_terms, terms.data(), terms.size() * 8, cudaMemcpyHostToDevice, ctx->s));
+    CU(h2d(ctx, d_terms, terms.data(), terms.size() * 8));
   ST(aalloc(ctx, jq.size(), &d_jq));
   ST(aalloc(ctx, jb.size() ? jb.size() : 1, &d_jb));
   ST(aalloc(ctx, rp.size(), &d_rp));
   ST(aalloc(ctx, jq.size(), &d_out));
-  CU(cudaMemcpyAsync(d_jq, jq.data(), jq.size() * sizeof(JQuery), cudaMemcpyHostToDevice, ctx->s));
-  if (!jb.empty()) CU(cudaMemcpyAsync(d_jb, jb.data(), jb.size() * sizeof(JBack), cudaMemcpyHostToDevice, ctx->s));
-  CU(cudaMemcpyAsync(d_rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, ctx->s));
+  CU(h2d(ctx, d_jq, jq.data(), jq.size() * sizeof(JQuery)));
+  if (!jb.empty()) CU(h2d(ctx, d_jb, jb.data(), jb.size() * sizeof(JBack)));
+  CU(h2d(ctx, d_rp, rp.data(), rp.size() * 8));
   const uint64_t cap_ms = ctx->opts.time_cap_ms ? ctx->opts.time_cap_ms : 600000u;
   JoinArgs a;
   std::memset(&a, 0, sizeof a);
@@ -918,10 +943,14 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   CU(cudaEventRecord(ctx->ev[7], ctx->s));
   CU(cudaGetLastError());
   std::vector<JOut> out(jq.size());
-  CU(cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(JOut), cudaMemcpyDeviceToHost, ctx->s));
   JControl hc;
-  CU(cudaMemcpyAsync(&hc, ctx->d_ctl, sizeof hc, cudaMemcpyDeviceToHost, ctx->s));
+  JOut *s_out = static_cast<JOut *>(stage(ctx, out.size() * sizeof(JOut)));
+  JControl *s_ctl = static_cast<JControl *>(stage(ctx, sizeof(JControl)));
+  CU(cudaMemcpyAsync(s_out ? s_out : out.data(), d_out, out.size() * sizeof(JOut), cudaMemcpyDeviceToHost, ctx->s));
+  CU(cudaMemcpyAsync(s_ctl ? s_ctl : &hc, ctx->d_ctl, sizeof hc, cudaMemcpyDeviceToHost, ctx->s));
   CU(cudaStreamSynchronize(ctx->s));
+  if (s_out) std::memcpy(out.data(), s_out, out.size() * sizeof(JOut));
+  if (s_ctl) std::memcpy(&hc, s_ctl, sizeof hc);
   w.join_ms = ev_ms(ctx->ev[6], ctx->ev[7]);
   // Donated tasks still queued when the grid stopped (deadline) were never
   // run: their queries are incomplete.
@@ -960,6 +989,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
 }
 
 gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_t *emb_dev, uint64_t emb_cap) {
+  ctx->h_used = 0;  // the previous wave's copies have completed (it ended with a synchronising readback)
   if (!ctx->loaded) {
     ctx->err = "no data graph loaded";
     return GEM_ERR_STATE;

@@ -96,6 +96,8 @@ inline uint32_t size_bucket(uint32_t nv) {
   return nv <= 4 ? 0 : nv <= 8 ? 1 : nv <= 12 ? 2 : nv <= 16 ? 3 : nv <= 24 ? 4 : 5;
 }
 
+constexpr size_t H_SMALL_BYTES = 4u << 20;  // pinned staging per context
+
 struct gem_ctx {
   gem_opts opts{};
   cudaStream_t s = nullptr;
@@ -123,7 +125,8 @@ struct gem_ctx {
   gem::JTask *d_queue = nullptr;
   gem::JQueueEnds *d_qends = nullptr;
   uint32_t *d_err = nullptr;
-  void *h_small = nullptr;
+  void *h_small = nullptr;           // pinned staging for a wave's small copies (H_SMALL_BYTES)
+  size_t h_used = 0;                 // bytes of h_small handed out in the current wave
   // join schedule: CUDA graph and per-size-bucket tuning (gem_autotune)
   gem::JoinGraph jgraph;
   Tune tune[6];

@@ -28,7 +28,11 @@ __global__ void __launch_bounds__(256) filter_kernel(DevGraph g, const FilterDes
     const uint32_t l = valid ? __ldg(g.lab + v) : 0u;
     const uint32_t d = valid ? __ldg(g.deg + v) : 0u;
     const uint8_t *row = (g.nlc_stride && valid) ? g.nlc + v * g.nlc_stride : nullptr;
-    for (uint32_t qi = 0; qi < nquery; ++qi) {
+    // this block's group of queries (blockIdx.y): small graphs have too few
+    // tiles to fill the GPU with whole waves of queries per warp
+    const uint32_t qper = (nquery + gridDim.y - 1) / gridDim.y;
+    const uint32_t q0 = blockIdx.y * qper, q1 = q0 + qper < nquery ? q0 + qper : nquery;
+    for (uint32_t qi = q0; qi < q1; ++qi) {
       const FilterDesc *q = descs + qi;
       const uint32_t nq = q->nq, T = q->threshold, nql = q->nql;
       uint32_t pmask = 0;
@@ -79,8 +83,13 @@ void launch_filter(const DevGraph &g, const FilterDesc *d_desc, uint32_t nquery,
   if (nwords == 0 || nquery == 0) return;
   uint64_t blocks = (nwords + 7) / 8;
   if (blocks > 148ull * 16) blocks = 148ull * 16;
+  // split the wave's queries over grid.y until about 148 x 48 warps run
+  uint64_t groups = (148ull * 48 + nwords - 1) / nwords;
+  if (groups > nquery) groups = nquery;
+  if (groups > 65535) groups = 65535;
+  if (groups == 0) groups = 1;
   count_launch();
-  filter_kernel<<<(uint32_t)blocks, 256, 0, s>>>(g, d_desc, nquery, rb, nwords);
+  filter_kernel<<<dim3((uint32_t)blocks, (uint32_t)groups), 256, 0, s>>>(g, d_desc, nquery, rb, nwords);
 }
 
 __global__ void compact_kernel(uint64_t *__restrict__ rb, const uint64_t *__restrict__ ex, uint32_t nrows,
