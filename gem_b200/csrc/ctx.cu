@@ -668,31 +668,48 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   std::vector<uint64_t> stb(src.size() + 1);
   CU(d2h_sync(ctx, stb.data(), d_stb, 8 * stb.size()));
   CU(cudaGetLastError());
-  // edges
-  uint64_t tiles = 0, offs = 0;
+  // edges, grouped by source so that one pass over a source's tiles serves
+  // all its tables
+  struct EdgeReq {
+    uint32_t s, qi, j, k;
+  };
+  std::vector<EdgeReq> reqs;
   w.edge_of.assign(w.q.size(), {});
   for (size_t qi = 0; qi < w.q.size(); ++qi) {
     if (!w.active[qi]) continue;
     const Plan &p = w.plan[qi];
-    w.edge_of[qi].assign(QV * QV, UINT32_MAX);
+    w.edge_of[qi].assign((size_t)p.n * QV, UINT32_MAX);
     for (uint32_t k = 1; k < p.n; ++k)
-      for (uint32_t j : p.back[k]) {
-        const uint32_t r = w.row_base[qi] + p.order[j];
-        const uint32_t s = (uint32_t)row_src[r];
-        TabEdge e;
-        e.src = s;
-        e.pad = 0;
-        e.rb_w = w.d_rb + (uint64_t)(w.row_base[qi] + p.order[k]) * w.nwords;
-        e.tile_base = tiles;
-        e.ntiles = stb[s + 1] - stb[s];
-        e.off_base = offs;
-        e.offsets = nullptr;
-        tiles += e.ntiles;
-        offs += (uint64_t)src[s].nkeys + 1;
-        w.edge_of[qi][j * QV + k] = (uint32_t)edge.size();
-        edge.push_back(e);
-      }
+      for (uint32_t j : p.back[k])
+        reqs.push_back({(uint32_t)row_src[w.row_base[qi] + p.order[j]], (uint32_t)qi, j, k});
   }
+  std::stable_sort(reqs.begin(), reqs.end(), [](const EdgeReq &x, const EdgeReq &y) { return x.s < y.s; });
+  std::vector<uint32_t> sedge(2 * src.size(), 0);
+  uint64_t tiles = 0, offs = 0;
+  for (const EdgeReq &rq : reqs) {
+    const Plan &p = w.plan[rq.qi];
+    TabEdge e;
+    e.src = rq.s;
+    e.pad = 0;
+    e.rb_w = w.d_rb + (uint64_t)(w.row_base[rq.qi] + p.order[rq.k]) * w.nwords;
+    e.tile_base = tiles;
+    e.ntiles = stb[rq.s + 1] - stb[rq.s];
+    e.off_base = offs;
+    e.offsets = nullptr;
+    tiles += e.ntiles;
+    offs += (uint64_t)src[rq.s].nkeys + 1;
+    if (sedge[2 * rq.s + 1] == 0) sedge[2 * rq.s] = (uint32_t)edge.size();
+    sedge[2 * rq.s + 1]++;
+    w.edge_of[rq.qi][rq.j * QV + rq.k] = (uint32_t)edge.size();
+    edge.push_back(e);
+  }
+  const uint64_t src_tiles = stb[src.size()];
+  uint32_t *d_sedge, *d_tkey, *d_tsrc;
+  ST(aalloc(ctx, sedge.size(), &d_sedge));
+  CU(h2d(ctx, d_sedge, sedge.data(), sedge.size() * 4));
+  ST(aalloc(ctx, src_tiles ? src_tiles : 1, &d_tkey));
+  ST(aalloc(ctx, src_tiles ? src_tiles : 1, &d_tsrc));
+  launch_tile_keys(d_src, (uint32_t)src.size(), nkeys, d_tp, d_tkey, d_tsrc, ctx->s);
   uint64_t *d_offs;
   ST(aalloc(ctx, offs, &d_offs));
   for (auto &e : edge) e.offsets = d_offs + e.off_base;
@@ -704,14 +721,15 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   ST(aalloc(ctx, tiles ? tiles : 1, &d_mask));
   ST(aalloc(ctx, tiles + 1, &d_vp));
   ST(aalloc(ctx, scan_tmp_words(tiles), &d_tmp2));
-  launch_table_count(ctx->g, d_src, d_edge, (uint32_t)edge.size(), d_tp, tiles, d_mask, ctx->s);
+  launch_table_count(ctx->g, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, src_tiles, d_mask, ctx->s);
   launch_scan(d_mask, SCAN_POPC_U32, tiles, d_vp, d_tmp2, ctx->s);
   uint64_t nvals = 0;
   CU(d2h_sync(ctx, &nvals, d_vp + tiles, 8));
   CU(cudaGetLastError());
   ST(aalloc(ctx, nvals ? nvals : 1, &w.d_values));
   launch_table_offsets(d_src, d_edge, (uint32_t)edge.size(), d_tp, d_vp, offs, ctx->s);
-  launch_table_write(ctx->g, d_src, d_edge, (uint32_t)edge.size(), d_tp, tiles, d_mask, d_vp, w.d_values, ctx->s);
+  launch_table_write(ctx->g, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, src_tiles, d_mask, d_vp, w.d_values,
+                     ctx->s);
   CU(cudaGetLastError());
   w.edges = edge;
   w.table_values = nvals;

@@ -342,7 +342,7 @@ __device__ __forceinline__ uint32_t list_member8(const JoinArgs &a, uint64_t &cu
 // Warp-collective: caches the longest suffix lists keyed by levels below L
 // (the prefix is sf/sidx).  Lists already cached stay in their slots.
 __device__ void cache_suffix_lists(const JoinArgs &a, const JQuery *__restrict__ Q, uint32_t L,
-                                   const uint32_t *sidx, const ListCache &lc) {
+                                   const uint32_t *sidx, const ListCache &lc, bool copy = true) {
   const uint32_t lane = lane_id();
   const uint32_t n = Q->n, ne = Q->n_enum;
   if (ne >= n || n > QV) {
@@ -368,6 +368,8 @@ __device__ void cache_suffix_lists(const JoinArgs &a, const JQuery *__restrict__
     lc.rng[2 * lane] = ~0ull;
   }
   if (lane == 0) lc.rng[64] = b0;
+  __syncwarp();  // every lane reads the range table
+  if (!copy) return;
   uint64_t pick_lo[LIST_CACHE_SLOTS], pick_hi[LIST_CACHE_SLOTS];
 #pragma unroll
   for (int k = 0; k < (int)LIST_CACHE_SLOTS; ++k) {
@@ -410,6 +412,7 @@ __device__ void cache_suffix_lists(const JoinArgs &a, const JQuery *__restrict__
     }
     __syncwarp();
   }
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
@@ -1623,7 +1626,9 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
           }
           __syncwarp();
           if (lvl > 0 && filled_epoch != epoch) {
-            cache_suffix_lists(a, Q, lvl, sidx, lc);
+            // copying lists into shared memory pays only when the prefix has
+            // more than this chunk at its last level
+            cache_suffix_lists(a, Q, lvl, sidx, lc, end > pos + 32);
             filled_epoch = epoch;
           }
           bool flat_done = false;

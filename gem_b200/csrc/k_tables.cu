@@ -14,8 +14,6 @@
 
 namespace gem {
 
-constexpr uint32_t TILES_PER_WARP = 16;
-
 // Last index i in [lo, hi) with a[i] <= x (requires a[lo] <= x).
 __device__ __forceinline__ uint64_t last_le(const uint64_t *__restrict__ a, uint64_t lo, uint64_t hi, uint64_t x) {
   while (hi - lo > 1) {
@@ -34,14 +32,6 @@ __device__ __forceinline__ uint32_t find_src(const TabSource *__restrict__ src, 
   return lo;
 }
 
-__device__ __forceinline__ uint32_t find_edge(const TabEdge *__restrict__ e, uint32_t ne, uint64_t t) {
-  uint32_t lo = 0, hi = ne;
-  while (hi - lo > 1) {
-    uint32_t mid = (lo + hi) >> 1;
-    if (e[mid].tile_base <= t) lo = mid; else hi = mid;
-  }
-  return lo;
-}
 
 __global__ void key_tiles_kernel(DevGraph g, const TabSource *__restrict__ src, uint32_t nsrc, uint64_t nkeys,
                                  uint32_t *__restrict__ tiles) {
@@ -51,6 +41,7 @@ __global__ void key_tiles_kernel(DevGraph g, const TabSource *__restrict__ src, 
     tiles[k] = (__ldg(g.deg + v) + 31u) >> 5;
   }
 }
+
 
 void launch_key_tiles(const DevGraph &g, const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, uint32_t *tiles,
                       cudaStream_t s) {
@@ -73,88 +64,110 @@ void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nk
   source_tile_bases_kernel<<<(nsrc + 256) / 256, 256, 0, s>>>(d_src, nsrc, nkeys, tp, out);
 }
 
-// Walks the tiles [t0, t1) of the flattened edge-tile space; calls
-// fn(edge, arc_index_or_~0, nbr) once per lane per tile with the tile index.
+// Tile t of the flattened source-tile space (the 32-arc tiles of every key of
+// every source): the key it belongs to and its source.
+__global__ void tile_keys_kernel(const TabSource *__restrict__ src, uint32_t nsrc, uint64_t nkeys,
+                                 const uint64_t *__restrict__ tp, uint32_t *__restrict__ tkey,
+                                 uint32_t *__restrict__ tsrc) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nkeys; k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = find_src(src, nsrc, k);
+    for (uint64_t t = tp[k], e = tp[k + 1]; t < e; ++t) {
+      tkey[t] = (uint32_t)k;
+      tsrc[t] = s;
+    }
+  }
+}
+
+void launch_tile_keys(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp, uint32_t *tkey,
+                      uint32_t *tsrc, cudaStream_t s) {
+  if (nkeys == 0) return;
+  uint64_t blocks = (nkeys + 255) / 256;
+  if (blocks > 148ull * 32) blocks = 148ull * 32;
+  count_launch();
+  tile_keys_kernel<<<(uint32_t)blocks, 256, 0, s>>>(d_src, nsrc, nkeys, tp, tkey, tsrc);
+}
+
+// One warp per TILE_UNROLL consecutive source tiles: the tiles' key, vertex,
+// offsets and neighbour loads are independent and overlap; each tile is then
+// tested against (count) or copied for (write) every edge of its source, so
+// a source's adjacency is read once however many tables it keys.
+constexpr int TILE_UNROLL = 4;
+
 template <bool WRITE>
-__global__ void __launch_bounds__(256) table_tiles_kernel(DevGraph g, const TabSource *__restrict__ srcs,
-                                                          const TabEdge *__restrict__ edges, uint32_t nedge,
-                                                          const uint64_t *__restrict__ tp, uint64_t total_tiles,
-                                                          uint32_t *__restrict__ mask, const uint64_t *__restrict__ vp,
-                                                          uint32_t *__restrict__ values) {
+__global__ void __launch_bounds__(256) table_src_kernel(DevGraph g, const TabSource *__restrict__ srcs,
+                                                        const uint32_t *__restrict__ sedge,
+                                                        const TabEdge *__restrict__ edges,
+                                                        const uint64_t *__restrict__ tp,
+                                                        const uint32_t *__restrict__ tkey,
+                                                        const uint32_t *__restrict__ tsrc, uint64_t ntile,
+                                                        uint32_t *__restrict__ mask, const uint64_t *__restrict__ vp,
+                                                        uint32_t *__restrict__ values) {
   const uint32_t lane = dev::lane_id();
   const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t t0 = (blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * TILES_PER_WARP;
-       t0 < total_tiles; t0 += nwarps * TILES_PER_WARP) {
-    const uint64_t t1 = min(t0 + TILES_PER_WARP, total_tiles);
-    uint32_t e = find_edge(edges, nedge, t0);
-    TabEdge E = edges[e];
-    TabSource S = srcs[E.src];
-    uint64_t sbase = tp[S.key_base];
-    uint64_t st = sbase + (t0 - E.tile_base);
-    uint64_t k = last_le(tp, S.key_base, S.key_base + S.nkeys, st);
-    uint64_t k_next_tile = __ldg(tp + k + 1);
-    uint32_t v = __ldg(S.keys + (k - S.key_base));
-    uint64_t a0 = __ldg(g.off + v), a1 = __ldg(g.off + v + 1);
-    for (uint64_t t = t0; t < t1; ++t, ++st) {
-      if (t >= E.tile_base + E.ntiles) {  // next edge
-        e = find_edge(edges, nedge, t);
-        E = edges[e];
-        S = srcs[E.src];
-        sbase = tp[S.key_base];
-        st = sbase + (t - E.tile_base);
-        k = last_le(tp, S.key_base, S.key_base + S.nkeys, st);
-        k_next_tile = __ldg(tp + k + 1);
-        v = __ldg(S.keys + (k - S.key_base));
-        a0 = __ldg(g.off + v);
-        a1 = __ldg(g.off + v + 1);
-      }
-      while (st >= k_next_tile) {  // next key with at least one tile
-        ++k;
-        k_next_tile = __ldg(tp + k + 1);
-        v = __ldg(S.keys + (k - S.key_base));
-        a0 = __ldg(g.off + v);
-        a1 = __ldg(g.off + v + 1);
-      }
-      const uint64_t arc = a0 + (st - __ldg(tp + k)) * 32 + lane;
-      if (!WRITE) {
-        bool hit = false;
-        if (arc < a1) hit = dev::rank_member(E.rb_w, __ldg(g.nbr + arc));
-        uint32_t m = __ballot_sync(dev::FULL, hit);
-        if (lane == 0) mask[t] = m;
-      } else {
-        uint32_t m = __ldg(mask + t);
-        if (m & (1u << lane)) {
-          uint64_t pos = __ldg(vp + t) + __popc(m & ((1u << lane) - 1u));
-          values[pos] = __ldg(g.nbr + arc);
+  for (uint64_t base = (blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * TILE_UNROLL; base < ntile;
+       base += nwarps * TILE_UNROLL) {
+    uint32_t x[TILE_UNROLL], sx[TILE_UNROLL];
+    uint64_t lt[TILE_UNROLL];
+    bool xv[TILE_UNROLL];
+#pragma unroll
+    for (int i = 0; i < TILE_UNROLL; ++i) {
+      const uint64_t t = base + i;
+      const bool tv = t < ntile;
+      const uint32_t k = tv ? __ldg(tkey + t) : 0u, sidx = tv ? __ldg(tsrc + t) : 0u;
+      const uint64_t kb = srcs[sidx].key_base;
+      const uint32_t *keys = srcs[sidx].keys;
+      const uint32_t v = tv ? __ldg(keys + (k - kb)) : 0u;
+      const uint64_t tk = tv ? __ldg(tp + k) : 0ull, stb = tv ? __ldg(tp + kb) : 0ull;
+      const uint64_t a0 = tv ? __ldg(g.off + v) : 0ull, a1 = tv ? __ldg(g.off + v + 1) : 0ull;
+      const uint64_t arc = a0 + (t - tk) * 32 + lane;
+      sx[i] = sidx;
+      lt[i] = t - stb;  // the tile's index among its source's tiles
+      xv[i] = tv && arc < a1;
+      x[i] = xv[i] ? __ldg(g.nbr + arc) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < TILE_UNROLL; ++i) {
+      if (base + i >= ntile) break;  // the same in every lane
+      const uint32_t e0 = __ldg(sedge + 2 * sx[i]), ne = __ldg(sedge + 2 * sx[i] + 1);
+      for (uint32_t e = e0; e < e0 + ne; ++e) {
+        const uint64_t et = edges[e].tile_base + lt[i];
+        if (!WRITE) {
+          const bool hit = xv[i] && dev::rank_member(edges[e].rb_w, x[i]);
+          const uint32_t m = __ballot_sync(dev::FULL, hit);
+          if (lane == 0) mask[et] = m;
+        } else {
+          const uint32_t m = __ldg(mask + et);
+          if (m & (1u << lane)) values[__ldg(vp + et) + __popc(m & ((1u << lane) - 1u))] = x[i];
         }
       }
     }
   }
 }
 
-static uint32_t tile_blocks(uint64_t total_tiles) {
-  uint64_t warps = (total_tiles + TILES_PER_WARP - 1) / TILES_PER_WARP;
+static uint32_t src_tile_blocks(uint64_t ntile) {
+  uint64_t warps = (ntile + TILE_UNROLL - 1) / TILE_UNROLL;
   uint64_t blocks = (warps + 7) / 8;
-  if (blocks > 148ull * 16) blocks = 148ull * 16;
+  if (blocks > 148ull * 32) blocks = 148ull * 32;
   if (blocks == 0) blocks = 1;
   return (uint32_t)blocks;
 }
 
-void launch_table_count(const DevGraph &g, const TabSource *d_src, const TabEdge *d_edge, uint32_t nedge,
-                        const uint64_t *tp, uint64_t total_tiles, uint32_t *mask, cudaStream_t s) {
-  if (total_tiles == 0) return;
+void launch_table_count(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
+                        uint32_t *mask, cudaStream_t s) {
+  if (ntile == 0) return;
   count_launch();
-  table_tiles_kernel<false><<<tile_blocks(total_tiles), 256, 0, s>>>(g, d_src, d_edge, nedge, tp, total_tiles, mask,
-                                                                     nullptr, nullptr);
+  table_src_kernel<false><<<src_tile_blocks(ntile), 256, 0, s>>>(g, d_src, sedge, d_edge, tp, tkey, tsrc, ntile, mask,
+                                                                  nullptr, nullptr);
 }
 
-void launch_table_write(const DevGraph &g, const TabSource *d_src, const TabEdge *d_edge, uint32_t nedge,
-                        const uint64_t *tp, uint64_t total_tiles, const uint32_t *mask, const uint64_t *vp,
-                        uint32_t *values, cudaStream_t s) {
-  if (total_tiles == 0) return;
+void launch_table_write(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
+                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, cudaStream_t s) {
+  if (ntile == 0) return;
   count_launch();
-  table_tiles_kernel<true><<<tile_blocks(total_tiles), 256, 0, s>>>(g, d_src, d_edge, nedge, tp, total_tiles,
-                                                                    const_cast<uint32_t *>(mask), vp, values);
+  table_src_kernel<true><<<src_tile_blocks(ntile), 256, 0, s>>>(g, d_src, sedge, d_edge, tp, tkey, tsrc, ntile,
+                                                                 const_cast<uint32_t *>(mask), vp, values);
 }
 
 __device__ __forceinline__ uint32_t find_edge_off(const TabEdge *__restrict__ e, uint32_t ne, uint64_t i) {

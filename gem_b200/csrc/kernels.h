@@ -110,18 +110,24 @@ struct TabEdge {             // a directed table T(u -> w)
 // tiles[k] = ceil(deg(key k) / 32) over the flattened key space.
 void launch_key_tiles(const DevGraph &g, const TabSource *d_src, uint32_t nsrc, uint64_t nkeys,
                       uint32_t *tiles, cudaStream_t s);
-// mask[t] = 32-bit membership mask of tile t of every edge.
-void launch_table_count(const DevGraph &g, const TabSource *d_src, const TabEdge *d_edge,
-                        uint32_t nedge, const uint64_t *tp, uint64_t total_tiles, uint32_t *mask,
-                        cudaStream_t s);
+// tkey[t] / tsrc[t]: the key and the source of tile t of the flattened
+// source-tile space (tp: exclusive scan of the key tiles).
+void launch_tile_keys(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp, uint32_t *tkey,
+                      uint32_t *tsrc, cudaStream_t s);
+// mask[edge.tile_base + i] = 32-bit membership mask of tile i of the edge's
+// source, for every edge of every source (sedge: {first edge, edges} per
+// source; a source's edges are consecutive).
+void launch_table_count(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
+                        uint32_t *mask, cudaStream_t s);
 // out[i] = tp[d_src[i].key_base] for i < nsrc, out[nsrc] = tp[nkeys].
 void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp,
                               uint64_t *out, cudaStream_t s);
 void launch_table_offsets(const TabSource *d_src, const TabEdge *d_edge, uint32_t nedge,
                           const uint64_t *tp, const uint64_t *vp, uint64_t total_offsets,
                           cudaStream_t s);
-void launch_table_write(const DevGraph &g, const TabSource *d_src, const TabEdge *d_edge,
-                        uint32_t nedge, const uint64_t *tp, uint64_t total_tiles,
+void launch_table_write(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
                         const uint32_t *mask, const uint64_t *vp, uint32_t *values, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
