@@ -44,6 +44,7 @@ EXPORTS = (
     "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
     "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static", "gem_set_schedule", "gem_get_schedule",
+    "gem_relaxed_sets", "gem_relaxed_run",
 )
 
 
@@ -125,6 +126,9 @@ def lib():
         L.gem_submit.argtypes = [vp, C.POINTER(_Query), C.c_int, u64p]
         L.gem_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Result), C.POINTER(C.c_int)]
         L.gem_autotune.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, C.c_uint32, u32p]
+        L.gem_relaxed_sets.argtypes = [C.POINTER(_Query), C.c_uint32, C.c_uint32, u64p, u32p]
+        L.gem_relaxed_run.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, C.c_uint32, u64p,
+                                      C.POINTER(_Result), u32p]
         L.gem_set_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
         L.gem_get_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
         L.gem_filter_static.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(_Query), C.c_uint32, u32p, vp,
@@ -290,6 +294,21 @@ def gen_queries(graph, k, density=ANY, count=1, seed=0x51000, max_e=MAX_QE):
     return out
 
 
+def relaxed_sets(q, threshold, cap=4096):
+    """Edge masks (bit j = edge j of q kept) of q's relaxed queries at `threshold` (gem_relaxed_sets)."""
+    ets = np.zeros(max(cap, 1), np.uint64)
+    n = C.c_uint32()
+    qc = q._c()
+    _check(lib().gem_relaxed_sets(C.byref(qc), threshold, cap, _p64(ets), C.byref(n)), what="relaxed_sets")
+    return [int(x) for x in ets[:n.value]]
+
+
+def relaxed_query(q, et):
+    """The relaxed query of q that keeps the edges in mask et."""
+    keep = [e for j, e in enumerate(q.edges.tolist()) if (et >> j) & 1]
+    return Query(q.labels, keep)
+
+
 def embedding_hash(f):
     f = np.ascontiguousarray(f, dtype=np.uint32)
     return int(lib().gem_embedding_hash(_p32(f), len(f)))
@@ -377,6 +396,16 @@ class Context:
             for r in out:
                 r["error"] = m.decode() if m else ""
         return st, out
+
+    def relaxed(self, q, threshold, mode=MODE_COUNT, cap=4096):
+        """Relaxed matching (gem_relaxed_run): [(edge mask, Result)] for q's relaxed queries."""
+        ets = np.zeros(max(cap, 1), np.uint64)
+        rs = (_Result * max(cap, 1))()
+        n = C.c_uint32()
+        qc = q._c()
+        st = lib().gem_relaxed_run(self._h, C.byref(qc), threshold, mode, cap, _p64(ets), rs, C.byref(n))
+        _check(st, self._h, "relaxed")
+        return [(int(ets[i]), Result._from(rs[i])) for i in range(n.value)]
 
     def batch_counts(self, qs, mode=MODE_COUNT):
         """gem_batch_run without per-query dicts: (status, counts u64[n], statuses i32[n])."""

@@ -183,7 +183,8 @@ typedef struct gem_result {
 } gem_result;
 
 /* Run one query end to end on the device (filter -> index -> edge tables ->
- * join), synchronously.  threshold must be 0 (exact matching).  In
+ * join), synchronously.  threshold must be 0 (exact matching; relaxed
+ * matching is gem_relaxed_run).  In
  * ENUMERATE mode up to emb_cap embeddings are written to emb_out as nv u32
  * per embedding in query-vertex order (order of embeddings unspecified);
  * more than emb_cap embeddings return GEM_ERR_OVERFLOW with the exact count.
@@ -197,6 +198,22 @@ gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold,
  * Replaces the out-of-core directory batch loop (out-of-core/src/main.cu:334-410). */
 gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n,
                          int mode, gem_result *res);
+
+/* Relaxed matching (the reference's -t T; in-core/lib/plan/src/relax.cpp:84-142
+ * and the per-relaxed-query counts of in-core/src/main.cu:229-236).  The
+ * relaxed queries of q at `threshold` are its edge subsets that still connect
+ * all its vertices with at most `threshold` of its edges removed; each keeps
+ * q's vertices and labels.  gem_relaxed_sets lists them (host only): ets[i]
+ * has bit j set when q's edge j (in q's order) is kept; fewest edges removed
+ * first, then by mask descending.  gem_relaxed_run counts each exactly, as
+ * its own query, in one gem_batch_run, with res[i] for ets[i].  At most cap
+ * relaxed queries: with more, GEM_ERR_LIMIT and *n_out = cap + 1.  Queries
+ * with more than 64 edges return GEM_ERR_LIMIT.  A query with one edge or
+ * none has only itself (the reference lists none). */
+gem_status gem_relaxed_sets(const gem_query *q, uint32_t threshold, uint32_t cap, uint64_t *ets,
+                            uint32_t *n_out);
+gem_status gem_relaxed_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold, int mode, uint32_t cap,
+                           uint64_t *ets, gem_result *res, uint32_t *n_out);
 
 /* Autotuner (no counterpart in the reference): for each query-size bucket
  * (<=4, <=8, <=12, <=16, <=24, <=32 vertices) present in qs, runs a sample of

@@ -15,8 +15,12 @@ minute), so the case list is short and skips queries whose counts run into
 the billions; the fixture is rewritten after every case and the run stops
 starting new cases once `budget_s` seconds have passed.
 
+With a threshold argument > 0 the binary runs relaxed matching (-t T) on a
+smaller list of queries (at most RELAXED_MAX_EDGES edges) and prints one
+count per relaxed query; all of them are recorded with their edge sets.
+
 Usage (on a GPU machine):
-    python tests/golden/make_ref_counts.py <out.json> [work_dir] [budget_s]
+    python tests/golden/make_ref_counts.py <out.json> [work_dir] [budget_s] [threshold]
 """
 import json
 import os
@@ -42,6 +46,11 @@ GRAPHS = [
 # Those sizes are left out and no query with more than MAX_QUERY_EDGES edges
 # is run.
 MAX_QUERY_EDGES = 10
+GRAPHS_RELAXED = [
+    ("rmat10_l3", 10, 8, 3, 0.0, 0x5201, [(4, gem.ANY), (4, gem.DENSE), (5, gem.ANY), (5, gem.DENSE)]),
+    ("rmat11_l6z", 11, 8, 6, 1.0, 0x5202, [(4, gem.ANY), (5, gem.DENSE)]),
+]
+RELAXED_MAX_EDGES = 8
 PER_SIZE = 2
 
 
@@ -49,6 +58,9 @@ def main():
     out = sys.argv[1]
     work = sys.argv[2] if len(sys.argv) > 2 else os.path.join(os.path.dirname(out), "ref_inputs")
     budget_s = float(sys.argv[3]) if len(sys.argv) > 3 else 1e9
+    threshold = int(sys.argv[4]) if len(sys.argv) > 4 else 0
+    graphs = GRAPHS_RELAXED if threshold else GRAPHS
+    max_edges = RELAXED_MAX_EDGES if threshold else MAX_QUERY_EDGES
     binary = os.path.join(ROOT, "oracle", "_ref", "GEM_ic")
     os.makedirs(work, exist_ok=True)
     cases = []
@@ -56,17 +68,17 @@ def main():
 
     def save():
         with open(out, "w") as f:
-            json.dump({"binary": "oracle/_ref/GEM_ic (in-core, built by oracle/ref/Makefile)", "threshold": 0,
+            json.dump({"binary": "oracle/_ref/GEM_ic (in-core, built by oracle/ref/Makefile)", "threshold": threshold,
                        "cases": cases}, f, indent=0)
 
-    for gname, scale, ef, nl, zs, seed, sizes in GRAPHS:
+    for gname, scale, ef, nl, zs, seed, sizes in graphs:
         g = gem.HostGraph.rmat(scale, ef, seed=seed).set_labels(nl, zs, seed=seed ^ 0x4C)
         gpath = os.path.join(work, gname + ".graph")
         g.write_text(gpath)
         gd = dict(name=gname, scale=scale, edge_factor=ef, labels=nl, zipf_s=zs, seed=seed)
         for (k, dens) in sizes:
             for i, q in enumerate(gem.gen_queries(g, k, dens, PER_SIZE, seed=seed * 131 + k * 7 + dens)):
-                if q.ne < 2 or q.ne > MAX_QUERY_EDGES or q.nv > 16:
+                if q.ne < 2 or q.ne > max_edges or q.nv > 16:
                     continue
                 if time.time() - t_start > budget_s:
                     print("budget reached", flush=True)
@@ -75,7 +87,8 @@ def main():
                 q.write_text(qpath)
                 t0 = time.time()
                 try:
-                    r = subprocess.run([binary, "-q", qpath, "-d", gpath, "-t", "0", "-g", "0"], capture_output=True,
+                    r = subprocess.run([binary, "-q", qpath, "-d", gpath, "-t", str(threshold), "-g", "0"],
+                                       capture_output=True,
                                        text=True, timeout=120)
                     m = re.findall(r"Relaxed Query ET ([01]+): (\d+) matches", r.stdout)
                     rec = dict(graph=gd, labels=q.labels.tolist(), edges=q.edges.tolist(), exit=r.returncode,

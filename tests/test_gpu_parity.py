@@ -356,3 +356,47 @@ def test_counts_match_reference_binary():
     for ctx in graphs.values():
         ctx.close()
     assert checked >= 10
+
+
+def test_relaxed_counts_match_oracle(small, gctx):
+    """gem_relaxed_run: every relaxed query's count equals the oracle's count
+    of that query (each relaxed query is matched exactly)."""
+    for k, dens, t in ((4, gem.DENSE, 2), (5, gem.ANY, 1), (6, gem.SPARSE, 1)):
+        for q in gem.gen_queries(small, k, dens, 1, seed=300 + k):
+            out = gctx.relaxed(q, t)
+            assert [et for et, _ in out] == gem.relaxed_sets(q, t)
+            for et, r in out:
+                assert r["status"] == "OK", r
+                exp, _, ok = oracle.count(small, gem.relaxed_query(q, et), want_hash=False)
+                assert ok and r["count"] == exp, (q.edges.tolist(), bin(et), r["count"], exp)
+
+
+REF_RELAXED = os.path.join(os.path.dirname(__file__), "golden", "ref_relaxed.json")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_RELAXED), reason="reference relaxed fixture not generated")
+def test_relaxed_counts_match_reference_binary():
+    """gem_relaxed_run at the reference's threshold returns the reference
+    binary's relaxed queries with its printed counts (mod 2^32)."""
+    with open(REF_RELAXED) as f:
+        data = json.load(f)
+    ctxs, checked = {}, 0
+    for c in data["cases"]:
+        if c["exit"] != 0 or not c["printed"]:
+            continue
+        gd = c["graph"]
+        if gd["name"] not in ctxs:
+            g = gem.HostGraph.rmat(gd["scale"], gd["edge_factor"], seed=gd["seed"]).set_labels(
+                gd["labels"], gd["zipf_s"], seed=gd["seed"] ^ 0x4C)
+            ctx = gem.Context(time_cap_ms=60000)
+            ctx.load_graph(g)
+            ctxs[gd["name"]] = ctx
+        ref = {int(et, 2): cnt for et, cnt in zip(c["et"], c["printed"])}
+        got = ctxs[gd["name"]].relaxed(gem.Query(c["labels"], c["edges"]), data["threshold"])
+        assert {et for et, _ in got} == set(ref)
+        for et, r in got:
+            assert r["status"] == "OK" and r["count"] % (1 << 32) == ref[et], (c["edges"], bin(et), r["count"])
+            checked += 1
+    for ctx in ctxs.values():
+        ctx.close()
+    assert checked >= 20

@@ -125,3 +125,55 @@ def test_random_walk_queries(k, dens):
             assert avg > 3
     qs2 = gem.gen_queries(g, k, dens, 12, seed=77)
     assert all(np.array_equal(a.edges, b.edges) and np.array_equal(a.labels, b.labels) for a, b in zip(qs, qs2))
+
+
+def _relaxed_py(q, threshold):
+    """Independent enumeration: edge subsets with at most `threshold` edges
+    removed whose edges connect all query vertices."""
+    import itertools
+    ne, nv = q.ne, q.nv
+    edges = q.edges.tolist()
+    out = set()
+    for r in range(0, min(threshold, ne) + 1):
+        for removed in itertools.combinations(range(ne), r):
+            keep = [j for j in range(ne) if j not in removed]
+            adj = {u: set() for u in range(nv)}
+            for j in keep:
+                a, b = edges[j]
+                adj[a].add(b)
+                adj[b].add(a)
+            seen, stack = {0}, [0]
+            while stack:
+                u = stack.pop()
+                for w in adj[u] - seen:
+                    seen.add(w)
+                    stack.append(w)
+            if len(seen) == nv:
+                out.add(sum(1 << j for j in keep))
+    return out
+
+
+def test_relaxed_sets_match_enumeration():
+    """gem_relaxed_sets: the connected spanning edge subsets with at most T
+    edges removed, fewest removed first (in-core/lib/plan/src/relax.cpp:84-142)."""
+    qs = [gem.Query([0, 0, 0, 0], [(0, 1), (1, 2), (2, 3), (3, 0), (0, 2)]),
+          gem.Query([1, 2, 1], [(0, 1), (1, 2), (0, 2)]),
+          gem.Query([0, 1, 2, 3], [(0, 1), (1, 2), (2, 3)]),
+          gem.Query([0] * 5, [(i, j) for i in range(5) for j in range(i + 1, 5)]),
+          gem.Query([3], [])]
+    g = gem.HostGraph.rmat(10, 8, seed=7).set_labels(3, seed=8)
+    qs += gem.gen_queries(g, 6, gem.DENSE, 4, seed=9) + gem.gen_queries(g, 8, gem.ANY, 4, seed=10)
+    for q in qs:
+        for t in (0, 1, 2, 3):
+            got = gem.relaxed_sets(q, t)
+            assert set(got) == _relaxed_py(q, t), (q.edges.tolist(), t)
+            assert len(got) == len(set(got))
+            removed = [q.ne - bin(x).count("1") for x in got]
+            assert removed == sorted(removed) and (not got or got[0] == (1 << q.ne) - 1)
+
+
+def test_relaxed_sets_cap():
+    q = gem.Query([0] * 5, [(i, j) for i in range(5) for j in range(i + 1, 5)])
+    n = len(gem.relaxed_sets(q, 3))
+    with pytest.raises(gem.GemError):
+        gem.relaxed_sets(q, 3, cap=n - 1)

@@ -110,3 +110,38 @@ def test_oracle_matches_reference_binary():
         assert c["et"][0] == "0" * (32 - len(c["edges"])) + "1" * len(c["edges"])
         checked += 1
     assert checked >= 10
+
+
+REF_RELAXED = os.path.join(os.path.dirname(__file__), "golden", "ref_relaxed.json")
+
+
+def _ref_relaxed_cases():
+    with open(REF_RELAXED) as f:
+        data = json.load(f)
+    graphs = {}
+    for c in data["cases"]:
+        if c["exit"] != 0 or not c["printed"]:
+            continue
+        gd = c["graph"]
+        if gd["name"] not in graphs:
+            graphs[gd["name"]] = gem.HostGraph.rmat(gd["scale"], gd["edge_factor"], seed=gd["seed"]).set_labels(
+                gd["labels"], gd["zipf_s"], seed=gd["seed"] ^ 0x4C)
+        yield data["threshold"], graphs[gd["name"]], gem.Query(c["labels"], c["edges"]), \
+            {int(et, 2): cnt for et, cnt in zip(c["et"], c["printed"])}
+
+
+@pytest.mark.skipif(not os.path.exists(REF_RELAXED), reason="reference relaxed fixture not generated")
+def test_relaxed_sets_and_oracle_match_reference_binary():
+    """The reference binary's relaxed queries at -t 1 (one printed line per
+    relaxed query, its 32-bit edge set and a uint32 count) are exactly
+    gem_relaxed_sets' edge sets, and each printed count equals the oracle's
+    count of that relaxed query mod 2^32."""
+    checked = 0
+    for t, g, q, ref in _ref_relaxed_cases():
+        assert set(gem.relaxed_sets(q, t)) == set(ref), (q.edges.tolist(), ref)
+        for et, printed in ref.items():
+            cnt, _, ok = oracle.count(g, gem.relaxed_query(q, et), want_hash=False, work_cap=300_000_000)
+            if ok:
+                assert cnt % (1 << 32) == printed, (q.edges.tolist(), bin(et), cnt, printed)
+                checked += 1
+    assert checked >= 20
