@@ -18,6 +18,11 @@ bounded step; the section reports, per query under a device time cap,
 whether it completed and the enumeration rate.  A query that exceeds the cap
 is reported as capped, never as an exact count.
 
+The `serving` section submits the headline queries one by one through
+gem_submit / gem_poll under Poisson arrivals (1,000 / 5,000 / 20,000 per
+second, one second each) and reports latency percentiles and the achieved
+rate; every result is checked against the batched count.
+
 `value` is device-timed (CUDA events around each batch, inputs resident in
 HBM), `e2e` is wall time around the C-ABI call from host buffers (query
 arrays in, results out).  L2 is flushed between steps (a 256 MiB write).
@@ -252,6 +257,10 @@ def run_gem(args):
                  "queries_per_s_wall": pn / (sum(lat) / 1e3) if lat else None,
                  "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99), "counts_equal_batched": same}
     ctx.close()
+    serving = None
+    if rank == 0 and args.serve_seconds > 0:
+        ref = {i: r["count"] for i, r in enumerate(res_all[0])} if len(batch_of(args.warmup)) == len(pool) else {}
+        serving = serving_section(gem, args, local, g, pool, ref) if ref else None
     c2 = rmat22_section(gem, args, local) if rank == 0 and args.c2_sample > 0 else None
     if dist:
         dist.destroy_process_group()
@@ -287,6 +296,7 @@ def run_gem(args):
         "plain": plain,
         "phase_ms": {k: round(v, 3) for k, v in phase.items()},
         "autotune": tuned,
+        "serving": serving,
         "rmat22": c2,
         "e2e": {"value": e2e_exact / twall if twall > 0 else 0.0, "unit": "queries/s", "counts_equal": e2e_same,
                 "h2d_bytes_per_step": h2d // args.steps,
@@ -301,6 +311,53 @@ def run_gem(args):
     if args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(g, pool, args)
     print(json.dumps(line), flush=True)
+
+
+def serving_section(gem, args, local, g, pool, ref_counts):
+    """Continuous batching through gem_submit / gem_poll under Poisson arrivals
+    of the headline queries (cycled), one stream per rate: latency from the
+    arrival to the result being visible, achieved rate, and every count
+    checked against the batched run's."""
+    import collections
+    import random
+    out = {"queries": "the headline pool, cycled", "seconds_per_rate": args.serve_seconds, "rates": []}
+    with gem.Context(device=local, time_cap_ms=args.cap_ms) as c:
+        c.load_graph(g)
+        for lam in [float(x) for x in args.serve_rates.split(",") if x]:
+            rng = random.Random(0x5E12 + int(lam))
+            arr, t = [], 0.0
+            while True:
+                t += rng.expovariate(lam)
+                if t > args.serve_seconds:
+                    break
+                arr.append(t)
+            pending, lat, same, busy, i = collections.deque(), [], True, 0, 0
+            t0 = time.perf_counter()
+            while i < len(arr) or pending:
+                now = time.perf_counter() - t0
+                while i < len(arr) and arr[i] <= now:
+                    qi = i % len(pool)
+                    tk = c.submit(pool[qi])
+                    if tk is None:  # admission busy: the arrival waits
+                        busy += 1
+                        break
+                    pending.append((tk, arr[i], qi))
+                    i += 1
+                while pending:  # oldest first
+                    tk, ta, qi = pending[0]
+                    r = c.poll(tk)
+                    if r is None:
+                        break
+                    lat.append((time.perf_counter() - t0 - ta) * 1e3)
+                    same &= r["status"] == "OK" and r["count"] == ref_counts[qi]
+                    pending.popleft()
+                if not pending and i < len(arr):
+                    time.sleep(max(0.0, arr[i] - (time.perf_counter() - t0)))
+            wall = time.perf_counter() - t0
+            out["rates"].append({"lambda_qps": lam, "queries": len(lat), "achieved_qps": len(lat) / wall,
+                                 "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99), "counts_equal_batched": same,
+                                 "admission_busy": busy})
+    return out
 
 
 def profiled_traffic(key):
@@ -409,6 +466,8 @@ def main():
     ap.add_argument("--c2-sample", type=int, default=8, help="scale-22 queries in the rmat22 section (0 = skip)")
     ap.add_argument("--c2-cap-ms", type=int, default=1000)
     ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--serve-seconds", type=float, default=1.0, help="per arrival rate in the serving section (0 = skip)")
+    ap.add_argument("--serve-rates", default="1000,5000,20000", help="Poisson arrival rates (queries/s)")
     ap.add_argument("--cpu-work-cap", type=int, default=1_000_000_000)
     args = ap.parse_args()
     if args.impl == "reference":
