@@ -543,6 +543,31 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 }
 
 // Runs the filter for every query of the wave; fills w.rows / counts / lists.
+// Balanced lane-level counting code of a plan (JQuery::flat): the subset
+// values per prefix match (at most FLAT_MAX_VALUES, each an intersection of
+// at most three lists) and those needing a scan, or 0 when not eligible.
+static uint32_t flat_code(const Plan &p, int mode) {
+  if (mode != GEM_MODE_COUNT || p.groups.empty()) return 0;
+  uint32_t nval = 0, nscan = 0;
+  for (const Plan::Group &g : p.groups)
+    for (uint32_t S = 1; S < (1u << g.size); ++S) {
+      uint32_t nl = 0;
+      for (uint32_t b = 0; b < g.size; ++b)
+        if (S & (1u << b)) nl += (uint32_t)p.back[g.first + b].size();
+      if (nl < 1 || nl > 3) return 0;
+      ++nval;
+      nscan += nl >= 2;
+    }
+  return nval <= FLAT_MAX_VALUES ? nval | (nscan << 8) : 0;
+}
+
+// Queries counted through the (root, first level) pair pool: count mode, an
+// enumerated prefix of a root and one neighbour level, a closed-form suffix
+// eligible for balanced counting, and the neighbourhood hash.
+static bool pair_pool(const gem_ctx *ctx, const Plan &p, int mode) {
+  return ctx->vnh_off && mode == GEM_MODE_COUNT && p.n_enum == 2 && p.n >= 3 && flat_code(p, mode) != 0;
+}
+
 // A slice of the pinned staging buffer for one copy of the current wave, or
 // null when it is used up (the copy then goes through pageable memory).
 static void *stage(gem_ctx *ctx, size_t bytes) {
@@ -686,11 +711,13 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   std::stable_sort(reqs.begin(), reqs.end(), [](const EdgeReq &x, const EdgeReq &y) { return x.s < y.s; });
   std::vector<uint32_t> sedge(2 * src.size(), 0);
   uint64_t tiles = 0, offs = 0;
+  bool key_map = false;
   for (const EdgeReq &rq : reqs) {
     const Plan &p = w.plan[rq.qi];
     TabEdge e;
     e.src = rq.s;
-    e.pad = 0;
+    e.flags = (rq.qi < w.pair.size() && w.pair[rq.qi] && rq.j == 0 && rq.k == 1) ? TAB_KEY_MAP : 0u;
+    key_map |= e.flags != 0;
     e.rb_w = w.d_rb + (uint64_t)(w.row_base[rq.qi] + p.order[rq.k]) * w.nwords;
     e.tile_base = tiles;
     e.ntiles = stb[rq.s + 1] - stb[rq.s];
@@ -727,9 +754,11 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   CU(d2h_sync(ctx, &nvals, d_vp + tiles, 8));
   CU(cudaGetLastError());
   ST(aalloc(ctx, nvals ? nvals : 1, &w.d_values));
+  w.d_vkey = nullptr;
+  if (key_map) ST(aalloc(ctx, nvals ? nvals : 1, &w.d_vkey));
   launch_table_offsets(d_src, d_edge, (uint32_t)edge.size(), d_tp, d_vp, offs, ctx->s);
   launch_table_write(ctx->g, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, src_tiles, d_mask, d_vp, w.d_values,
-                     ctx->s);
+                     w.d_vkey, ctx->s);
   CU(cudaGetLastError());
   w.edges = edge;
   w.table_values = nvals;
@@ -815,7 +844,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   std::vector<JQuery> jq;
   std::vector<JBack> jb;
   std::vector<uint64_t> rp, terms, lpp;
-  std::vector<uint32_t> lpq;
+  std::vector<uint32_t> lpq, lp2q;
   uint64_t lp_roots = 0;
   w.jq_index.assign(w.q.size(), UINT32_MAX);
   uint64_t roots = 0;
@@ -834,24 +863,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
       J.term_count[gi] = (uint32_t)p.groups[gi].terms.size();
       terms.insert(terms.end(), p.groups[gi].terms.begin(), p.groups[gi].terms.end());
     }
-    // balanced lane-level counting: at most FLAT_MAX_VALUES subset values per
-    // prefix match, each an intersection of at most three lists
-    {
-      uint32_t nval = 0, nscan = 0;
-      bool ok = mode == GEM_MODE_COUNT && J.n_groups > 0;
-      for (uint32_t gi = 0; ok && gi < J.n_groups; ++gi) {
-        const uint32_t first = J.grp_first[gi], gs = J.grp_size[gi];
-        for (uint32_t S = 1; ok && S < (1u << gs); ++S) {
-          uint32_t nl = 0;
-          for (uint32_t b = 0; b < gs; ++b)
-            if (S & (1u << b)) nl += (uint32_t)p.back[first + b].size();
-          ok = nl >= 1 && nl <= 3;
-          ++nval;
-          nscan += nl >= 2;
-        }
-      }
-      J.flat = ok && nval <= FLAT_MAX_VALUES ? nval | (nscan << 8) : 0;
-    }
+    J.flat = flat_code(p, mode);
     J.root_u = p.order[0];
     const uint32_t r0 = w.row_base[qi] + p.order[0];
     J.root_cand = w.d_cand + w.c_base[r0];
@@ -887,6 +899,11 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
       lp_roots += J.n_root;
       J.root_base = roots;
       rp.push_back(roots);
+    } else if (w.pair[qi] && w.d_vkey) {
+      // (root, first level) pair pool; an empty range in the ordinary pool
+      lp2q.push_back((uint32_t)jq.size());
+      J.root_base = roots;
+      rp.push_back(roots);
     } else {
       rp.push_back(roots);
       roots += J.n_root;
@@ -896,6 +913,8 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   rp.push_back(roots);
   lpp.push_back(lp_roots);
   w.out.assign(w.q.size(), JOut());
+  uint32_t *d_lp2q = nullptr;
+  uint64_t *d_lp2p = nullptr;
   if (jq.empty()) return GEM_OK;
   JQuery *d_jq;
   JBack *d_jb;
@@ -907,6 +926,11 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   ST(aalloc(ctx, lpq.size() ? lpq.size() : 1, &d_lpq));
   ST(aalloc(ctx, lpp.size(), &d_lpp));
   if (!lpq.empty()) CU(h2d(ctx, d_lpq, lpq.data(), lpq.size() * 4));
+  if (!lp2q.empty()) {
+    ST(aalloc(ctx, lp2q.size(), &d_lp2q));
+    ST(aalloc(ctx, lp2q.size() + 1, &d_lp2p));  // filled by the prepare kernel
+    CU(h2d(ctx, d_lp2q, lp2q.data(), lp2q.size() * 4));
+  }
   CU(h2d(ctx, d_lpp, lpp.data(), lpp.size() * 8));
   if (!terms.empty())
     CU(h2d(ctx, d_terms, terms.data(), terms.size() * 8));
@@ -932,6 +956,10 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   a.lp_prefix = d_lpp;
   a.lp_nq = (uint32_t)lpq.size();
   a.lp_roots = lp_roots;
+  a.lp2_query = d_lp2q;
+  a.lp2_nq = (uint32_t)lp2q.size();
+  a.lp2_prefix = d_lp2p;
+  a.vkey = w.d_vkey;
   a.out = d_out;
   a.ctl = ctx->d_ctl;
   a.queue = ctx->d_queue;
@@ -1054,6 +1082,8 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
       return GEM_ERR_INTERNAL;
     }
   }
+  w.pair.assign(nq, 0);
+  for (size_t qi = 0; qi < nq; ++qi) w.pair[qi] = w.active[qi] && pair_pool(ctx, w.plan[qi], mode);
   w.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
   ST(wave_tables(ctx, w));
   ST(phase_sync("edge tables"));

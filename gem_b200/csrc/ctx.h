@@ -59,6 +59,8 @@ struct Wave {
   std::vector<std::vector<uint32_t>> idx_kind;  // per query, per level
   std::vector<std::vector<const gem::CuckooTable *>> ck_of;
   std::vector<std::vector<uint32_t>> edge_of;   // per query: [j*QV+k] -> edge index
+  std::vector<uint8_t> pair;        // query counted through the (root, first level) pair pool
+  uint32_t *d_vkey = nullptr;       // key positions of the pool queries' root-table values
   uint32_t nrows = 0, nwords = 0, nsrc = 0;
   uint64_t *d_rb = nullptr;       // rank bitmaps, nrows x nwords
   uint32_t *d_cand = nullptr;     // candidate lists back to back

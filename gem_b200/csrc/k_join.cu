@@ -437,7 +437,17 @@ struct LaneCtx {
   const uint32_t *sf, *sidx;
   ListCache lc;
   uint64_t deadline;  // device time cap (%globaltimer ns)
+  // the root (level 0) is this lane's own, not the warp's shared prefix
+  uint32_t own0 = 0, w0 = 0, widx0 = 0;
 };
+
+// Vertex and candidate position of prefix level j for this lane.
+__device__ __forceinline__ uint32_t lvl_vertex(const LaneCtx &x, uint32_t j) {
+  return j == x.L ? x.w : (x.own0 && j == 0) ? x.w0 : x.sf[j];
+}
+__device__ __forceinline__ uint32_t lvl_index(const LaneCtx &x, uint32_t j) {
+  return j == x.L ? x.widx : (x.own0 && j == 0) ? x.widx0 : x.sidx[j];
+}
 
 // List li of the subset `members` of a suffix group: its range, its key
 // vertex (f of the key level) and the level of the member it belongs to.
@@ -455,8 +465,8 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
       const JBack *b = a.backs + M->back_base + li;
       const uint32_t kl = b->lvl;
       if (!inb(a, SITE_KEYLVL, kl, (uint64_t)x.L + 1)) return;
-      kv = kl == x.L ? x.w : x.sf[kl];
-      if (kl < x.L) {  // keyed by the prefix: the warp's range table has it
+      kv = lvl_vertex(x, kl);
+      if (kl < x.L && !(x.own0 && kl == 0)) {  // keyed by the shared prefix: the warp's range table has it
         const uint32_t ti = M->back_base + li - (uint32_t)x.lc.rng[64];
         if (ti < 32 && x.lc.rng[2 * ti] != ~0ull) {
           lo = x.lc.rng[2 * ti];
@@ -464,7 +474,7 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
           return;
         }
       }
-      const uint32_t kidx = kl == x.L ? x.widx : x.sidx[kl];
+      const uint32_t kidx = lvl_index(x, kl);
       table_range(a, b, kidx, lo, hi);
       return;
     }
@@ -510,7 +520,7 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
     uint64_t c = len, cur = slo;
     for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
-      const uint32_t v = j == x.L ? x.w : x.sf[j];  // a prefix vertex: not known to be in C(u_s)
+      const uint32_t v = lvl_vertex(x, j);  // a prefix vertex: not known to be in C(u_s)
       cur = slo;
       const bool in = ss >= 0 || !hash ? list_member(a, x.lc, ss, slo, shi, cur, v)
                                        : vnh_list_has(a, x.Q, skv, sml, ~0u, v);
@@ -547,7 +557,7 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
     uint32_t okm = (1u << n) - 1u;
     for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
-      const uint32_t d = j == x.L ? x.w : x.sf[j];
+      const uint32_t d = lvl_vertex(x, j);
 #pragma unroll
       for (int k = 0; k < 8; ++k)
         if (vv[k] == d) okm &= ~(1u << k);
@@ -617,7 +627,7 @@ __device__ uint64_t lane_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
     bool ok = true;
     for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
-      ok = v != (j == x.L ? x.w : x.sf[j]);
+      ok = v != lvl_vertex(x, j);
     }
     for (uint32_t i = 0; i < nl && ok; ++i) {
       if (i == s) continue;
@@ -698,6 +708,16 @@ struct FlatOrigin {
   uint64_t pos, end;  // the chunk's positions [pos, end) in the source list
 };
 
+// v (any vertex) in a list: its cache slot, the neighbourhood hash with a
+// candidate test, or a binary search.
+__device__ __forceinline__ bool list_has_vertex(const JoinArgs &a, const LaneCtx &x, int slot, uint64_t lo,
+                                                uint64_t hi, uint32_t kv, uint32_t ml, uint32_t v) {
+  if (slot >= 0) return smem_contains(x.lc.buf + slot * LIST_CACHE_CAP, (uint32_t)(hi - lo), v);
+  if (a.vnh_off) return vnh_list_has(a, x.Q, kv, ml, ~0u, v);
+  uint64_t cur = lo;
+  return list_member(a, x.lc, -1, lo, hi, cur, v);
+}
+
 // Counts the suffix completions of the chunk's prefix matches (lanes in m);
 // *my_cnt receives this lane's.  While the chunk holds more than
 // a.flat_donate_blocks blocks and other warps are idle, the positions of the
@@ -718,7 +738,7 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
   bool act = (m >> lane) & 1u;
   const uint32_t jbase = __popc(m & ((1u << lane) - 1u)) * nscan;
   const uint32_t ng = Q->n_groups < MAX_GROUPS ? Q->n_groups : MAX_GROUPS;
-  uint64_t val[FLAT_MAX_VALUES] = {0, 0, 0, 0};
+  uint64_t val[FLAT_MAX_VALUES] = {0, 0, 0, 0};  // one-list values, or the duplicate corrections of jobs
   uint32_t my_blocks = 0;
   // ---- stage 1: this lane's subsets: one-list values directly, the others as jobs
   if (act) {
@@ -750,7 +770,7 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
           uint64_t cnt = shi - slo, cur = slo;
           for (uint32_t dm = dup; dm; dm &= dm - 1) {
             const uint32_t j = __ffs(dm) - 1;
-            const uint32_t v = j == x.L ? x.w : x.sf[j];
+            const uint32_t v = lvl_vertex(x, j);
             cur = slo;
             const bool in = ss >= 0 ? list_member(a, x.lc, ss, slo, shi, cur, v)
                                     : vnh_list_has(a, Q, skv, sml, ~0u, v);
@@ -766,13 +786,25 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
         const uint32_t akv = ia == 0 ? kv[0] : kv[1], bkv = ib == 1 ? kv[1] : kv[2];
         const uint32_t aml = ia == 0 ? ml[0] : ml[1], bml = ib == 1 ? ml[1] : ml[2];
         const int sa = cache_slot(x.lc, alo, ahi), sb = nl > 2 ? cache_slot(x.lc, blo, bhi) : -1;
+        // With a shared prefix the blocks skip the earlier same-label
+        // vertices themselves; with a per-lane root the job counts the whole
+        // intersection and those vertices (distinct) found in it are
+        // subtracted afterwards.
+        uint64_t corr = 0;
+        for (uint32_t dm = x.own0 ? dup : 0u; dm; dm &= dm - 1) {
+          const uint32_t d = lvl_vertex(x, __ffs(dm) - 1);
+          if (list_has_vertex(a, x, ss, slo, shi, skv, sml, d) && list_has_vertex(a, x, sa, alo, ahi, akv, aml, d) &&
+              (nl < 3 || list_has_vertex(a, x, sb, blo, bhi, bkv, bml, d)))
+            ++corr;
+        }
+        val[k] = corr;
         FJob jb;
         jb.s = ss >= 0 ? 0 : slo;
         jb.len = (uint32_t)(shi - slo);
         jb.ra = flat_probe_word(a, sa, alo, ahi, akv);
         jb.rb = nl > 2 ? flat_probe_word(a, sb, blo, bhi, bkv) : 0;
         jb.w = x.w;
-        jb.dup = dup;
+        jb.dup = x.own0 ? 0u : dup;
         jb.meta = (nl > 2 ? 1u : 0u) | ((uint32_t)(ss + 1) << 1) | ((uint32_t)(sa + 1) << 3) |
                   ((uint32_t)(sb + 1) << 5) | ((sml & 31u) << 7) | ((aml & 31u) << 12) | ((bml & 31u) << 17);
         jobs[jbase + jn] = jb;
@@ -795,7 +827,7 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
   // hand the upper half of the work to idle warps while the chunk is large
   uint32_t keep = m;  // lanes whose prefix matches stay here
   uint64_t give_end = org.end;
-  while (total > a.flat_donate_blocks) {
+  while (org.q != ~0u && total > a.flat_donate_blocks) {
     const int idle_now = __shfl_sync(FULL, lane == 0 ? (int)(ld_vol(&a.ctl->idle) > 0) : 0, 0);
     if (!idle_now) break;
     // first lane whose work starts at or after half of the remaining blocks
@@ -853,7 +885,7 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
                 : ss1 ? x.lc.buf[(ss1 - 1) * LIST_CACHE_CAP + off + k]
                       : __ldg(a.values + jb.s + off + k);
       uint32_t okm = (1u << n) - 1u;
-      for (uint32_t dm = jb.dup; dm; dm &= dm - 1) {
+      for (uint32_t dm = jb.dup; dm; dm &= dm - 1) {  // shared prefix: jb.w is level L, the rest shared
         const uint32_t j = __ffs(dm) - 1;
         const uint32_t d = j == x.L ? jb.w : x.sf[j];
 #pragma unroll
@@ -878,7 +910,7 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
       for (uint32_t S = 1; S < (1u << gs) && k < FLAT_MAX_VALUES; ++S, ++k) {
         uint32_t nl = 0;
         for (uint32_t mm = S; mm; mm &= mm - 1) nl += Q->lv[(first + __ffs(mm) - 1) & 31u].nback;
-        const uint64_t v = nl == 1 ? val[k] : (uint64_t)res[jbase + jn++];
+        const uint64_t v = nl == 1 ? val[k] : (uint64_t)res[jbase + jn++] - val[k];
         if (S < 4) sv[S] = v;
       }
       if (gs == 1) {
@@ -978,7 +1010,7 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
     bool hit = false;
     uint64_t cur = s_lo;
     if ((dup_mask >> lane) & 1u) {
-      const uint32_t v = lane == x.L ? x.w : x.sf[lane];  // a prefix vertex: not known to be in C(u_s)
+      const uint32_t v = lvl_vertex(x, lane);  // a prefix vertex: not known to be in C(u_s)
       const int slot = cache_slot(x.lc, s_lo, s_hi);
       hit = slot >= 0 || !hash ? list_member(a, x.lc, slot, s_lo, s_hi, cur, v)
                                : vnh_list_has(a, x.Q, s_kv, s_ml, ~0u, v);
@@ -1057,7 +1089,7 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
     }
     for (uint32_t dm = dup_mask; dm && ok; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
-      ok = v != (j == x.L ? x.w : x.sf[j]);
+      ok = v != lvl_vertex(x, j);
     }
     cnt += __popc(__ballot_sync(FULL, ok));
   }
@@ -1414,6 +1446,98 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
         if (lane == 0 && k) atomicAdd(&a.out[qh].count, (unsigned long long)k);
       }
       if (lane == 0) st.nodes += (a.lp_roots - base) < 32 ? (a.lp_roots - base) : 32;
+    }
+  }
+
+  // ---------------------------------------------------------------- (root, first level) pairs
+  // Queries whose enumerated prefix is a root and one neighbour level: their
+  // prefix matches are the entries of the root's edge table, taken 32 at a
+  // time (each query's range padded to whole chunks), one match per lane with
+  // its own root, so short neighbour lists still fill the warp.
+  if (a.lp2_nq) {
+    const uint64_t total = a.lp2_prefix[a.lp2_nq];
+    uint32_t it = 0;
+    for (;;) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&ctl->lp2_next, 32ull);
+      base = __shfl_sync(FULL, base, 0);
+      if (base >= total) break;
+      if ((++it & 15u) == 0) {
+        int stop = 0;
+        if (lane == 0) {
+          if (ld_vol(&ctl->err) != DERR_NONE) stop = 1;
+          else if (globaltimer_ns() > deadline) {
+            set_error(&ctl->err, DERR_TIMEOUT);
+            stop = 1;
+          }
+          if (stop) {
+            // this chunk and every unclaimed one are abandoned
+            const unsigned long long r0 = atomicExch(&ctl->lp2_next, (unsigned long long)total);
+            const unsigned long long from = base < r0 ? base : r0;
+            for (uint32_t k = find_query(a.lp2_prefix, a.lp2_nq, from); k < a.lp2_nq; ++k)
+              atomicOr(&a.out[a.lp2_query[k]].pad[0], 1ull);
+          }
+        }
+        if (__shfl_sync(FULL, stop, 0)) break;
+      }
+      const uint32_t qk = find_query(a.lp2_prefix, a.lp2_nq, base);
+      const uint32_t q = a.lp2_query[qk];
+      if (!inb(a, SITE_QUERY, q, a.nquery)) break;
+      const JQuery *Q = a.queries + q;
+      const JLevel *L1 = &Q->lv[1];
+      if (!inb(a, SITE_BACK, L1->back_base, a.n_backs)) break;
+      const JBack *b = a.backs + L1->back_base;
+      const uint64_t e0 = __ldg(b->off), e1 = __ldg(b->off + b->nkeys);
+      const uint64_t p = e0 + (base - __ldg(a.lp2_prefix + qk)) + lane;
+      bool valid = p < e1 && inb(a, SITE_RANGE, p, a.n_values);
+      uint32_t f0 = 0, k0 = 0, f1 = 0, i1 = 0;
+      if (valid) {
+        k0 = __ldg(a.vkey + p);
+        valid = inb(a, SITE_ROOT, k0, Q->n_root);
+        if (valid) {
+          f0 = __ldg(Q->root_cand + k0);
+          f1 = __ldg(a.values + p);
+          i1 = index_of(a, L1, f1);
+        }
+      }
+      const uint32_t m = __ballot_sync(FULL, valid);
+      LaneCtx x;
+      x.Q = Q;
+      x.L = 1;
+      x.w = f1;
+      x.widx = i1;
+      x.sf = sf;
+      x.sidx = sidx;
+      x.lc = lc;
+      x.deadline = deadline;
+      x.own0 = 1;
+      x.w0 = f0;
+      x.widx0 = k0;
+      FlatOrigin org;
+      org.q = ~0u;  // lanes hold different roots: no task can carry the chunk
+      org.src = 0;
+      org.pos = org.end = 0;
+      uint64_t cnt = 0;
+      if (!flat_lane_chunk(a, x, m, fbuf, org, c, pushed, st, cnt)) {
+        bool heavy = false;
+        cnt = valid ? lane_suffix_count(a, x, st, heavy) : 0;
+        for (uint32_t hm = __ballot_sync(FULL, heavy); hm; hm &= hm - 1) {
+          const uint32_t hl = __ffs(hm) - 1;
+          LaneCtx y = x;
+          y.w = __shfl_sync(FULL, f1, hl);
+          y.widx = __shfl_sync(FULL, i1, hl);
+          y.w0 = __shfl_sync(FULL, f0, hl);
+          y.widx0 = __shfl_sync(FULL, k0, hl);
+          const uint64_t k = warp_suffix_count(a, y, st);
+          if (lane == hl) cnt += k;
+        }
+      }
+#pragma unroll
+      for (int d = 16; d; d >>= 1) cnt += __shfl_xor_sync(FULL, cnt, d);
+      if (lane == 0) {
+        if (cnt) atomicAdd(&a.out[q].count, (unsigned long long)cnt);
+        st.nodes += __popc(m);
+      }
     }
   }
 
@@ -1807,8 +1931,22 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
 // Zeroes the control block and the per-query outputs, resets the task queue
 // and sets the deadline; runs right before the join in the same graph.
 __global__ void join_prepare_kernel(JControl *ctl, JOut *out, uint32_t nquery, JTask *cells, JQueueEnds *qends,
-                                    uint64_t cap_ns) {
+                                    uint64_t cap_ns, const JQuery *queries, const JBack *backs,
+                                    const uint32_t *lp2q, uint32_t lp2_nq, uint64_t *lp2_prefix) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  // pair pool: each query's (root, first level) pairs are the entries of its
+  // root table, padded to whole chunks of 32 so no chunk spans two queries
+  if (t == 0 && lp2_nq) {
+    uint64_t acc = 0;
+    for (uint32_t i = 0; i < lp2_nq; ++i) {
+      lp2_prefix[i] = acc;
+      const JQuery *Q = queries + lp2q[i];
+      const JBack *b = backs + Q->lv[1].back_base;
+      const uint64_t n = b->off[b->nkeys] - b->off[0];
+      acc += (n + 31) & ~31ull;
+    }
+    lp2_prefix[lp2_nq] = acc;
+  }
   for (uint32_t i = t; i < TASK_CAP; i += nt) cells[i].seq = i & (QUEUE_SUBQ_CAP - 1);
   for (uint32_t i = t; i < QUEUE_SUBQ; i += nt) {
     qends[i].head = 0;
@@ -1871,7 +2009,12 @@ cudaError_t launch_join_graph(JoinGraph &jg, const JoinArgs &a, uint64_t cap_ns,
   JTask *cells = a.queue;
   JQueueEnds *qends = a.qends;
   uint64_t cap = cap_ns;
-  void *prep_params[] = {&ctl, &out, &nq, &cells, &qends, &cap};
+  const JQuery *queries = a.queries;
+  const JBack *backs = a.backs;
+  const uint32_t *lp2q = a.lp2_query;
+  uint32_t lp2_nq = a.lp2_nq;
+  uint64_t *lp2_prefix = const_cast<uint64_t *>(a.lp2_prefix);
+  void *prep_params[] = {&ctl, &out, &nq, &cells, &qends, &cap, &queries, &backs, &lp2q, &lp2_nq, &lp2_prefix};
   void *join_params[] = {&args};
   cudaKernelNodeParams pp = {};
   pp.func = (void *)join_prepare_kernel;

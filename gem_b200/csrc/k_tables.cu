@@ -101,12 +101,12 @@ __global__ void __launch_bounds__(256) table_src_kernel(DevGraph g, const TabSou
                                                         const uint32_t *__restrict__ tkey,
                                                         const uint32_t *__restrict__ tsrc, uint64_t ntile,
                                                         uint32_t *__restrict__ mask, const uint64_t *__restrict__ vp,
-                                                        uint32_t *__restrict__ values) {
+                                                        uint32_t *__restrict__ values, uint32_t *__restrict__ vkey) {
   const uint32_t lane = dev::lane_id();
   const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   for (uint64_t base = (blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * TILE_UNROLL; base < ntile;
        base += nwarps * TILE_UNROLL) {
-    uint32_t x[TILE_UNROLL], sx[TILE_UNROLL];
+    uint32_t x[TILE_UNROLL], sx[TILE_UNROLL], kx[TILE_UNROLL];
     uint64_t lt[TILE_UNROLL];
     bool xv[TILE_UNROLL];
 #pragma unroll
@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(256) table_src_kernel(DevGraph g, const TabSou
       const uint64_t a0 = tv ? __ldg(g.off + v) : 0ull, a1 = tv ? __ldg(g.off + v + 1) : 0ull;
       const uint64_t arc = a0 + (t - tk) * 32 + lane;
       sx[i] = sidx;
+      kx[i] = (uint32_t)(k - kb);  // the key's position in its source's candidate list
       lt[i] = t - stb;  // the tile's index among its source's tiles
       xv[i] = tv && arc < a1;
       x[i] = xv[i] ? __ldg(g.nbr + arc) : 0u;
@@ -137,7 +138,11 @@ __global__ void __launch_bounds__(256) table_src_kernel(DevGraph g, const TabSou
           if (lane == 0) mask[et] = m;
         } else {
           const uint32_t m = __ldg(mask + et);
-          if (m & (1u << lane)) values[__ldg(vp + et) + __popc(m & ((1u << lane) - 1u))] = x[i];
+          if (m & (1u << lane)) {
+            const uint64_t pos = __ldg(vp + et) + __popc(m & ((1u << lane) - 1u));
+            values[pos] = x[i];
+            if (edges[e].flags & TAB_KEY_MAP) vkey[pos] = kx[i];
+          }
         }
       }
     }
@@ -158,16 +163,17 @@ void launch_table_count(const DevGraph &g, const TabSource *d_src, const uint32_
   if (ntile == 0) return;
   count_launch();
   table_src_kernel<false><<<src_tile_blocks(ntile), 256, 0, s>>>(g, d_src, sedge, d_edge, tp, tkey, tsrc, ntile, mask,
-                                                                  nullptr, nullptr);
+                                                                  nullptr, nullptr, nullptr);
 }
 
 void launch_table_write(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
                         const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, cudaStream_t s) {
+                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, uint32_t *vkey,
+                        cudaStream_t s) {
   if (ntile == 0) return;
   count_launch();
   table_src_kernel<true><<<src_tile_blocks(ntile), 256, 0, s>>>(g, d_src, sedge, d_edge, tp, tkey, tsrc, ntile,
-                                                                 const_cast<uint32_t *>(mask), vp, values);
+                                                                 const_cast<uint32_t *>(mask), vp, values, vkey);
 }
 
 __device__ __forceinline__ uint32_t find_edge_off(const TabEdge *__restrict__ e, uint32_t ne, uint64_t i) {

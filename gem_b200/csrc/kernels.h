@@ -100,7 +100,7 @@ struct TabSource {           // a (query, query vertex) whose candidates are tab
 };
 struct TabEdge {             // a directed table T(u -> w)
   uint32_t src;              // index into TabSource
-  uint32_t pad;
+  uint32_t flags;            // TAB_KEY_MAP: the write pass also records each value's key position
   const uint64_t *rb_w;      // rank bitmap row of the target w (membership)
   uint64_t tile_base;        // first tile of this edge in the flattened edge-tile space
   uint64_t ntiles;
@@ -126,9 +126,11 @@ void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nk
 void launch_table_offsets(const TabSource *d_src, const TabEdge *d_edge, uint32_t nedge,
                           const uint64_t *tp, const uint64_t *vp, uint64_t total_offsets,
                           cudaStream_t s);
+constexpr uint32_t TAB_KEY_MAP = 1;
 void launch_table_write(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
                         const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, cudaStream_t s);
+                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, uint32_t *vkey,
+                        cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Cuckoo hash: vertex id -> position in C(u).  Two bucketised tables of
@@ -255,6 +257,7 @@ struct JTask {
 // its own, so the atomics on one do not queue behind traffic to the others.
 struct JControl {
   alignas(128) unsigned long long lp_next;    // next root of the lane-parallel pool
+  alignas(128) unsigned long long lp2_next;   // next chunk of the (root, first level) pair pool
   alignas(128) unsigned long long root_next;  // next root of the ordinary pool
   alignas(128) unsigned long long pending;    // tasks published and not yet taken
   alignas(128) unsigned int busy;             // warps holding work
@@ -298,6 +301,10 @@ struct JoinArgs {
   uint32_t lane_scan_max;    // longest intersection one lane does alone
   uint32_t nv;               // data vertices (bounds of rank-bitmap probes)
   uint32_t flat_donate_blocks; // balanced counting: chunks above this many blocks are split with idle warps
+  const uint32_t *lp2_query; // queries whose prefix is (root, first level): their pair pool
+  uint32_t lp2_nq;
+  const uint64_t *lp2_prefix; // lp2_nq + 1 chunk-padded pair offsets (written by the prepare kernel)
+  const uint32_t *vkey;       // per value of the pool queries' root tables: its key's position
   const uint64_t *vnh_off;   // neighbourhood hash offsets (nv + 1), or null: binary search
   const uint32_t *vnh_slots;
   uint64_t n_values;         // entries of `values`
