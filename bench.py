@@ -167,7 +167,9 @@ def run_gem(args):
     B = args.batch
     ctx = gem.Context(device=local, time_cap_ms=args.cap_ms)
     ctx.load_graph(g)
-    tuned = ctx.autotune(pool[: min(len(pool), 48)], trial_cap_ms=args.cap_ms) if args.autotune else {}
+    # the tuner runs the timed batch's queries (untimed); a wave's join lasts as long
+    # as its heaviest query, so a sample without it tunes for the wrong critical path
+    tuned = ctx.autotune(pool[: min(len(pool), args.batch)], trial_cap_ms=args.cap_ms) if args.autotune else {}
 
     def batch_of(step):
         i = (step * world + rank) * B

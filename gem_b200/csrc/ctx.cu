@@ -1370,7 +1370,7 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
     std::string e;
     if (make_host_query(&qs[i], h, e) != GEM_OK) continue;
     auto &v = byb[size_bucket(h.nv)];
-    if (v.size() < 32) v.push_back(h);
+    if (v.size() < 256) v.push_back(h);
   }
   const int occ = ctx->join_bps[mode];
   std::vector<uint32_t> bps_c = {(uint32_t)occ};
@@ -1398,14 +1398,21 @@ extern "C" gem_status gem_autotune(gem_ctx *ctx, const gem_query *qs, uint32_t n
         ctx->tune[b].lane_scan_max = sc.lsm;
         ctx->tune[b].donate_min_desc = sc.dmd;
         ctx->tune[b].split_blocks = sc.split;
-        Wave w;
-        w.q = byb[b];
-        ctx->arena.reset();
-        st = run_wave(ctx, w, 0, mode, nullptr, 0);
+        // each candidate runs twice; the faster run counts (sub-millisecond joins are noisy)
+        double cost = 1e300;
+        for (int rep = 0; rep < 2 && st == GEM_OK; ++rep) {
+          Wave w;
+          w.q = byb[b];
+          ctx->arena.reset();
+          st = run_wave(ctx, w, 0, mode, nullptr, 0);
+          if (st != GEM_OK) break;
+          uint32_t timeouts = 0;
+          for (size_t i = 0; i < w.q.size(); ++i) timeouts += w.out[i].pad[0] ? 1 : 0;
+          const double c = w.join_ms + (double)timeouts * ctx->opts.time_cap_ms;
+          cost = c < cost ? c : cost;
+          if (timeouts) break;  // a capped trial is not repeated
+        }
         if (st != GEM_OK) break;
-        uint32_t timeouts = 0;
-        for (size_t i = 0; i < w.q.size(); ++i) timeouts += w.out[i].pad[0] ? 1 : 0;
-        const double cost = w.join_ms + (double)timeouts * ctx->opts.time_cap_ms;
         if (cost < best_cost) {
           best_cost = cost;
           best.blocks_per_sm = bps;

@@ -437,16 +437,16 @@ struct LaneCtx {
   const uint32_t *sf, *sidx;
   ListCache lc;
   uint64_t deadline;  // device time cap (%globaltimer ns)
-  // the root (level 0) is this lane's own, not the warp's shared prefix
-  uint32_t own0 = 0, w0 = 0, widx0 = 0;
+  // prefix level ownp (if < QV) is this lane's own, not the warp's shared prefix
+  uint32_t ownp = 0xFFu, wp = 0, widxp = 0;
 };
 
 // Vertex and candidate position of prefix level j for this lane.
 __device__ __forceinline__ uint32_t lvl_vertex(const LaneCtx &x, uint32_t j) {
-  return j == x.L ? x.w : (x.own0 && j == 0) ? x.w0 : x.sf[j];
+  return j == x.L ? x.w : j == x.ownp ? x.wp : x.sf[j];
 }
 __device__ __forceinline__ uint32_t lvl_index(const LaneCtx &x, uint32_t j) {
-  return j == x.L ? x.widx : (x.own0 && j == 0) ? x.widx0 : x.sidx[j];
+  return j == x.L ? x.widx : j == x.ownp ? x.widxp : x.sidx[j];
 }
 
 // List li of the subset `members` of a suffix group: its range, its key
@@ -466,7 +466,7 @@ __device__ __forceinline__ void lane_list(const JoinArgs &a, const LaneCtx &x, u
       const uint32_t kl = b->lvl;
       if (!inb(a, SITE_KEYLVL, kl, (uint64_t)x.L + 1)) return;
       kv = lvl_vertex(x, kl);
-      if (kl < x.L && !(x.own0 && kl == 0)) {  // keyed by the shared prefix: the warp's range table has it
+      if (kl < x.L && kl != x.ownp) {  // keyed by the shared prefix: the warp's range table has it
         const uint32_t ti = M->back_base + li - (uint32_t)x.lc.rng[64];
         if (ti < 32 && x.lc.rng[2 * ti] != ~0ull) {
           lo = x.lc.rng[2 * ti];
@@ -787,11 +787,11 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
         const uint32_t aml = ia == 0 ? ml[0] : ml[1], bml = ib == 1 ? ml[1] : ml[2];
         const int sa = cache_slot(x.lc, alo, ahi), sb = nl > 2 ? cache_slot(x.lc, blo, bhi) : -1;
         // With a shared prefix the blocks skip the earlier same-label
-        // vertices themselves; with a per-lane root the job counts the whole
+        // vertices themselves; with a per-lane level the job counts the whole
         // intersection and those vertices (distinct) found in it are
         // subtracted afterwards.
         uint64_t corr = 0;
-        for (uint32_t dm = x.own0 ? dup : 0u; dm; dm &= dm - 1) {
+        for (uint32_t dm = x.ownp < QV ? dup : 0u; dm; dm &= dm - 1) {
           const uint32_t d = lvl_vertex(x, __ffs(dm) - 1);
           if (list_has_vertex(a, x, ss, slo, shi, skv, sml, d) && list_has_vertex(a, x, sa, alo, ahi, akv, aml, d) &&
               (nl < 3 || list_has_vertex(a, x, sb, blo, bhi, bkv, bml, d)))
@@ -804,7 +804,7 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
         jb.ra = flat_probe_word(a, sa, alo, ahi, akv);
         jb.rb = nl > 2 ? flat_probe_word(a, sb, blo, bhi, bkv) : 0;
         jb.w = x.w;
-        jb.dup = x.own0 ? 0u : dup;
+        jb.dup = x.ownp < QV ? 0u : dup;
         jb.meta = (nl > 2 ? 1u : 0u) | ((uint32_t)(ss + 1) << 1) | ((uint32_t)(sa + 1) << 3) |
                   ((uint32_t)(sb + 1) << 5) | ((sml & 31u) << 7) | ((aml & 31u) << 12) | ((bml & 31u) << 17);
         jobs[jbase + jn] = jb;
@@ -1510,9 +1510,9 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
       x.sidx = sidx;
       x.lc = lc;
       x.deadline = deadline;
-      x.own0 = 1;
-      x.w0 = f0;
-      x.widx0 = k0;
+      x.ownp = 0;
+      x.wp = f0;
+      x.widxp = k0;
       FlatOrigin org;
       org.q = ~0u;  // lanes hold different roots: no task can carry the chunk
       org.src = 0;
@@ -1526,8 +1526,8 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
           LaneCtx y = x;
           y.w = __shfl_sync(FULL, f1, hl);
           y.widx = __shfl_sync(FULL, i1, hl);
-          y.w0 = __shfl_sync(FULL, f0, hl);
-          y.widx0 = __shfl_sync(FULL, k0, hl);
+          y.wp = __shfl_sync(FULL, f0, hl);
+          y.widxp = __shfl_sync(FULL, k0, hl);
           const uint64_t k = warp_suffix_count(a, y, st);
           if (lane == hl) cnt += k;
         }
@@ -1935,17 +1935,38 @@ __global__ void join_prepare_kernel(JControl *ctl, JOut *out, uint32_t nquery, J
                                     const uint32_t *lp2q, uint32_t lp2_nq, uint64_t *lp2_prefix) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   // pair pool: each query's (root, first level) pairs are the entries of its
-  // root table, padded to whole chunks of 32 so no chunk spans two queries
-  if (t == 0 && lp2_nq) {
-    uint64_t acc = 0;
-    for (uint32_t i = 0; i < lp2_nq; ++i) {
-      lp2_prefix[i] = acc;
-      const JQuery *Q = queries + lp2q[i];
-      const JBack *b = backs + Q->lv[1].back_base;
-      const uint64_t n = b->off[b->nkeys] - b->off[0];
-      acc += (n + 31) & ~31ull;
+  // root table, padded to whole chunks of 32 so no chunk spans two queries;
+  // block 0 scans the padded sizes, one query per thread
+  if (blockIdx.x == 0 && lp2_nq) {
+    __shared__ uint64_t wsum[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint64_t carry = 0;
+    for (uint32_t b0 = 0; b0 < lp2_nq; b0 += blockDim.x) {
+      const uint32_t i = b0 + threadIdx.x;
+      uint64_t n = 0;
+      if (i < lp2_nq) {
+        const JQuery *Q = queries + lp2q[i];
+        const JBack *b = backs + Q->lv[1].back_base;
+        n = ((b->off[b->nkeys] - b->off[0]) + 31) & ~31ull;
+      }
+      uint64_t incl = n;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t o = __shfl_up_sync(FULL, incl, d);
+        if (lane >= (uint32_t)d) incl += o;
+      }
+      if (lane == 31) wsum[warp] = incl;
+      __syncthreads();
+      uint64_t before = carry, tile = 0;
+      for (uint32_t w = 0; w < nw; ++w) {
+        if (w < warp) before += wsum[w];
+        tile += wsum[w];
+      }
+      if (i < lp2_nq) lp2_prefix[i] = before + incl - n;
+      carry += tile;
+      __syncthreads();  // wsum is rewritten by the next step
     }
-    lp2_prefix[lp2_nq] = acc;
+    if (threadIdx.x == 0) lp2_prefix[lp2_nq] = carry;
   }
   for (uint32_t i = t; i < TASK_CAP; i += nt) cells[i].seq = i & (QUEUE_SUBQ_CAP - 1);
   for (uint32_t i = t; i < QUEUE_SUBQ; i += nt) {

@@ -216,10 +216,12 @@ gem_status gem_relaxed_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold,
                            uint64_t *ets, gem_result *res, uint32_t *n_out);
 
 /* Autotuner (no counterpart in the reference): for each query-size bucket
- * (<=4, <=8, <=12, <=16, <=24, <=32 vertices) present in qs, runs a sample of
- * up to 32 of its queries under each candidate join schedule (blocks per SM of
- * the persistent grid, deepest level that donates work), each trial capped at
- * trial_cap_ms, and keeps the fastest for later waves of this context.
+ * (<=4, <=8, <=12, <=16, <=24, <=32 vertices) present in qs, runs the first
+ * 256 of its queries as one wave under each candidate join schedule (blocks
+ * per SM of the persistent grid, deepest level that donates work), twice per
+ * candidate, each trial capped at trial_cap_ms, and keeps the fastest for
+ * later waves of this context.  The sample should hold the workload's heavy
+ * queries: a wave's join time is that of its slowest query.
  * Candidate schedules combine blocks per SM with the deepest donating level,
  * the smallest donated half at the lane-parallel level and the root batch.
  * report (optional, 18 entries): per bucket {blocks_per_sm,
