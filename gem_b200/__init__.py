@@ -44,7 +44,7 @@ EXPORTS = (
     "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
     "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static", "gem_set_schedule", "gem_get_schedule",
-    "gem_relaxed_sets", "gem_relaxed_run",
+    "gem_relaxed_sets", "gem_relaxed_run", "gem_ctx_ooc_stats",
 )
 
 
@@ -62,7 +62,14 @@ class _Query(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("device_budget_bytes", C.c_uint64), ("pinned_budget_bytes", C.c_uint64),
                 ("ooc", C.c_int), ("time_cap_ms", C.c_uint32), ("index_kind", C.c_uint32),
-                ("admit_gb", C.c_uint32), ("reserved", C.c_uint32 * 5)]
+                ("admit_gb", C.c_uint32), ("ooc_part_kib", C.c_uint32), ("ooc_stream", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
+
+
+class _OocStats(C.Structure):
+    _fields_ = [("partitions", C.c_uint32), ("reserved0", C.c_uint32), ("max_part_bytes", C.c_uint64),
+                ("waves_streamed", C.c_uint64), ("waves_in_place", C.c_uint64), ("parts_streamed", C.c_uint64),
+                ("bytes_streamed", C.c_uint64)]
 
 
 class _Schedule(C.Structure):
@@ -131,6 +138,7 @@ def lib():
                                       C.POINTER(_Result), u32p]
         L.gem_set_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
         L.gem_get_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
+        L.gem_ctx_ooc_stats.argtypes = [vp, C.POINTER(_OocStats)]
         L.gem_filter_static.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(_Query), C.c_uint32, u32p, vp,
                                         C.c_uint64, vp]
         _lib = L
@@ -331,9 +339,13 @@ class Context:
     """One GPU with a resident data graph (gem_ctx)."""
 
     def __init__(self, device=0, budget_bytes=0, time_cap_ms=0, index_kind=IDX_AUTO, ooc=False, pinned_bytes=0,
-                 admit_gb=0):
+                 admit_gb=0, ooc_part_kib=0, ooc_stream=0):
+        """ooc_part_kib / ooc_stream: out-of-core adjacency partition size (KiB, 0 = 16 MiB) and whether
+        table builds stream partitions (0 = when the sources fill them enough, 1 = always, 2 = never)."""
         o = _Opts()
         o.admit_gb = admit_gb
+        o.ooc_part_kib = ooc_part_kib
+        o.ooc_stream = ooc_stream
         o.device = device
         o.device_budget_bytes = budget_bytes
         o.pinned_budget_bytes = pinned_bytes
@@ -450,6 +462,12 @@ class Context:
         sc = _Schedule()
         _check(lib().gem_get_schedule(self._h, query_vertices, C.byref(sc)), self._h, "get_schedule")
         return {k: int(getattr(sc, k)) for k in SCHEDULE_FIELDS}
+
+    def ooc_stats(self):
+        """Out-of-core partition streaming counters since the graph was loaded (gem_ctx_ooc_stats)."""
+        st = _OocStats()
+        _check(lib().gem_ctx_ooc_stats(self._h, C.byref(st)), self._h, "ooc_stats")
+        return {k: int(getattr(st, k)) for k, _ in _OocStats._fields_ if k != "reserved0"}
 
     def submit(self, q, mode=MODE_COUNT):
         """Serving: returns a ticket, or None when admission is busy (retry later)."""

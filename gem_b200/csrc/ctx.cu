@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -161,6 +162,17 @@ static void free_graph(gem_ctx *ctx) {
     cudaFreeHost(ctx->pinned_nbr);
     ctx->pinned_nbr = nullptr;
   }
+  if (ctx->part_mem) {
+    cudaFree(ctx->part_mem);
+    ctx->device_bytes -= ctx->part_bytes;
+  }
+  ctx->part_mem = nullptr;
+  ctx->part_bytes = 0;
+  ctx->d_part_v = nullptr;
+  ctx->d_stage[0] = ctx->d_stage[1] = nullptr;
+  ctx->part_v.clear();
+  ctx->part_a.clear();
+  ctx->ooc = gem_ooc_stats{};
   if (ctx->graph_mem) {
     cudaFree(ctx->graph_mem);
     ctx->device_bytes -= ctx->graph_bytes;
@@ -194,11 +206,82 @@ extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   for (auto &ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
+  for (int b = 0; b < 2; ++b) {
+    if (ctx->ev_ready[b]) cudaEventDestroy(ctx->ev_ready[b]);
+    if (ctx->ev_free[b]) cudaEventDestroy(ctx->ev_free[b]);
+  }
+  if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
   if (ctx->s) cudaStreamDestroy(ctx->s);
   delete ctx;
 }
 
 extern "C" const char *gem_last_error(const gem_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+// Out-of-core: splits the adjacency into vertex ranges of at most
+// ooc_part_kib KiB (a vertex whose list alone is longer gets a range of its
+// own) and allocates the partition bounds and two staging buffers of the
+// largest partition's size, plus the side stream and events of the copies.
+static gem_status ooc_partitions(gem_ctx *ctx, const gem_hgraph *hg) {
+  const uint32_t nv = hg->nv;
+  const uint64_t cap_bytes = (uint64_t)(ctx->opts.ooc_part_kib ? ctx->opts.ooc_part_kib : 16384u) << 10;
+  const uint64_t cap = cap_bytes / 4 ? cap_bytes / 4 : 1;  // arcs per partition
+  ctx->part_v.assign(1, 0);
+  ctx->part_a.assign(1, 0);
+  uint64_t max_arcs = 0;
+  for (uint32_t v = 0; v < nv;) {
+    const uint64_t a0 = hg->off[v];
+    uint32_t u = v + 1;
+    if (hg->off[u] - a0 <= cap) {
+      // the last u in (v, nv] with off[u] - a0 <= cap
+      uint32_t lo = u, hi = nv + 1;
+      while (hi - lo > 1) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (hg->off[mid] - a0 <= cap) lo = mid; else hi = mid;
+      }
+      u = lo;
+    }
+    ctx->part_v.push_back(u);
+    ctx->part_a.push_back(hg->off[u]);
+    max_arcs = std::max<uint64_t>(max_arcs, hg->off[u] - a0);
+    v = u;
+  }
+  const uint32_t P = (uint32_t)ctx->part_v.size() - 1;
+  auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
+  const uint64_t b_pv = al(4ull * (P + 1)), b_st = al(4ull * (max_arcs ? max_arcs : 1));
+  const uint64_t total = b_pv + 2 * b_st;
+  if (ctx->device_bytes + total > ctx->budget) {
+    ctx->err = "out-of-core staging buffers do not fit the device budget";
+    return GEM_ERR_OOM;
+  }
+  char *p = nullptr;
+  if (cudaMalloc(&p, total) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->err = "cudaMalloc out-of-core staging buffers";
+    return GEM_ERR_OOM;
+  }
+  ctx->part_mem = p;
+  ctx->part_bytes = total;
+  ctx->device_bytes += total;
+  ctx->d_part_v = (uint32_t *)p;
+  ctx->d_stage[0] = (uint32_t *)(p + b_pv);
+  ctx->d_stage[1] = (uint32_t *)(p + b_pv + b_st);
+  CU(cudaMemcpyAsync(ctx->d_part_v, ctx->part_v.data(), 4ull * (P + 1), cudaMemcpyHostToDevice, ctx->s));
+  if (!ctx->s_copy) CU(cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking));
+  for (int b = 0; b < 2; ++b) {
+    if (!ctx->ev_ready[b]) CU(cudaEventCreateWithFlags(&ctx->ev_ready[b], cudaEventDisableTiming));
+    if (!ctx->ev_free[b]) CU(cudaEventCreateWithFlags(&ctx->ev_free[b], cudaEventDisableTiming));
+  }
+  ctx->ooc = gem_ooc_stats{};
+  ctx->ooc.partitions = P;
+  ctx->ooc.max_part_bytes = 4 * max_arcs;
+  return GEM_OK;
+}
+
+extern "C" gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out) {
+  if (!ctx || !out) return GEM_ERR_ARG;
+  *out = ctx->ooc;
+  return GEM_OK;
+}
 
 extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   if (!ctx || !hg) return GEM_ERR_ARG;
@@ -248,6 +331,8 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
     ctx->pinned_nbr = h;
     if (na) std::memcpy(h, hg->nbr.data(), 4ull * na);
     CU(cudaHostGetDevicePointer((void **)&d_nbr, h, 0));
+    const gem_status pst = ooc_partitions(ctx, hg);
+    if (pst != GEM_OK) return pst;
   } else if (na) {
     CU(cudaMemcpyAsync(d_nbr, hg->nbr.data(), 4ull * na, cudaMemcpyHostToDevice, ctx->s));
   }
@@ -748,7 +833,86 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   ST(aalloc(ctx, tiles ? tiles : 1, &d_mask));
   ST(aalloc(ctx, tiles + 1, &d_vp));
   ST(aalloc(ctx, scan_tmp_words(tiles), &d_tmp2));
-  launch_table_count(ctx->g, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, src_tiles, d_mask, ctx->s);
+  // Out-of-core: group the tiles by adjacency partition; stream the
+  // partitions they touch when those are filled enough (their bytes at most
+  // twice what the tiles would read from the mapped adjacency), else read in
+  // place.
+  const uint32_t nparts = ctx->part_v.empty() ? 0u : (uint32_t)ctx->part_v.size() - 1;
+  std::vector<uint64_t> pstart;
+  uint32_t *d_tord = nullptr;
+  bool streamed = false;
+  if (ctx->opts.ooc && nparts && ctx->opts.ooc_stream != 2 && src_tiles && src_tiles < (1ull << 32)) {
+    uint32_t *d_tpart, *d_hist;
+    ST(aalloc(ctx, src_tiles, &d_tpart));
+    ST(aalloc(ctx, nparts, &d_hist));
+    CU(cudaMemsetAsync(d_hist, 0, 4ull * nparts, ctx->s));
+    launch_tile_partition(d_src, d_tkey, d_tsrc, src_tiles, ctx->d_part_v, nparts, d_tpart, d_hist, ctx->s);
+    std::vector<uint32_t> hist(nparts);
+    CU(d2h_sync(ctx, hist.data(), d_hist, 4ull * nparts));
+    uint64_t need = 0;
+    for (uint32_t p = 0; p < nparts; ++p)
+      if (hist[p]) need += 4 * (ctx->part_a[p + 1] - ctx->part_a[p]);
+    streamed = ctx->opts.ooc_stream == 1 || need <= 2 * 128 * src_tiles;
+    if (streamed) {
+      pstart.assign(nparts + 1, 0);
+      for (uint32_t p = 0; p < nparts; ++p) pstart[p + 1] = pstart[p] + hist[p];
+      std::vector<uint32_t> cursor(nparts);
+      for (uint32_t p = 0; p < nparts; ++p) cursor[p] = (uint32_t)pstart[p];
+      CU(h2d(ctx, d_hist, cursor.data(), 4ull * nparts));
+      ST(aalloc(ctx, src_tiles, &d_tord));
+      launch_tile_scatter(d_tpart, src_tiles, nparts, d_hist, d_tord, ctx->s);
+    }
+  }
+  if (ctx->opts.ooc) ++(streamed ? ctx->ooc.waves_streamed : ctx->ooc.waves_in_place);
+  // One table pass (count or write) over every tile: in place, or partition
+  // by partition with the copy of the next partition (side stream, the other
+  // staging buffer) overlapping the kernel of the current one.
+  auto table_pass = [&](bool write) -> gem_status {
+    TabPass P;
+    P.off = ctx->g.off;
+    P.nbr = ctx->g.nbr;
+    P.arc_shift = 0;
+    P.tord = nullptr;
+    P.t0 = 0;
+    P.t1 = src_tiles;
+    if (!streamed) {
+      if (write)
+        launch_table_write(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, d_vp, w.d_values, w.d_vkey,
+                           ctx->s);
+      else
+        launch_table_count(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, ctx->s);
+      return GEM_OK;
+    }
+    // a staging buffer is free once the main stream has passed what used it
+    CU(cudaEventRecord(ctx->ev_free[0], ctx->s));
+    CU(cudaEventRecord(ctx->ev_free[1], ctx->s));
+    uint32_t k = 0;
+    for (uint32_t p = 0; p < nparts; ++p) {
+      if (pstart[p + 1] == pstart[p]) continue;
+      const int b = (int)(k++ & 1u);
+      const uint64_t a0 = ctx->part_a[p], bytes = 4 * (ctx->part_a[p + 1] - a0);
+      CU(cudaStreamWaitEvent(ctx->s_copy, ctx->ev_free[b], 0));
+      CU(cudaMemcpyAsync(ctx->d_stage[b], static_cast<const uint32_t *>(ctx->pinned_nbr) + a0, bytes,
+                         cudaMemcpyHostToDevice, ctx->s_copy));
+      CU(cudaEventRecord(ctx->ev_ready[b], ctx->s_copy));
+      CU(cudaStreamWaitEvent(ctx->s, ctx->ev_ready[b], 0));
+      P.nbr = ctx->d_stage[b];
+      P.arc_shift = a0;
+      P.tord = d_tord;
+      P.t0 = pstart[p];
+      P.t1 = pstart[p + 1];
+      if (write)
+        launch_table_write(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, d_vp, w.d_values, w.d_vkey,
+                           ctx->s);
+      else
+        launch_table_count(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, ctx->s);
+      CU(cudaEventRecord(ctx->ev_free[b], ctx->s));
+      ctx->ooc.parts_streamed += 1;
+      ctx->ooc.bytes_streamed += bytes;
+    }
+    return GEM_OK;
+  };
+  ST(table_pass(false));
   launch_scan(d_mask, SCAN_POPC_U32, tiles, d_vp, d_tmp2, ctx->s);
   uint64_t nvals = 0;
   CU(d2h_sync(ctx, &nvals, d_vp + tiles, 8));
@@ -757,8 +921,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   w.d_vkey = nullptr;
   if (key_map) ST(aalloc(ctx, nvals ? nvals : 1, &w.d_vkey));
   launch_table_offsets(d_src, d_edge, (uint32_t)edge.size(), d_tp, d_vp, offs, ctx->s);
-  launch_table_write(ctx->g, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, src_tiles, d_mask, d_vp, w.d_values,
-                     w.d_vkey, ctx->s);
+  ST(table_pass(true));
   CU(cudaGetLastError());
   w.edges = edge;
   w.table_values = nvals;
@@ -1189,26 +1352,41 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
     vs[i] = make_host_query(&qs[i], all[i], e);
     res[i].status = vs[i];
   }
-  // waves: as many queries as the per-wave row limit allows
+  // waves: as many queries as the per-wave row limit allows; a wave whose
+  // tables do not fit the device budget is split in halves and retried, down
+  // to single queries
   const uint32_t max_rows = ctx->wave_max_rows;
-  uint32_t i = 0, wave_no = 0;
-  gem_status first_err = GEM_OK;
-  while (i < n) {
-    Wave w;
+  std::deque<std::vector<uint32_t>> todo;
+  for (uint32_t i = 0; i < n;) {
     std::vector<uint32_t> ids;
     uint32_t rows = 0;
     while (i < n && (ids.empty() || rows + all[i].nv <= max_rows)) {
       if (vs[i] == GEM_OK) {
         ids.push_back(i);
         rows += all[i].nv;
-        w.q.push_back(all[i]);
       }
       ++i;
     }
-    if (ids.empty()) continue;
+    if (!ids.empty()) todo.push_back(std::move(ids));
+  }
+  uint32_t wave_no = 0;
+  gem_status first_err = GEM_OK;
+  while (!todo.empty()) {
+    std::vector<uint32_t> ids = std::move(todo.front());
+    todo.pop_front();
+    Wave w;
+    for (uint32_t id : ids) w.q.push_back(all[id]);
     ctx->arena.reset();
     gem_status st = run_wave(ctx, w, 0, mode, nullptr, 0);
     if (st != GEM_OK) {
+      cudaStreamSynchronize(ctx->s);  // the failed wave's copies and kernels are done before reuse
+      cudaGetLastError();
+      if (st == GEM_ERR_OOM && ids.size() > 1) {
+        const size_t h = ids.size() / 2;
+        todo.push_front(std::vector<uint32_t>(ids.begin() + h, ids.end()));
+        todo.push_front(std::vector<uint32_t>(ids.begin(), ids.begin() + h));
+        continue;
+      }
       for (uint32_t id : ids) res[id].status = st;
       if (first_err == GEM_OK) first_err = st;
       continue;

@@ -117,6 +117,17 @@ struct gem_ctx {
   const uint64_t *vnh_off = nullptr;
   const uint32_t *vnh_slots = nullptr;
   void *pinned_nbr = nullptr;        // out-of-core: mapped pinned adjacency
+  // out-of-core partition streaming: vertex ranges of at most ooc_part_kib
+  // KiB of adjacency, two device staging buffers and a side copy stream
+  std::vector<uint32_t> part_v;      // partition vertex bounds (partitions + 1)
+  std::vector<uint64_t> part_a;      // their arc bounds
+  char *part_mem = nullptr;          // d_part_v and both staging buffers
+  uint64_t part_bytes = 0;
+  uint32_t *d_part_v = nullptr;
+  uint32_t *d_stage[2] = {nullptr, nullptr};
+  cudaStream_t s_copy = nullptr;
+  cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  gem_ooc_stats ooc{};
   uint64_t graph_bytes = 0;
   std::vector<uint64_t> label_freq;  // vertices per label
   std::vector<uint64_t> label_arcs;  // sum of degrees per label

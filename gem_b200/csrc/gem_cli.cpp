@@ -4,7 +4,7 @@
 //
 //   gem -q <query file | directory of Q_<id>.in> -d <data graph> [-t N] [-g GPU]
 //       [--eviction POLICY] [--ooc] [--budget-gb X] [--mode count|hash]
-//       [--count-u32] [--time-cap-ms N]
+//       [--count-u32] [--time-cap-ms N] [--ooc-part-kib N] [--ooc-stream auto|always|never]
 //
 // Output lines follow the reference: per-phase "… time: <us> us" lines, two
 // "Join Time" lines, "=== Final Results ===" and
@@ -37,12 +37,15 @@ struct Args {
   bool ooc = false, u32 = false;
   double budget_gb = 0;
   unsigned time_cap_ms = 0;
+  unsigned ooc_part_kib = 0;  // out-of-core adjacency partition (0 = library default)
+  unsigned ooc_stream = 0;    // 0 auto, 1 always, 2 never
 };
 
 void usage() {
   std::fprintf(stderr,
                "usage: gem -q <query file|dir> -d <data graph> [-t 0..10] [-g GPU] [--eviction P]\n"
-               "           [--ooc] [--budget-gb X] [--mode count|hash] [--count-u32] [--time-cap-ms N]\n");
+               "           [--ooc] [--budget-gb X] [--mode count|hash] [--count-u32] [--time-cap-ms N]\n"
+               "           [--ooc-part-kib N] [--ooc-stream auto|always|never]\n");
 }
 
 bool parse(int argc, char **argv, Args &a) {
@@ -88,6 +91,19 @@ bool parse(int argc, char **argv, Args &a) {
     } else if (s == "--time-cap-ms") {
       if (!(v = need("--time-cap-ms"))) return false;
       a.time_cap_ms = (unsigned)std::atoi(v);
+    } else if (s == "--ooc-part-kib") {
+      if (!(v = need("--ooc-part-kib"))) return false;
+      a.ooc_part_kib = (unsigned)std::atoi(v);
+    } else if (s == "--ooc-stream") {
+      if (!(v = need("--ooc-stream"))) return false;
+      const std::string m = v;
+      if (m == "auto") a.ooc_stream = 0;
+      else if (m == "always") a.ooc_stream = 1;
+      else if (m == "never") a.ooc_stream = 2;
+      else {
+        std::fprintf(stderr, "ERROR: --ooc-stream must be auto, always or never\n");
+        return false;
+      }
     } else if (s == "-h" || s == "--help") {
       return false;
     } else {
@@ -235,6 +251,8 @@ int main(int argc, char **argv) {
   o.device_budget_bytes = (uint64_t)(a.budget_gb * (1ull << 30));
   o.ooc = a.ooc ? 1 : 0;
   o.time_cap_ms = a.time_cap_ms;
+  o.ooc_part_kib = a.ooc_part_kib;
+  o.ooc_stream = a.ooc_stream;
   gem_ctx *ctx = nullptr;
   st = gem_ctx_create(&o, &ctx);
   if (st == GEM_OK) st = gem_ctx_load_graph(ctx, hg);

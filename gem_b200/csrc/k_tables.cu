@@ -90,45 +90,48 @@ void launch_tile_keys(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, con
 // One warp per TILE_UNROLL consecutive source tiles: the tiles' key, vertex,
 // offsets and neighbour loads are independent and overlap; each tile is then
 // tested against (count) or copied for (write) every edge of its source, so
-// a source's adjacency is read once however many tables it keys.
+// a source's adjacency is read once however many tables it keys.  The warps
+// cover positions [t0, t1) of the tile order `tord` (identity when null), and
+// a key's arcs are read at nbr[arc - arc_shift]: the resident (or mapped)
+// adjacency with shift 0, or a streamed partition that starts at arc_shift.
 constexpr int TILE_UNROLL = 4;
 
 template <bool WRITE>
-__global__ void __launch_bounds__(256) table_src_kernel(DevGraph g, const TabSource *__restrict__ srcs,
+__global__ void __launch_bounds__(256) table_src_kernel(TabPass P, const TabSource *__restrict__ srcs,
                                                         const uint32_t *__restrict__ sedge,
                                                         const TabEdge *__restrict__ edges,
                                                         const uint64_t *__restrict__ tp,
                                                         const uint32_t *__restrict__ tkey,
-                                                        const uint32_t *__restrict__ tsrc, uint64_t ntile,
+                                                        const uint32_t *__restrict__ tsrc,
                                                         uint32_t *__restrict__ mask, const uint64_t *__restrict__ vp,
                                                         uint32_t *__restrict__ values, uint32_t *__restrict__ vkey) {
   const uint32_t lane = dev::lane_id();
   const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t base = (blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * TILE_UNROLL; base < ntile;
-       base += nwarps * TILE_UNROLL) {
+  for (uint64_t base = P.t0 + (blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * TILE_UNROLL;
+       base < P.t1; base += nwarps * TILE_UNROLL) {
     uint32_t x[TILE_UNROLL], sx[TILE_UNROLL], kx[TILE_UNROLL];
     uint64_t lt[TILE_UNROLL];
     bool xv[TILE_UNROLL];
 #pragma unroll
     for (int i = 0; i < TILE_UNROLL; ++i) {
-      const uint64_t t = base + i;
-      const bool tv = t < ntile;
+      const bool tv = base + i < P.t1;
+      const uint64_t t = !tv ? 0ull : P.tord ? (uint64_t)__ldg(P.tord + base + i) : base + i;
       const uint32_t k = tv ? __ldg(tkey + t) : 0u, sidx = tv ? __ldg(tsrc + t) : 0u;
       const uint64_t kb = srcs[sidx].key_base;
       const uint32_t *keys = srcs[sidx].keys;
       const uint32_t v = tv ? __ldg(keys + (k - kb)) : 0u;
       const uint64_t tk = tv ? __ldg(tp + k) : 0ull, stb = tv ? __ldg(tp + kb) : 0ull;
-      const uint64_t a0 = tv ? __ldg(g.off + v) : 0ull, a1 = tv ? __ldg(g.off + v + 1) : 0ull;
+      const uint64_t a0 = tv ? __ldg(P.off + v) : 0ull, a1 = tv ? __ldg(P.off + v + 1) : 0ull;
       const uint64_t arc = a0 + (t - tk) * 32 + lane;
       sx[i] = sidx;
       kx[i] = (uint32_t)(k - kb);  // the key's position in its source's candidate list
       lt[i] = t - stb;  // the tile's index among its source's tiles
       xv[i] = tv && arc < a1;
-      x[i] = xv[i] ? __ldg(g.nbr + arc) : 0u;
+      x[i] = xv[i] ? __ldg(P.nbr + (arc - P.arc_shift)) : 0u;
     }
 #pragma unroll
     for (int i = 0; i < TILE_UNROLL; ++i) {
-      if (base + i >= ntile) break;  // the same in every lane
+      if (base + i >= P.t1) break;  // the same in every lane
       const uint32_t e0 = __ldg(sedge + 2 * sx[i]), ne = __ldg(sedge + 2 * sx[i] + 1);
       for (uint32_t e = e0; e < e0 + ne; ++e) {
         const uint64_t et = edges[e].tile_base + lt[i];
@@ -157,23 +160,123 @@ static uint32_t src_tile_blocks(uint64_t ntile) {
   return (uint32_t)blocks;
 }
 
-void launch_table_count(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                        uint32_t *mask, cudaStream_t s) {
-  if (ntile == 0) return;
+void launch_table_count(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint32_t *mask,
+                        cudaStream_t s) {
+  if (P.t1 <= P.t0) return;
   count_launch();
-  table_src_kernel<false><<<src_tile_blocks(ntile), 256, 0, s>>>(g, d_src, sedge, d_edge, tp, tkey, tsrc, ntile, mask,
-                                                                  nullptr, nullptr, nullptr);
+  table_src_kernel<false><<<src_tile_blocks(P.t1 - P.t0), 256, 0, s>>>(P, d_src, sedge, d_edge, tp, tkey, tsrc, mask,
+                                                                        nullptr, nullptr, nullptr);
 }
 
-void launch_table_write(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, uint32_t *vkey,
-                        cudaStream_t s) {
+void launch_table_write(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, const uint32_t *mask,
+                        const uint64_t *vp, uint32_t *values, uint32_t *vkey, cudaStream_t s) {
+  if (P.t1 <= P.t0) return;
+  count_launch();
+  table_src_kernel<true><<<src_tile_blocks(P.t1 - P.t0), 256, 0, s>>>(P, d_src, sedge, d_edge, tp, tkey, tsrc,
+                                                                       const_cast<uint32_t *>(mask), vp, values, vkey);
+}
+
+// Partition of every source tile (by its key vertex: the partition whose
+// vertex range [part_v[p], part_v[p + 1]) holds it) and the tiles per
+// partition.  Partitions are few (adjacency bytes / partition size), so the
+// counts go through a shared-memory histogram when they fit one.
+__global__ void tile_partition_kernel(const TabSource *__restrict__ srcs, const uint32_t *__restrict__ tkey,
+                                      const uint32_t *__restrict__ tsrc, uint64_t ntile,
+                                      const uint32_t *__restrict__ part_v, uint32_t nparts,
+                                      uint32_t *__restrict__ tpart, uint32_t *__restrict__ hist) {
+  __shared__ uint32_t sh[TILE_PART_SMEM];
+  const bool local = nparts <= TILE_PART_SMEM;
+  if (local)
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ntile; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t sidx = __ldg(tsrc + t);
+    const uint32_t v = __ldg(srcs[sidx].keys + (__ldg(tkey + t) - srcs[sidx].key_base));
+    uint32_t lo = 0, hi = nparts;  // last p with part_v[p] <= v
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(part_v + mid) <= v) lo = mid; else hi = mid;
+    }
+    tpart[t] = lo;
+    if (local) atomicAdd(sh + lo, 1u); else atomicAdd(hist + lo, 1u);
+  }
+  __syncthreads();
+  if (local)
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x)
+      if (sh[i]) atomicAdd(hist + i, sh[i]);
+}
+
+// tord[cursor[p]++] = t for every tile t of partition p (cursor starts at the
+// partition's first position); the order within a partition is immaterial.
+// Partitions are few, so a per-tile global atomic would serialise on a
+// handful of cursors: each block counts a chunk of SCATTER_ITEMS tiles per
+// thread in shared memory (one atomic per warp and partition, lanes of the
+// same partition found with __match_any_sync), reserves each partition's
+// range with one global atomic, then writes.
+constexpr int SCATTER_ITEMS = 8;
+
+__global__ void __launch_bounds__(256) tile_scatter_kernel(const uint32_t *__restrict__ tpart, uint64_t ntile,
+                                                           uint32_t nparts, uint32_t *__restrict__ cursor,
+                                                           uint32_t *__restrict__ tord) {
+  __shared__ uint32_t cnt[TILE_PART_SMEM], base[TILE_PART_SMEM];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t chunk = (uint64_t)blockDim.x * SCATTER_ITEMS;
+  for (uint64_t c0 = blockIdx.x * chunk; c0 < ntile; c0 += (uint64_t)gridDim.x * chunk) {
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    uint32_t pp[SCATTER_ITEMS], off[SCATTER_ITEMS];
+#pragma unroll
+    for (int it = 0; it < SCATTER_ITEMS; ++it) {
+      const uint64_t t = c0 + (uint64_t)it * blockDim.x + threadIdx.x;
+      const uint32_t p = t < ntile ? __ldg(tpart + t) : 0xFFFFFFFFu;
+      const uint32_t peers = __match_any_sync(dev::FULL, p);
+      const uint32_t leader = __ffs(peers) - 1;
+      uint32_t o = 0;
+      if (lane == leader && p != 0xFFFFFFFFu) o = atomicAdd(cnt + p, (uint32_t)__popc(peers));
+      pp[it] = p;
+      off[it] = __shfl_sync(dev::FULL, o, leader) + __popc(peers & ((1u << lane) - 1u));
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) base[i] = cnt[i] ? atomicAdd(cursor + i, cnt[i]) : 0u;
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < SCATTER_ITEMS; ++it)
+      if (pp[it] != 0xFFFFFFFFu) tord[base[pp[it]] + off[it]] = (uint32_t)(c0 + (uint64_t)it * blockDim.x + threadIdx.x);
+    __syncthreads();  // cnt and base are reset by the next chunk
+  }
+}
+
+// Fallback for more partitions than the shared-memory tables hold.
+__global__ void tile_scatter_global_kernel(const uint32_t *__restrict__ tpart, uint64_t ntile,
+                                           uint32_t *__restrict__ cursor, uint32_t *__restrict__ tord) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ntile; t += (uint64_t)gridDim.x * blockDim.x)
+    tord[atomicAdd(cursor + __ldg(tpart + t), 1u)] = (uint32_t)t;
+}
+
+void launch_tile_partition(const TabSource *d_src, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
+                           const uint32_t *part_v, uint32_t nparts, uint32_t *tpart, uint32_t *hist, cudaStream_t s) {
+  if (ntile == 0) return;
+  uint64_t blocks = (ntile + 255) / 256;
+  if (blocks > 148ull * 8) blocks = 148ull * 8;
+  count_launch();
+  tile_partition_kernel<<<(uint32_t)blocks, 256, 0, s>>>(d_src, tkey, tsrc, ntile, part_v, nparts, tpart, hist);
+}
+
+void launch_tile_scatter(const uint32_t *tpart, uint64_t ntile, uint32_t nparts, uint32_t *cursor, uint32_t *tord,
+                         cudaStream_t s) {
   if (ntile == 0) return;
   count_launch();
-  table_src_kernel<true><<<src_tile_blocks(ntile), 256, 0, s>>>(g, d_src, sedge, d_edge, tp, tkey, tsrc, ntile,
-                                                                 const_cast<uint32_t *>(mask), vp, values, vkey);
+  if (nparts <= TILE_PART_SMEM) {
+    uint64_t blocks = (ntile + 256 * SCATTER_ITEMS - 1) / (256 * SCATTER_ITEMS);
+    if (blocks > 148ull * 8) blocks = 148ull * 8;
+    tile_scatter_kernel<<<(uint32_t)blocks, 256, 0, s>>>(tpart, ntile, nparts, cursor, tord);
+  } else {
+    uint64_t blocks = (ntile + 255) / 256;
+    if (blocks > 148ull * 32) blocks = 148ull * 32;
+    tile_scatter_global_kernel<<<(uint32_t)blocks, 256, 0, s>>>(tpart, ntile, cursor, tord);
+  }
 }
 
 __device__ __forceinline__ uint32_t find_edge_off(const TabEdge *__restrict__ e, uint32_t ne, uint64_t i) {

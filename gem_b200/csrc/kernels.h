@@ -114,12 +114,30 @@ void launch_key_tiles(const DevGraph &g, const TabSource *d_src, uint32_t nsrc, 
 // source-tile space (tp: exclusive scan of the key tiles).
 void launch_tile_keys(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp, uint32_t *tkey,
                       uint32_t *tsrc, cudaStream_t s);
+// One pass of the table kernels over positions [t0, t1) of a tile order
+// (tord; null = the tiles themselves): key arcs are read at
+// nbr[arc - arc_shift], with off the device offsets of the data graph.
+struct TabPass {
+  const uint64_t *off;
+  const uint32_t *nbr;
+  uint64_t arc_shift;
+  const uint32_t *tord;
+  uint64_t t0, t1;
+};
 // mask[edge.tile_base + i] = 32-bit membership mask of tile i of the edge's
 // source, for every edge of every source (sedge: {first edge, edges} per
 // source; a source's edges are consecutive).
-void launch_table_count(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                        uint32_t *mask, cudaStream_t s);
+void launch_table_count(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint32_t *mask,
+                        cudaStream_t s);
+// Out-of-core partition streaming: tpart[t] = partition of tile t's key vertex
+// (part_v: nparts + 1 vertex bounds), hist[p] += tiles of partition p; then
+// the tiles grouped by partition into tord (cursor[p] = first position of p).
+constexpr uint32_t TILE_PART_SMEM = 4096;
+void launch_tile_partition(const TabSource *d_src, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
+                           const uint32_t *part_v, uint32_t nparts, uint32_t *tpart, uint32_t *hist, cudaStream_t s);
+void launch_tile_scatter(const uint32_t *tpart, uint64_t ntile, uint32_t nparts, uint32_t *cursor, uint32_t *tord,
+                         cudaStream_t s);
 // out[i] = tp[d_src[i].key_base] for i < nsrc, out[nsrc] = tp[nkeys].
 void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp,
                               uint64_t *out, cudaStream_t s);
@@ -127,10 +145,9 @@ void launch_table_offsets(const TabSource *d_src, const TabEdge *d_edge, uint32_
                           const uint64_t *tp, const uint64_t *vp, uint64_t total_offsets,
                           cudaStream_t s);
 constexpr uint32_t TAB_KEY_MAP = 1;
-void launch_table_write(const DevGraph &g, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                        const uint32_t *mask, const uint64_t *vp, uint32_t *values, uint32_t *vkey,
-                        cudaStream_t s);
+void launch_table_write(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
+                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, const uint32_t *mask,
+                        const uint64_t *vp, uint32_t *values, uint32_t *vkey, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Cuckoo hash: vertex id -> position in C(u).  Two bucketised tables of

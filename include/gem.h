@@ -139,13 +139,38 @@ typedef struct gem_opts {
   uint32_t time_cap_ms;         /* per-query/batch device time cap (0 = 600000) */
   uint32_t index_kind;          /* 0 = auto, 1 = rank bitmap, 2 = cuckoo hash */
   uint32_t admit_gb;            /* serving admission budget in GiB (0 = 120) */
-  uint32_t reserved[5];
+  uint32_t ooc_part_kib;        /* out-of-core: adjacency partition streamed per table pass, KiB (0 = 16384) */
+  uint32_t ooc_stream;          /* out-of-core table builds: 0 = stream partitions when the wave's
+                                   sources fill them enough, 1 = always stream, 2 = never (read the
+                                   mapped adjacency in place) */
+  uint32_t reserved[3];
 } gem_opts;
 
 gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out);
 void gem_ctx_destroy(gem_ctx *ctx);
 /* Thread-local description of the last failure on this context. */
 const char *gem_last_error(const gem_ctx *ctx);
+
+/* Out-of-core partition streaming counters of a context, cumulative since
+ * its graph was loaded (no counterpart in the reference, whose out-of-core
+ * mode keeps the data graph on the host and pages intermediate tries,
+ * out-of-core/lib/structure/src/memory_manager.cu:196-839).  In out-of-core
+ * mode the adjacency is split at load time into vertex ranges of at most
+ * ooc_part_kib KiB (a vertex whose list is longer gets a partition of its
+ * own); a table build either streams the partitions its sources touch into
+ * two device staging buffers on a side stream, each copy overlapping the
+ * table kernels of the previous partition, or reads the mapped adjacency in
+ * place. */
+typedef struct gem_ooc_stats {
+  uint32_t partitions;          /* partitions of the loaded graph */
+  uint32_t reserved0;
+  uint64_t max_part_bytes;      /* largest partition (each staging buffer's size) */
+  uint64_t waves_streamed;      /* table builds that streamed partitions */
+  uint64_t waves_in_place;      /* table builds that read the mapped adjacency */
+  uint64_t parts_streamed;      /* partition copies issued (two table passes per build) */
+  uint64_t bytes_streamed;      /* bytes those copies moved */
+} gem_ooc_stats;
+gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out);
 
 /* Upload (in-core) or pin (out-of-core) a host graph; derived per-graph
  * indexes (degrees, neighbour-label counts) are built on the device.

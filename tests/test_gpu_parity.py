@@ -313,6 +313,63 @@ def test_out_of_core_same_counts(small):
             assert (ra["count"], ra["emb_hash"]) == (rb["count"], rb["emb_hash"])
 
 
+def test_out_of_core_partition_streaming_same_counts(small):
+    """Out-of-core table builds that stream adjacency partitions (1 KiB each, so
+    hub lists get partitions of their own) or read the mapped adjacency in place
+    give the in-core counts and hashes, one query at a time and batched."""
+    qs = [q for q in gem.gen_queries(small, 5, gem.ANY, 6, seed=6200)
+          if oracle.count(small, q, want_hash=False, work_cap=100_000_000)[2]]
+    opts = dict(time_cap_ms=30000, ooc=True, budget_bytes=2 << 30, ooc_part_kib=1)
+    with gem.Context(time_cap_ms=30000) as a, gem.Context(ooc_stream=1, **opts) as b, \
+            gem.Context(ooc_stream=2, **opts) as c:
+        for x in (a, b, c):
+            x.load_graph(small)
+        st = b.ooc_stats()
+        assert st["partitions"] > 16 and st["max_part_bytes"] > 1024  # some vertex list exceeds 1 KiB
+        for q in qs:
+            ra = a.run(q, mode=gem.MODE_HASH)
+            for x in (b, c):
+                rx = x.run(q, mode=gem.MODE_HASH)
+                assert (rx["count"], rx["emb_hash"]) == (ra["count"], ra["emb_hash"])
+        _, rs_a = a.batch(qs, mode=gem.MODE_HASH)
+        _, rs_b = b.batch(qs, mode=gem.MODE_HASH)
+        assert [(r["count"], r["emb_hash"]) for r in rs_b] == [(r["count"], r["emb_hash"]) for r in rs_a]
+        sb, sc = b.ooc_stats(), c.ooc_stats()
+        assert sb["waves_streamed"] >= len(qs) + 1 and sb["waves_in_place"] == 0
+        assert sb["parts_streamed"] >= 2 * sb["waves_streamed"] and sb["bytes_streamed"] > 0
+        assert sc["waves_streamed"] == 0 and sc["waves_in_place"] == len(qs) and sc["bytes_streamed"] == 0
+
+
+def test_batch_splits_waves_under_a_tight_budget(small, gctx):
+    """A wave whose tables exceed the device budget is split and retried: at the
+    smallest budget that runs the batch, every result equals the plain run's and
+    the batch took more than one wave."""
+    qs = [q for k in (4, 5) for q in gem.gen_queries(small, k, gem.ANY, 40, seed=6300 + k)]
+    plain = [gctx.run(q, mode=gem.MODE_HASH) for q in qs]
+    assert all(p["status"] == "OK" for p in plain)
+    _, one = gctx.batch(qs, mode=gem.MODE_HASH)
+    assert len({r["wave"] for r in one}) == 1
+    # budgets rise in 256 KiB steps: the first one that runs every query holds
+    # the largest single query's wave but not the whole batch's
+    found = None
+    for kib in range(4096, 65536, 256):
+        try:
+            c = gem.Context(time_cap_ms=30000, budget_bytes=kib << 10)
+            c.load_graph(small)
+        except gem.GemError:
+            continue
+        with c:
+            st, rs = c.batch(qs, mode=gem.MODE_HASH)
+        if all(r["status"] == "OK" for r in rs):
+            found = (kib, rs)
+            break
+        assert all(r["status"] in ("OK", "ERR_OOM") for r in rs)
+    assert found is not None
+    kib, rs = found
+    assert [(r["count"], r["emb_hash"]) for r in rs] == [(p["count"], p["emb_hash"]) for p in plain]
+    assert len({r["wave"] for r in rs}) > 1, kib
+
+
 def test_autotune_keeps_results(small):
     qs = []
     for k in (3, 4, 6):
