@@ -18,6 +18,11 @@ bounded step; the section reports, per query under a device time cap,
 whether it completed and the enumeration rate.  A query that exceeds the cap
 is reported as capped, never as an exact count.
 
+Its `out_of_core` part runs one batch of 4-vertex queries on that graph in
+core, out of core with the adjacency streamed in partitions, and out of core
+reading the pinned adjacency in place, and reports each mode's table-build
+and wave times with equal counts.
+
 The `serving` section submits the headline queries one by one through
 gem_submit / gem_poll under Poisson arrivals (1,000 / 5,000 / 20,000 per
 second, one second each) and reports latency percentiles and the achieved
@@ -263,7 +268,15 @@ def run_gem(args):
     if rank == 0 and args.serve_seconds > 0:
         ref = {i: r["count"] for i, r in enumerate(res_all[0])} if len(batch_of(args.warmup)) == len(pool) else {}
         serving = serving_section(gem, args, local, g, pool, ref) if ref else None
-    c2 = rmat22_section(gem, args, local) if rank == 0 and args.c2_sample > 0 else None
+    c2 = None
+    if rank == 0 and (args.c2_sample > 0 or args.ooc_sample > 0):
+        t = time.time()
+        g22 = gem.HostGraph.rmat(22, 16, seed=0x47454D00 + 22).set_labels(16, 1.0, seed=(0x47454D00 + 22) ^ 0x4C)
+        gen22 = time.time() - t
+        c2 = rmat22_section(gem, args, local, g22, gen22) if args.c2_sample > 0 else {"graph_gen_s": round(gen22, 2)}
+        if args.ooc_sample > 0:
+            c2["out_of_core"] = out_of_core_section(gem, args, local, g22)
+        del g22
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -377,12 +390,9 @@ def profiled_traffic(key):
     return None, None
 
 
-def rmat22_section(gem, args, local):
+def rmat22_section(gem, args, local, g, gen_s):
     """Scale-22 R-MAT with 16 Zipf(1.0) labels and the 8s/8d/16s/16d query sets:
     per query, plain run under a device time cap (status, count, nodes/s)."""
-    t = time.time()
-    g = gem.HostGraph.rmat(22, 16, seed=0x47454D00 + 22).set_labels(16, 1.0, seed=(0x47454D00 + 22) ^ 0x4C)
-    gen_s = time.time() - t
     per = max(1, args.c2_sample // len(SETS))
     out = {"workload": "rmat22-ef16-zipf16", "time_cap_ms": args.c2_cap_ms, "graph_gen_s": round(gen_s, 2),
            "queries": []}
@@ -398,6 +408,53 @@ def rmat22_section(gem, args, local):
                                        "join_ms": round(r["ms"]["join"], 1),
                                        "prefix_matches_per_s": r["nodes"] / js if js > 0 else None})
     out["exact"] = sum(1 for x in out["queries"] if x["status"] == "OK")
+    return out
+
+
+def out_of_core_section(gem, args, local, g):
+    """The scale-22 graph out of core: one batch of random-walk 4-vertex queries
+    run in core, out of core with streamed adjacency partitions and out of
+    core reading the pinned adjacency in place.  Per mode the median over 3
+    batches of the table-build and wave device times (CUDA events) and the
+    streaming counters; the counts must be equal in every mode."""
+    import torch
+    dev = torch.device("cuda", local)
+    h = torch.empty((64 << 20) // 4, dtype=torch.int32).pin_memory()
+    d = torch.empty(h.shape, dtype=torch.int32, device=dev)
+    for _ in range(3):
+        d.copy_(h, non_blocking=True)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(8):
+        d.copy_(h, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    h2d_gbs = 8 * (64 << 20) / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    del h, d
+    qs = gem.gen_queries(g, 4, gem.ANY, args.ooc_sample, seed=0x00C0)
+    out = {"queries": len(qs), "query_set": "4a", "adjacency_bytes": 4 * int(g.info()["n_arcs"]),
+           "pinned_h2d_gbs": round(h2d_gbs, 1), "modes": {}}
+    counts = {}
+    for name, kw in (("in_core", {}), ("streamed", dict(ooc=True, ooc_stream=1)),
+                     ("in_place", dict(ooc=True, ooc_stream=2))):
+        with gem.Context(device=local, time_cap_ms=args.c2_cap_ms * 10, **kw) as c:
+            c.load_graph(g)
+            c.batch(qs)
+            tab, tot = [], []
+            for _ in range(3):
+                _, rs = c.batch(qs)
+                waves = {}
+                for r in rs:
+                    waves.setdefault(r["wave"], r)
+                tab.append(sum(w["ms"]["tables"] for w in waves.values()))
+                tot.append(sum(w["ms"]["total"] for w in waves.values()))
+            counts[name] = [r["count"] if r["status"] == "OK" else None for r in rs]
+            m = {"tables_ms": round(sorted(tab)[1], 2), "wave_ms": round(sorted(tot)[1], 2)}
+            if kw:
+                m["stats"] = c.ooc_stats()
+            out["modes"][name] = m
+    out["counts_equal"] = all(v == counts["in_core"] for v in counts.values()) and None not in counts["in_core"]
     return out
 
 
@@ -466,6 +523,8 @@ def main():
     ap.add_argument("--plain", type=int, default=100)
     ap.add_argument("--autotune", type=int, default=1)
     ap.add_argument("--c2-sample", type=int, default=8, help="scale-22 queries in the rmat22 section (0 = skip)")
+    ap.add_argument("--ooc-sample", type=int, default=50,
+                    help="4-vertex queries of the out-of-core comparison on the scale-22 graph (0 = skip)")
     ap.add_argument("--c2-cap-ms", type=int, default=1000)
     ap.add_argument("--cpu-sample", type=int, default=8)
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="per arrival rate in the serving section (0 = skip)")
