@@ -526,7 +526,7 @@ def main():
     ap.add_argument("--ooc-sample", type=int, default=50,
                     help="4-vertex queries of the out-of-core comparison on the scale-22 graph (0 = skip)")
     ap.add_argument("--c2-cap-ms", type=int, default=1000)
-    ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--cpu-sample", type=int, default=100, help="pool queries timed on the CPU oracle (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="per arrival rate in the serving section (0 = skip)")
     ap.add_argument("--serve-rates", default="1000,5000,20000", help="Poisson arrival rates (queries/s)")
     ap.add_argument("--cpu-work-cap", type=int, default=1_000_000_000)
