@@ -58,6 +58,25 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def batch_indices(step, rank, world, batch, pool_len):
+    """Pool indices of one rank's batch at a step: the ranks of a step take
+    consecutive batches of the cycled pool (weak scaling, no shared query)."""
+    i = (step * world + rank) * batch
+    return [(i + j) % pool_len for j in range(batch)]
+
+
+def reduce_over_ranks(dist, tdev, twall, exact, emb, capped, e2e_exact):
+    """Whole-job figures: the slowest rank's device and wall times, the sums of
+    the per-rank counts (every rank calls this, in the same order)."""
+    import torch
+    t = torch.tensor([tdev, twall, float(exact), float(emb), float(capped), float(e2e_exact)], dtype=torch.float64)
+    mx = t[:2].clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t[2:].clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(mx[1]), int(sm[0]), int(sm[1]), int(sm[2]), int(sm[3])
+
+
 class Clocks:
     """nvidia-smi sampler during the timed region."""
 
@@ -177,8 +196,7 @@ def run_gem(args):
     tuned = ctx.autotune(pool[: min(len(pool), args.batch)], trial_cap_ms=args.cap_ms) if args.autotune else {}
 
     def batch_of(step):
-        i = (step * world + rank) * B
-        return [pool[(i + j) % len(pool)] for j in range(B)]
+        return [pool[i] for i in batch_indices(step, rank, world, B, len(pool))]
 
     # warm-up (compiles nothing; touches code paths and the arena)
     for s in range(args.warmup):
@@ -236,13 +254,7 @@ def run_gem(args):
     jb = jbytes
     jt = jms / 1e3
     if dist:
-        t = torch.tensor([tdev, twall, float(exact), float(emb), float(capped), float(e2e_exact)], dtype=torch.float64)
-        mx = t.clone()
-        dist.all_reduce(mx[:2], op=dist.ReduceOp.MAX)
-        sm = t[2:].clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        tdev, twall = float(mx[0]), float(mx[1])
-        exact, emb, capped, e2e_exact = int(sm[0]), int(sm[1]), int(sm[2]), int(sm[3])
+        tdev, twall, exact, emb, capped, e2e_exact = reduce_over_ranks(dist, tdev, twall, exact, emb, capped, e2e_exact)
     # plain mode: the same queries, one gem_query_run each (rank 0)
     plain = {}
     if rank == 0 and args.plain > 0:
