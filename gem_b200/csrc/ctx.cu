@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -597,27 +598,6 @@ struct EvPair {
   cudaEvent_t a, b;
 };
 
-static void fill_filter_desc(const HostQuery &q, uint32_t threshold, uint32_t row_base, FilterDesc &d) {
-  std::memset(&d, 0, sizeof d);
-  d.nq = q.nv;
-  d.threshold = threshold;
-  d.row_base = row_base;
-  for (uint32_t u = 0; u < q.nv; ++u) {
-    d.lab[u] = q.lab[u];
-    d.deg[u] = q.deg(u);
-    uint32_t k = 0;
-    while (k < d.nql && d.ql[k] != q.lab[u]) ++k;
-    if (k == d.nql) d.ql[d.nql++] = q.lab[u];
-  }
-  for (uint32_t u = 0; u < q.nv; ++u)
-    for (uint32_t w = 0; w < q.nv; ++w)
-      if (q.adj[u] & (1u << w)) {
-        uint32_t k = 0;
-        while (d.ql[k] != q.lab[w]) ++k;
-        d.nlc[u][k]++;
-      }
-}
-
 static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0;
   if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
@@ -685,12 +665,63 @@ static cudaError_t d2h_sync(gem_ctx *ctx, void *dst, const void *src, size_t byt
 static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   const uint32_t nwords = (ctx->g.nv + 31) / 32;
   w.nwords = nwords;
-  uint32_t rows = 0;
-  std::vector<FilterDesc> fd(w.q.size());
+  // Rows.  The filter predicate of a query vertex depends only on its label,
+  // its degree and its neighbours' labels, so vertices that agree on the
+  // three (in one query or in several) share one row: its candidate list,
+  // rank bitmap and the tables it keys.
+  std::map<std::vector<uint32_t>, uint32_t> row_by_sig;
+  std::vector<std::vector<uint32_t>> row_sig;
+  w.row_of.assign(w.q.size(), std::vector<uint32_t>());
   for (size_t i = 0; i < w.q.size(); ++i) {
-    w.row_base[i] = rows;
-    fill_filter_desc(w.q[i], threshold, rows, fd[i]);
-    rows += w.q[i].nv;
+    const HostQuery &q = w.q[i];
+    w.row_of[i].resize(q.nv);
+    for (uint32_t u = 0; u < q.nv; ++u) {
+      std::vector<uint32_t> sig{q.lab[u], q.deg(u)};
+      for (uint32_t v = 0; v < q.nv; ++v)
+        if (q.adj[u] & (1u << v)) sig.push_back(q.lab[v]);
+      std::sort(sig.begin() + 2, sig.end());
+      if (w.share_rows) {
+        const auto it = row_by_sig.find(sig);
+        if (it != row_by_sig.end()) {
+          w.row_of[i][u] = it->second;
+          continue;
+        }
+        row_by_sig.emplace(sig, (uint32_t)row_sig.size());
+      }
+      w.row_of[i][u] = (uint32_t)row_sig.size();
+      row_sig.push_back(std::move(sig));
+    }
+  }
+  const uint32_t rows = (uint32_t)row_sig.size();
+  // descriptors: runs of up to QV rows whose neighbour labels number at most QV
+  std::vector<FilterDesc> fd;
+  for (uint32_t r = 0; r < rows;) {
+    FilterDesc d;
+    std::memset(&d, 0, sizeof d);
+    d.threshold = threshold;
+    d.row_base = r;
+    while (r < rows && d.nq < QV) {
+      const std::vector<uint32_t> &sg = row_sig[r];
+      uint32_t extra = 0;
+      for (size_t i = 2; i < sg.size(); ++i) {
+        bool seen = false;
+        for (uint32_t k = 0; k < d.nql && !seen; ++k) seen = d.ql[k] == sg[i];
+        for (size_t j = 2; j < i && !seen; ++j) seen = sg[j] == sg[i];
+        extra += seen ? 0u : 1u;
+      }
+      if (d.nq && d.nql + extra > QV) break;
+      d.lab[d.nq] = sg[0];
+      d.deg[d.nq] = sg[1];
+      for (size_t i = 2; i < sg.size(); ++i) {
+        uint32_t k = 0;
+        while (k < d.nql && d.ql[k] != sg[i]) ++k;
+        if (k == d.nql) d.ql[d.nql++] = sg[i];
+        d.nlc[d.nq][k]++;
+      }
+      ++d.nq;
+      ++r;
+    }
+    fd.push_back(d);
   }
   w.nrows = rows;
   FilterDesc *d_fd;
@@ -720,15 +751,15 @@ static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   launch_compact(w.d_rb, d_ex, rows, nwords, d_cbase, w.d_cand, ctx->s);
   CU(cudaGetLastError());
   w.cand_total = total;
-  // algorithmic bytes: labels + degrees of every vertex, the label-count rows
-  // of vertices whose label occurs in the query, the bit rows (write, scan,
-  // rank rewrite) and the candidate lists.
+  // algorithmic bytes, per descriptor: labels + degrees of every vertex, the
+  // label-count rows of vertices whose label occurs in its rows' neighbour
+  // labels, its bit rows (write, scan, rank rewrite); then the candidate lists.
   uint64_t b = 0;
-  for (size_t i = 0; i < w.q.size(); ++i) {
+  for (const FilterDesc &d : fd) {
     uint64_t lb = 8ull * ctx->g.nv;
-    for (uint32_t k = 0; k < fd[i].nql; ++k)
-      if (fd[i].ql[k] < ctx->label_freq.size()) lb += (uint64_t)ctx->g.nlc_stride * ctx->label_freq[fd[i].ql[k]];
-    lb += 8ull * nwords * w.q[i].nv * 4;
+    for (uint32_t k = 0; k < d.nql; ++k)
+      if (d.ql[k] < ctx->label_freq.size()) lb += (uint64_t)ctx->g.nlc_stride * ctx->label_freq[d.ql[k]];
+    lb += 8ull * nwords * d.nq * 4;
     b += lb;
   }
   w.bytes_filter = b + 4 * total;
@@ -747,7 +778,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
     const Plan &p = w.plan[qi];
     for (uint32_t k = 1; k < p.n; ++k)
       for (uint32_t j : p.back[k]) {
-        const uint32_t r = w.row_base[qi] + p.order[j];
+        const uint32_t r = w.row_of[qi][p.order[j]];
         if (row_src[r] < 0) {
           row_src[r] = (int)src.size();
           TabSource s;
@@ -791,19 +822,31 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
     w.edge_of[qi].assign((size_t)p.n * QV, UINT32_MAX);
     for (uint32_t k = 1; k < p.n; ++k)
       for (uint32_t j : p.back[k])
-        reqs.push_back({(uint32_t)row_src[w.row_base[qi] + p.order[j]], (uint32_t)qi, j, k});
+        reqs.push_back({(uint32_t)row_src[w.row_of[qi][p.order[j]]], (uint32_t)qi, j, k});
   }
   std::stable_sort(reqs.begin(), reqs.end(), [](const EdgeReq &x, const EdgeReq &y) { return x.s < y.s; });
   std::vector<uint32_t> sedge(2 * src.size(), 0);
   uint64_t tiles = 0, offs = 0;
   bool key_map = false;
+  // a table is keyed by its source row and filtered by its target row: queries
+  // (or twin query vertices) that need the same pair share one table
+  std::map<std::pair<uint32_t, uint32_t>, uint32_t> edge_by_rows;
   for (const EdgeReq &rq : reqs) {
     const Plan &p = w.plan[rq.qi];
+    const uint32_t tgt = w.row_of[rq.qi][p.order[rq.k]];
+    const uint32_t flags = (rq.qi < w.pair.size() && w.pair[rq.qi] && rq.j == 0 && rq.k == 1) ? TAB_KEY_MAP : 0u;
+    key_map |= flags != 0;
+    const auto found = edge_by_rows.find({rq.s, tgt});
+    if (found != edge_by_rows.end()) {
+      edge[found->second].flags |= flags;
+      w.edge_of[rq.qi][rq.j * QV + rq.k] = found->second;
+      continue;
+    }
+    edge_by_rows.emplace(std::make_pair(rq.s, tgt), (uint32_t)edge.size());
     TabEdge e;
     e.src = rq.s;
-    e.flags = (rq.qi < w.pair.size() && w.pair[rq.qi] && rq.j == 0 && rq.k == 1) ? TAB_KEY_MAP : 0u;
-    key_map |= e.flags != 0;
-    e.rb_w = w.d_rb + (uint64_t)(w.row_base[rq.qi] + p.order[rq.k]) * w.nwords;
+    e.flags = flags;
+    e.rb_w = w.d_rb + (uint64_t)tgt * w.nwords;
     e.tile_base = tiles;
     e.ntiles = stb[rq.s + 1] - stb[rq.s];
     e.off_base = offs;
@@ -943,7 +986,7 @@ static gem_status wave_index(gem_ctx *ctx, Wave &w) {
     for (uint32_t k = 0; k < p.n; ++k) {
       w.idx_kind[qi][k] = IDX_NONE;
       if (k == 0 || !p.need_idx[k]) continue;
-      const uint32_t r = w.row_base[qi] + p.order[k];
+      const uint32_t r = w.row_of[qi][p.order[k]];
       uint32_t kind = ctx->opts.index_kind;
       if (kind == 0) kind = IDX_RANK;
       w.idx_kind[qi][k] = kind;
@@ -1028,7 +1071,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
     }
     J.flat = flat_code(p, mode);
     J.root_u = p.order[0];
-    const uint32_t r0 = w.row_base[qi] + p.order[0];
+    const uint32_t r0 = w.row_of[qi][p.order[0]];
     J.root_cand = w.d_cand + w.c_base[r0];
     J.n_root = w.cnt[r0];
     J.root_base = roots;
@@ -1039,7 +1082,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
       L.back_base = (uint32_t)jb.size();
       L.dup_mask = p.dup_mask[k];
       L.idx_kind = k == 0 ? IDX_NONE : w.idx_kind[qi][k];
-      L.rb = w.d_rb + (uint64_t)(w.row_base[qi] + p.order[k]) * w.nwords;
+      L.rb = w.d_rb + (uint64_t)w.row_of[qi][p.order[k]] * w.nwords;
       L.ck = w.ck_of[qi][k];
       for (uint32_t j : p.back[k]) {
         const uint32_t ei = w.edge_of[qi][j * QV + k];
@@ -1049,7 +1092,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
         }
         JBack b;
         b.lvl = j;
-        b.nkeys = w.cnt[w.row_base[qi] + p.order[j]];
+        b.nkeys = w.cnt[w.row_of[qi][p.order[j]]];
         b.off = w.edges[ei].offsets;
         jb.push_back(b);
       }
@@ -1206,7 +1249,7 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
   CU(cudaSetDevice(ctx->opts.device));
   const uint64_t launches0 = g_launches.load();
   const size_t nq = w.q.size();
-  w.row_base.assign(nq, 0);
+  w.row_of.assign(nq, {});
   w.active.assign(nq, 1);
   w.plan.assign(nq, Plan());
   w.idx_kind.assign(nq, std::vector<uint32_t>(QV, 0));
@@ -1232,13 +1275,16 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
   for (size_t qi = 0; qi < nq; ++qi) {
     const HostQuery &q = w.q[qi];
     bool empty = false;
-    for (uint32_t u = 0; u < q.nv; ++u)
-      if (w.cnt[w.row_base[qi] + u] == 0) empty = true;
+    uint32_t qcnt[QV];
+    for (uint32_t u = 0; u < q.nv; ++u) {
+      qcnt[u] = w.cnt[w.row_of[qi][u]];
+      if (qcnt[u] == 0) empty = true;
+    }
     if (empty) {
       w.active[qi] = 0;
       continue;
     }
-    make_plan(q, &w.cnt[w.row_base[qi]], mode == GEM_MODE_COUNT && ctx->closed_form_suffix, w.plan[qi]);
+    make_plan(q, qcnt, mode == GEM_MODE_COUNT && ctx->closed_form_suffix, w.plan[qi]);
     std::string why;
     if (!validate_plan(q, w.plan[qi], why)) {
       ctx->err = "internal: invalid plan (" + why + ")";
@@ -1275,7 +1321,7 @@ void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r) {
   if (o.pad[0]) r->status = w.join_err == 1 || w.join_err == 0 ? GEM_ERR_TIMEOUT : GEM_ERR_INTERNAL;
   else if (w.join_err > 1) r->status = GEM_ERR_INTERNAL;
   uint64_t ct = 0;
-  for (uint32_t u = 0; u < w.q[qi].nv; ++u) ct += w.cnt[w.row_base[qi] + u];
+  for (uint32_t u = 0; u < w.q[qi].nv; ++u) ct += w.cnt[w.row_of[qi][u]];
   r->cand_total = ct;
   r->n_tables = w.active[qi] ? 0 : 0;
   if (w.active[qi]) {
@@ -1414,7 +1460,7 @@ extern "C" gem_status gem_filter(gem_ctx *ctx, const gem_query *q, uint32_t thre
   w.q.resize(1);
   ST(make_host_query(q, w.q[0], ctx->err));
   ctx->arena.reset();
-  w.row_base.assign(1, 0);
+  w.share_rows = false;  // rows in query-vertex order, one each
   ST(wave_filter(ctx, w, threshold));
   CU(cudaStreamSynchronize(ctx->s));
   for (uint32_t u = 0; u < q->nv; ++u) counts[u] = w.cnt[u];
@@ -1435,7 +1481,7 @@ extern "C" gem_status gem_edge_table(gem_ctx *ctx, const gem_query *q, uint32_t 
   const HostQuery &hq = w.q[0];
   if (u >= hq.nv || wv >= hq.nv || !(hq.adj[u] & (1u << wv))) return GEM_ERR_ARG;
   ctx->arena.reset();
-  w.row_base.assign(1, 0);
+  w.share_rows = false;  // rows in query-vertex order, one each
   w.active.assign(1, 1);
   ST(wave_filter(ctx, w, 0));
   // a two-level plan: u then w
@@ -1471,7 +1517,7 @@ extern "C" gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t
   ST(make_host_query(q, w.q[0], ctx->err));
   if (u >= w.q[0].nv) return GEM_ERR_ARG;
   ctx->arena.reset();
-  w.row_base.assign(1, 0);
+  w.share_rows = false;  // rows in query-vertex order, one each
   w.active.assign(1, 1);
   w.idx_kind.assign(1, std::vector<uint32_t>(QV, 0));
   w.ck_of.assign(1, std::vector<const CuckooTable *>(QV, nullptr));

@@ -53,7 +53,10 @@ void make_plan(const gem::HostQuery &q, const uint32_t *cnt, bool count_suffix, 
 // One wave: a set of queries processed by shared launches.
 struct Wave {
   std::vector<gem::HostQuery> q;
-  std::vector<uint32_t> row_base;   // first filter row of each query
+  // Filter rows: one per distinct (label, degree, neighbour labels) among the
+  // wave's query vertices, which have the same candidates in every query.
+  std::vector<std::vector<uint32_t>> row_of;  // per query, per query vertex: its row
+  bool share_rows = true;           // false: one row per query vertex (the phase entry points)
   std::vector<uint8_t> active;      // 0 = some C(u) empty (count 0)
   std::vector<Plan> plan;
   std::vector<std::vector<uint32_t>> idx_kind;  // per query, per level
