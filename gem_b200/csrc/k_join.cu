@@ -516,7 +516,9 @@ __device__ uint64_t lane_subset_count3(const JoinArgs &a, const LaneCtx &x, uint
   const uint64_t len = shi - slo;
   const int ss = cache_slot(x.lc, slo, shi);
   const bool hash = a.vnh_off != nullptr;
-  if (nl == 1) {
+  // Lists with one range are one list (members that share a filter row and
+  // key levels share their tables): the intersection is the list itself.
+  if (nl == 1 || (alo == slo && ahi == shi && (nl < 3 || (blo == slo && bhi == shi)))) {
     uint64_t c = len, cur = slo;
     for (uint32_t dm = dup_mask; dm; dm &= dm - 1) {
       const uint32_t j = __ffs(dm) - 1;
