@@ -280,6 +280,7 @@ static gem_status ooc_partitions(gem_ctx *ctx, const gem_hgraph *hg) {
 
 extern "C" gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out) {
   if (!ctx || !out) return GEM_ERR_ARG;
+  if (ctx->server) return GEM_ERR_STATE;  // the serving thread updates the counters
   *out = ctx->ooc;
   return GEM_OK;
 }

@@ -170,6 +170,7 @@ typedef struct gem_ooc_stats {
   uint64_t parts_streamed;      /* partition copies issued (two table passes per build) */
   uint64_t bytes_streamed;      /* bytes those copies moved */
 } gem_ooc_stats;
+/* GEM_ERR_STATE while the context serves (gem_submit): its waves update the counters. */
 gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out);
 
 /* Upload (in-core) or pin (out-of-core) a host graph; derived per-graph
