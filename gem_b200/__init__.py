@@ -44,7 +44,7 @@ EXPORTS = (
     "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
     "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static", "gem_set_schedule", "gem_get_schedule",
-    "gem_relaxed_sets", "gem_relaxed_run", "gem_ctx_ooc_stats",
+    "gem_relaxed_sets", "gem_relaxed_run", "gem_ctx_ooc_stats", "gem_plan_query",
 )
 
 
@@ -139,6 +139,7 @@ def lib():
         L.gem_set_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
         L.gem_get_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
         L.gem_ctx_ooc_stats.argtypes = [vp, C.POINTER(_OocStats)]
+        L.gem_plan_query.argtypes = [C.POINTER(_Query), u32p, C.c_int, u32p, u32p]
         L.gem_filter_static.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(_Query), C.c_uint32, u32p, vp,
                                         C.c_uint64, vp]
         _lib = L
@@ -309,6 +310,20 @@ def relaxed_sets(q, threshold, cap=4096):
     qc = q._c()
     _check(lib().gem_relaxed_sets(C.byref(qc), threshold, cap, _p64(ets), C.byref(n)), what="relaxed_sets")
     return [int(x) for x in ets[:n.value]]
+
+
+def plan(q, cand_counts, closed_form=True):
+    """Matching order of q given |C(u)| per query vertex (gem_plan_query): (n_enum, order), order[k] the
+    query vertex of level k; with closed_form, levels n_enum.. are counted in closed form."""
+    cnt = np.ascontiguousarray(cand_counts, dtype=np.uint32)
+    if len(cnt) < q.nv:
+        raise ValueError("one candidate count per query vertex")
+    order = np.zeros(max(q.nv, 1), np.uint32)
+    ne = C.c_uint32()
+    qc = q._c()
+    _check(lib().gem_plan_query(C.byref(qc), _p32(cnt), 1 if closed_form else 0, C.byref(ne), _p32(order)),
+           what="plan")
+    return ne.value, order[:q.nv].tolist()
 
 
 def relaxed_query(q, et):

@@ -592,6 +592,21 @@ static bool validate_plan(const HostQuery &q, const Plan &p, std::string &why) {
   return true;
 }
 
+extern "C" gem_status gem_plan_query(const gem_query *q, const uint32_t *cand_counts, int closed_form,
+                                     uint32_t *n_enum, uint32_t *order_out) {
+  if (!q || !cand_counts || !n_enum || !order_out) return GEM_ERR_ARG;
+  HostQuery hq;
+  std::string err;
+  const gem_status st = make_host_query(q, hq, err);
+  if (st != GEM_OK) return st;
+  Plan p;
+  make_plan(hq, cand_counts, closed_form != 0, p);
+  if (!validate_plan(hq, p, err)) return GEM_ERR_INTERNAL;
+  *n_enum = p.n_enum;
+  for (uint32_t k = 0; k < p.n; ++k) order_out[k] = p.order[k];
+  return GEM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Wave pipeline
 // ---------------------------------------------------------------------------

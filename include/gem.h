@@ -241,6 +241,16 @@ gem_status gem_relaxed_sets(const gem_query *q, uint32_t threshold, uint32_t cap
 gem_status gem_relaxed_run(gem_ctx *ctx, const gem_query *q, uint32_t threshold, int mode, uint32_t cap,
                            uint64_t *ets, gem_result *res, uint32_t *n_out);
 
+/* Matching order of q (host only).  Replaces the order that the reference's
+ * lattice gives single-edge extensions (in-core/lib/structure/src/lattice.cpp
+ * :41-185, unifiedTrie.cu:939-1018).  cand_counts[u] is |C(u)| (gem_filter
+ * returns it).  With closed_form = 1 (count mode) an independent set of q's
+ * vertices whose removal leaves the rest connected moves to the end and is
+ * counted in closed form: levels *n_enum .. nv-1.  order_out[k] (nv entries)
+ * is the query vertex matched at level k. */
+gem_status gem_plan_query(const gem_query *q, const uint32_t *cand_counts, int closed_form, uint32_t *n_enum,
+                          uint32_t *order_out);
+
 /* Autotuner (no counterpart in the reference): for each query-size bucket
  * (<=4, <=8, <=12, <=16, <=24, <=32 vertices) present in qs, runs the first
  * 256 of its queries as one wave under each candidate join schedule (blocks

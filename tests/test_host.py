@@ -177,3 +177,105 @@ def test_relaxed_sets_cap():
     n = len(gem.relaxed_sets(q, 3))
     with pytest.raises(gem.GemError):
         gem.relaxed_sets(q, 3, cap=n - 1)
+
+
+# ---------------------------------------------------------------------------
+# Planner (gem_plan_query), against a restatement of its rules: the closed-form
+# suffix is an independent set chosen greedily (lowest degree, then most
+# candidates, then lowest id) whose removal leaves the rest connected, with at
+# most 4 suffix vertices per label, at most 16 labels and at most 32 backward
+# lists per label group; the root has the fewest candidates per incident edge;
+# each later level has the most matched neighbours, non-leaves first, then
+# fewest candidates, highest degree, lowest id; suffix levels follow, by label.
+# ---------------------------------------------------------------------------
+def _plan_model(q, cnt, closed_form):
+    n = q.nv
+    adj = [0] * n
+    for a, b in q.edges.tolist():
+        adj[a] |= 1 << b
+        adj[b] |= 1 << a
+    deg = [bin(x).count("1") for x in adj]
+    lab = [int(x) for x in q.labels]
+
+    def connected_without(rem):
+        alive = ((1 << n) - 1) & ~rem
+        if not alive:
+            return False
+        seen = alive & -alive
+        frontier = seen
+        while frontier:
+            nxt = 0
+            for u in range(n):
+                if frontier >> u & 1:
+                    nxt |= adj[u]
+            nxt &= alive & ~seen
+            seen |= nxt
+            frontier = nxt
+        return seen == alive
+
+    S = 0
+    if closed_form and n >= 2:
+        for u in sorted(range(n), key=lambda u: (deg[u], -int(cnt[u]), u)):
+            if adj[u] & S:
+                continue
+            S2 = S | 1 << u
+            if not connected_without(S2):
+                continue
+            members = [w for w in range(n) if S2 >> w & 1]
+            same = [w for w in members if lab[w] == lab[u]]
+            nback = deg[u] + sum(deg[w] for w in same if w != u)
+            if len(same) > 4 or nback > 32 or len({lab[w] for w in members}) > 16:
+                continue
+            S = S2
+    nenum = n - bin(S).count("1")
+    used, order = 0, []
+    for k in range(nenum):
+        best = None
+        for u in range(n):
+            if (used | S) >> u & 1:
+                continue
+            back = bin(adj[u] & used).count("1")
+            if k > 0 and back == 0:
+                continue
+            d = deg[u]
+            key = (int(int(cnt[u]) / (d + 1) * 1024.0), -d, u) if k == 0 else (-back, 1 if d <= 1 else 0, int(cnt[u]), -d, u)
+            if best is None or key < best[0]:
+                best = (key, u)
+        order.append(best[1])
+        used |= 1 << best[1]
+    suffix = sorted((u for u in range(n) if S >> u & 1), key=lambda u: (lab[u], u))
+    return nenum, order + suffix, adj
+
+
+@pytest.mark.parametrize("closed_form", [True, False])
+def test_planner_matches_its_rules(closed_form):
+    g = gem.HostGraph.rmat(12, 8, seed=11).set_labels(3, seed=12)
+    rng = np.random.default_rng(5)
+    n_checked = 0
+    for k, dens in ((3, gem.ANY), (4, gem.ANY), (5, gem.SPARSE), (6, gem.DENSE), (8, gem.ANY), (12, gem.SPARSE),
+                    (16, gem.DENSE), (32, gem.SPARSE)):
+        for q in gem.gen_queries(g, k, dens, 6, seed=700 + k):
+            cnt = rng.integers(1, 5000, size=q.nv)
+            ne, order = gem.plan(q, cnt, closed_form)
+            exp_ne, exp_order, adj = _plan_model(q, cnt, closed_form)
+            assert (ne, order) == (exp_ne, exp_order), (q.labels.tolist(), q.edges.tolist(), cnt.tolist())
+            # structure: a permutation; the prefix grows connected; the suffix is independent
+            assert sorted(order) == list(range(q.nv))
+            seen = 1 << order[0]
+            for u in order[1:ne]:
+                assert adj[u] & seen
+                seen |= 1 << u
+            suf = order[ne:]
+            assert all(not (adj[u] >> v & 1) for u in suf for v in suf)
+            if not closed_form:
+                assert ne == q.nv
+            n_checked += 1
+    assert n_checked >= 40
+
+
+def test_planner_rejects_bad_input():
+    q = gem.Query([0, 1, 2], [(0, 1)])  # disconnected
+    with pytest.raises(gem.GemError):
+        gem.plan(q, [5, 5, 5])
+    with pytest.raises(ValueError):
+        gem.plan(gem.Query([0, 1], [(0, 1)]), [5])
