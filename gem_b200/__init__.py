@@ -44,7 +44,7 @@ EXPORTS = (
     "gem_ctx_create", "gem_ctx_destroy", "gem_last_error", "gem_ctx_load_graph", "gem_query_run",
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
     "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static", "gem_set_schedule", "gem_get_schedule",
-    "gem_relaxed_sets", "gem_relaxed_run", "gem_ctx_ooc_stats", "gem_plan_query",
+    "gem_relaxed_sets", "gem_relaxed_run", "gem_ctx_ooc_stats", "gem_plan_query", "gem_hgraph_partitions",
 )
 
 
@@ -140,6 +140,7 @@ def lib():
         L.gem_get_schedule.argtypes = [vp, C.c_uint32, C.POINTER(_Schedule)]
         L.gem_ctx_ooc_stats.argtypes = [vp, C.POINTER(_OocStats)]
         L.gem_plan_query.argtypes = [C.POINTER(_Query), u32p, C.c_int, u32p, u32p]
+        L.gem_hgraph_partitions.argtypes = [vp, C.c_uint32, u32p, C.c_uint32, u32p]
         L.gem_filter_static.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(_Query), C.c_uint32, u32p, vp,
                                         C.c_uint64, vp]
         _lib = L
@@ -266,6 +267,16 @@ class HostGraph:
             seed = 0x47454D4C
         _check(lib().gem_hgraph_set_labels(self._h, nlabels, zipf_s, seed), what="set_labels")
         return self
+
+    def partitions(self, part_kib=0):
+        """Vertex bounds of the out-of-core adjacency partitions (gem_hgraph_partitions; part_kib 0 = 16 MiB)."""
+        n = C.c_uint32()
+        st = lib().gem_hgraph_partitions(self._h, part_kib, None, 0, C.byref(n))
+        if st not in (0, 3):
+            _check(st, what="partitions")
+        out = np.zeros(n.value + 1, np.uint32)
+        _check(lib().gem_hgraph_partitions(self._h, part_kib, _p32(out), n.value + 1, C.byref(n)), what="partitions")
+        return out
 
     def info(self):
         nv, na, ml, md = C.c_uint32(), C.c_uint64(), C.c_uint32(), C.c_uint32()

@@ -222,12 +222,15 @@ extern "C" const char *gem_last_error(const gem_ctx *ctx) { return ctx ? ctx->er
 // ooc_part_kib KiB (a vertex whose list alone is longer gets a range of its
 // own) and allocates the partition bounds and two staging buffers of the
 // largest partition's size, plus the side stream and events of the copies.
-static gem_status ooc_partitions(gem_ctx *ctx, const gem_hgraph *hg) {
+// Partition bounds of a CSR: vertex ranges of at most cap_bytes of arcs (a
+// vertex whose list alone is longer gets a range of its own), each as long
+// as the bound allows.  pv gets the vertex bounds, pa their arc offsets.
+static uint64_t partition_bounds(const gem_hgraph *hg, uint64_t cap_bytes, std::vector<uint32_t> &pv,
+                                 std::vector<uint64_t> &pa) {
   const uint32_t nv = hg->nv;
-  const uint64_t cap_bytes = (uint64_t)(ctx->opts.ooc_part_kib ? ctx->opts.ooc_part_kib : 16384u) << 10;
   const uint64_t cap = cap_bytes / 4 ? cap_bytes / 4 : 1;  // arcs per partition
-  ctx->part_v.assign(1, 0);
-  ctx->part_a.assign(1, 0);
+  pv.assign(1, 0);
+  pa.assign(1, 0);
   uint64_t max_arcs = 0;
   for (uint32_t v = 0; v < nv;) {
     const uint64_t a0 = hg->off[v];
@@ -241,11 +244,29 @@ static gem_status ooc_partitions(gem_ctx *ctx, const gem_hgraph *hg) {
       }
       u = lo;
     }
-    ctx->part_v.push_back(u);
-    ctx->part_a.push_back(hg->off[u]);
+    pv.push_back(u);
+    pa.push_back(hg->off[u]);
     max_arcs = std::max<uint64_t>(max_arcs, hg->off[u] - a0);
     v = u;
   }
+  return max_arcs;
+}
+
+extern "C" gem_status gem_hgraph_partitions(const gem_hgraph *g, uint32_t part_kib, uint32_t *part_v, uint32_t cap,
+                                            uint32_t *n_out) {
+  if (!g || !n_out || (cap && !part_v)) return GEM_ERR_ARG;
+  std::vector<uint32_t> pv;
+  std::vector<uint64_t> pa;
+  partition_bounds(g, (uint64_t)(part_kib ? part_kib : 16384u) << 10, pv, pa);
+  *n_out = (uint32_t)pv.size() - 1;
+  if (pv.size() > cap) return GEM_ERR_LIMIT;
+  std::memcpy(part_v, pv.data(), 4 * pv.size());
+  return GEM_OK;
+}
+
+static gem_status ooc_partitions(gem_ctx *ctx, const gem_hgraph *hg) {
+  const uint64_t cap_bytes = (uint64_t)(ctx->opts.ooc_part_kib ? ctx->opts.ooc_part_kib : 16384u) << 10;
+  const uint64_t max_arcs = partition_bounds(hg, cap_bytes, ctx->part_v, ctx->part_a);
   const uint32_t P = (uint32_t)ctx->part_v.size() - 1;
   auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
   const uint64_t b_pv = al(4ull * (P + 1)), b_st = al(4ull * (max_arcs ? max_arcs : 1));

@@ -172,6 +172,11 @@ typedef struct gem_ooc_stats {
 } gem_ooc_stats;
 /* GEM_ERR_STATE while the context serves (gem_submit): its waves update the counters. */
 gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out);
+/* The out-of-core partitions of g for a partition size of part_kib KiB (0 =
+ * 16384): part_v[0..n] (n + 1 entries) are the vertex bounds, *n_out = n.
+ * GEM_ERR_LIMIT when cap < n + 1 (*n_out is still set).  Host only. */
+gem_status gem_hgraph_partitions(const gem_hgraph *g, uint32_t part_kib, uint32_t *part_v, uint32_t cap,
+                                 uint32_t *n_out);
 
 /* Upload (in-core) or pin (out-of-core) a host graph; derived per-graph
  * indexes (degrees, neighbour-label counts) are built on the device.

@@ -279,3 +279,27 @@ def test_planner_rejects_bad_input():
         gem.plan(q, [5, 5, 5])
     with pytest.raises(ValueError):
         gem.plan(gem.Query([0, 1], [(0, 1)]), [5])
+
+
+@pytest.mark.parametrize("part_kib", [1, 4, 64])
+def test_out_of_core_partitions(part_kib):
+    """Partition bounds (gem_hgraph_partitions): consecutive vertex ranges that
+    cover every vertex, each of at most part_kib KiB of arcs unless it holds a
+    single vertex whose list is longer, and each as long as the bound allows."""
+    g = gem.HostGraph.rmat(12, 8, seed=21).set_labels(3, seed=22)
+    off, _, _ = g.arrays()
+    cap = (part_kib << 10) // 4
+    pv = g.partitions(part_kib)
+    assert pv[0] == 0 and pv[-1] == g.nv and np.all(np.diff(pv.astype(np.int64)) > 0)
+    big = 0
+    for a, b in zip(pv[:-1].tolist(), pv[1:].tolist()):
+        arcs = int(off[b] - off[a])
+        if b - a == 1 and arcs > cap:
+            big += 1  # a hub list longer than a partition: alone
+        else:
+            assert arcs <= cap
+        if b < g.nv:
+            assert int(off[b + 1] - off[a]) > cap  # one more vertex would not fit
+    if part_kib == 1:
+        assert big > 0  # this graph has lists longer than 256 arcs
+    assert len(g.partitions(0)) == 2  # the default 16 MiB holds the whole graph
