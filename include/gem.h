@@ -173,8 +173,10 @@ typedef struct gem_ooc_stats {
 /* GEM_ERR_STATE while the context serves (gem_submit): its waves update the counters. */
 gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out);
 /* The out-of-core partitions of g for a partition size of part_kib KiB (0 =
- * 16384): part_v[0..n] (n + 1 entries) are the vertex bounds, *n_out = n.
- * GEM_ERR_LIMIT when cap < n + 1 (*n_out is still set).  Host only. */
+ * 16384), as gem_ctx_load_graph cuts them (no counterpart in the reference,
+ * which does not partition the data graph): part_v[0..n] (n + 1 entries) are
+ * the vertex bounds, *n_out = n.  GEM_ERR_LIMIT when cap < n + 1 (*n_out is
+ * still set).  Host only. */
 gem_status gem_hgraph_partitions(const gem_hgraph *g, uint32_t part_kib, uint32_t *part_v, uint32_t cap,
                                  uint32_t *n_out);
 
