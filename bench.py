@@ -337,6 +337,7 @@ def run_gem(args):
     }
     if args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(g, pool, args)
+        line["host_path"] = host_path_baseline(g, pool[:B], (phase["filter"] + phase["tables"]) / args.steps)
     print(json.dumps(line), flush=True)
 
 
@@ -468,6 +469,32 @@ def out_of_core_section(gem, args, local, g):
             out["modes"][name] = m
     out["counts_equal"] = all(v == counts["in_core"] for v in counts.values()) and None not in counts["in_core"]
     return out
+
+
+def host_path_baseline(g, qs, gpu_ms_per_step):
+    """The reference's host-side path for one batch: its out-of-core filter and
+    edge-table build (OpenMP, out-of-core/lib/filter/src/filter.cu:61-295 and
+    out-of-core/lib/structure/src/unifiedTrie.cu:1224-1427, restated in the
+    oracle with the reference's worker counts) on the host cores, beside the
+    GPU's filter + tables phases per step.  The reference builds both
+    directions of every query edge whose source has query degree > 1."""
+    import oracle
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ntab = 0
+    for q in qs:
+        cand = oracle.filter_mt(g, q)
+        deg = np.bincount(q.edges.reshape(-1), minlength=q.nv) if q.ne else np.zeros(q.nv, int)
+        for a, b in q.edges.tolist():
+            for s, t in ((a, b), (b, a)):
+                if deg[s] > 1:
+                    oracle.edge_table_mt(g, cand[s], cand[t])
+                    ntab += 1
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"filter_tables_ms_per_batch": round(ms, 2), "gpu_filter_tables_ms_per_step": round(gpu_ms_per_step, 3),
+            "gpu_speedup": round(ms / gpu_ms_per_step, 1) if gpu_ms_per_step > 0 else None,
+            "threads": {"filter": min(16, cores), "tables": min(4, cores)}, "queries": len(qs), "tables": ntab,
+            "kind": "port"}
 
 
 def cpu_baseline(g, pool, args):

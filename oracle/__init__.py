@@ -29,6 +29,11 @@ def lib():
         L.oracle_edge_table.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u64p, u32p,
                                         C.c_uint64]
         L.oracle_edge_table.restype = C.c_int64
+        L.oracle_filter_mt.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p,
+                                       C.c_uint32, u32p, u32p, C.c_uint64, C.c_int]
+        L.oracle_edge_table_mt.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u64p, u32p,
+                                           C.c_uint64, C.c_int]
+        L.oracle_edge_table_mt.restype = C.c_int64
         L.oracle_count.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p, C.c_int,
                                    C.c_int, C.c_uint64, u64p, u64p, u64p]
         L.oracle_brute.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p, u64p, u64p]
@@ -105,6 +110,39 @@ def filter(g, q, threshold=0):
         out.append(cand[at:at + int(counts[u])].copy())
         at += int(counts[u])
     return out
+
+
+def filter_mt(g, q, threshold=0, threads=0):
+    """filter() on threads (0: the reference's out-of-core worker count, min(16, all))."""
+    off, nbr, lab = _graph(g)
+    ql, qe, qn, qm = _query(q)
+    counts = np.zeros(qn, np.uint32)
+    cap = qn * len(lab)
+    cand = np.zeros(max(cap, 1), np.uint32)
+    r = lib().oracle_filter_mt(len(lab), _p64(off), _p32(nbr), _p32(lab), qn, _p32(ql), qm, _p32(qe), threshold,
+                               _p32(counts), _p32(cand), cap, threads)
+    assert r == 0
+    out, at = [], 0
+    for u in range(qn):
+        out.append(cand[at:at + int(counts[u])].copy())
+        at += int(counts[u])
+    return out
+
+
+def edge_table_mt(g, cu, cw, threads=0):
+    """edge_table() on threads (0: the reference's out-of-core worker count, min(4, all))."""
+    off, nbr, lab = _graph(g)
+    cu = np.ascontiguousarray(cu, dtype=np.uint32)
+    cw = np.ascontiguousarray(cw, dtype=np.uint32)
+    offsets = np.zeros(len(cu) + 1, np.uint64)
+    cap = int((off[cu.astype(np.int64) + 1] - off[cu.astype(np.int64)]).sum()) + 1 if len(cu) else 1
+    vals = np.zeros(cap, np.uint32)
+    r = lib().oracle_edge_table_mt(len(lab), _p64(off), _p32(nbr),
+                                   _p32(cu if cu.size else np.zeros(1, np.uint32)), len(cu),
+                                   _p32(cw if cw.size else np.zeros(1, np.uint32)), len(cw), _p64(offsets),
+                                   _p32(vals), cap, threads)
+    assert r >= 0
+    return offsets, vals[:r].copy()
 
 
 def edge_table(g, cu, cw):

@@ -151,6 +151,123 @@ int64_t oracle_edge_table(uint32_t nv, const uint64_t *off, const uint32_t *nbr,
   return overflow ? -1 : (int64_t)p;
 }
 
+/*
+ * The same filter on threads (nt <= 0: min(16, omp_get_max_threads()), the
+ * worker count of the reference's out-of-core filterSSM, out-of-core/lib/
+ * filter/src/filter.cu:47-58): data vertices in parallel, each vertex's
+ * neighbour-label counts computed once and tested against every query vertex,
+ * then the lists compacted in vertex order.  Same output as oracle_filter.
+ */
+int oracle_filter_mt(uint32_t nv, const uint64_t *off, const uint32_t *nbr, const uint32_t *lab,
+                     uint32_t qn, const uint32_t *qlab, uint32_t qm, const uint32_t *qedges,
+                     uint32_t T, uint32_t *counts, uint32_t *cand, uint64_t cand_cap, int nt) {
+  if (nt <= 0) {
+    nt = omp_get_max_threads();
+    if (nt > 16) nt = 16;
+  }
+  uint32_t qadj[OR_MAX_QV];
+  build_qadj(qn, qm, qedges, qadj);
+  uint32_t ql[OR_MAX_QV], nql = 0;
+  for (uint32_t u = 0; u < qn; ++u) {
+    uint32_t k = 0;
+    while (k < nql && ql[k] != qlab[u]) ++k;
+    if (k == nql) ql[nql++] = qlab[u];
+  }
+  uint32_t qnlc[OR_MAX_QV][OR_MAX_QV], qdeg[OR_MAX_QV];
+  memset(qnlc, 0, sizeof qnlc);
+  for (uint32_t u = 0; u < qn; ++u) {
+    qdeg[u] = (uint32_t)__builtin_popcount(qadj[u]);
+    for (uint32_t w = 0; w < qn; ++w)
+      if (qadj[u] & (1u << w)) {
+        uint32_t k = 0;
+        while (ql[k] != qlab[w]) ++k;
+        qnlc[u][k]++;
+      }
+  }
+  uint32_t *mask = (uint32_t *)malloc((nv ? nv : 1) * sizeof(uint32_t));
+  if (!mask) return -2;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+  for (int64_t vi = 0; vi < (int64_t)nv; ++vi) {
+    const uint32_t v = (uint32_t)vi;
+    uint32_t m = 0;
+    for (uint32_t u = 0; u < qn; ++u)
+      if (lab[v] == qlab[u] && qdeg[u] <= (uint32_t)(off[v + 1] - off[v]) + T) m |= 1u << u;
+    if (m) {
+      uint32_t dnlc[OR_MAX_QV];
+      memset(dnlc, 0, sizeof dnlc);
+      for (uint64_t i = off[v]; i < off[v + 1]; ++i) {
+        const uint32_t l = lab[nbr[i]];
+        for (uint32_t k = 0; k < nql; ++k)
+          if (ql[k] == l) { dnlc[k]++; break; }
+      }
+      for (uint32_t mm = m; mm; mm &= mm - 1) {
+        const uint32_t u = (uint32_t)__builtin_ctz(mm);
+        uint32_t diff = 0;
+        for (uint32_t k = 0; k < nql; ++k)
+          if (qnlc[u][k] > dnlc[k]) diff += qnlc[u][k] - dnlc[k];
+        if (diff > T) m &= ~(1u << u);
+      }
+    }
+    mask[v] = m;
+  }
+  uint64_t pos = 0;
+  int overflow = 0;
+  for (uint32_t u = 0; u < qn; ++u) {
+    uint32_t c = 0;
+    for (uint32_t v = 0; v < nv; ++v)
+      if ((mask[v] >> u) & 1u) {
+        if (pos < cand_cap) cand[pos] = v; else overflow = 1;
+        ++pos;
+        ++c;
+      }
+    counts[u] = c;
+  }
+  free(mask);
+  return overflow ? -1 : 0;
+}
+
+/*
+ * The same edge-candidate table on threads (nt <= 0: min(4,
+ * omp_get_max_threads()), the worker count of the reference's out-of-core
+ * construct_edge_candidates_cpu, out-of-core/lib/structure/src/unifiedTrie.cu
+ * :26-37): a parallel count pass over the keys, a prefix sum, a parallel write
+ * pass.  Same output as oracle_edge_table.
+ */
+int64_t oracle_edge_table_mt(uint32_t nv, const uint64_t *off, const uint32_t *nbr,
+                             const uint32_t *cu, uint32_t nu, const uint32_t *cw, uint32_t nw,
+                             uint64_t *offsets, uint32_t *values, uint64_t values_cap, int nt) {
+  if (nt <= 0) {
+    nt = omp_get_max_threads();
+    if (nt > 4) nt = 4;
+  }
+  uint8_t *inw = (uint8_t *)calloc(nv ? nv : 1, 1);
+  if (!inw) return -2;
+  for (uint32_t i = 0; i < nw; ++i) inw[cw[i]] = 1;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256)
+  for (int64_t ii = 0; ii < (int64_t)nu; ++ii) {
+    const uint32_t v = cu[ii];
+    uint64_t c = 0;
+    for (uint64_t j = off[v]; j < off[v + 1]; ++j) c += inw[nbr[j]];
+    offsets[ii + 1] = c;
+  }
+  offsets[0] = 0;
+  for (uint32_t i = 0; i < nu; ++i) offsets[i + 1] += offsets[i];
+  const uint64_t total = offsets[nu];
+  if (total > values_cap) {
+    free(inw);
+    return -1;
+  }
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256)
+  for (int64_t ii = 0; ii < (int64_t)nu; ++ii) {
+    const uint32_t v = cu[ii];
+    uint64_t p = offsets[ii];
+    for (uint64_t j = off[v]; j < off[v + 1]; ++j)
+      if (inw[nbr[j]]) values[p++] = nbr[j];
+  }
+  free(inw);
+  return (int64_t)total;
+}
+
 /* ---------------------------------------------------------------------- */
 /* Backtracking counter                                                    */
 /* ---------------------------------------------------------------------- */

@@ -145,3 +145,23 @@ def test_relaxed_sets_and_oracle_match_reference_binary():
                 assert cnt % (1 << 32) == printed, (q.edges.tolist(), bin(et), cnt, printed)
                 checked += 1
     assert checked >= 20
+
+
+@pytest.mark.parametrize("threads", [1, 3, 0])
+def test_threaded_filter_and_tables_equal_the_checkers(threads):
+    """The OpenMP restatements of the reference's out-of-core host filter and
+    table build (timed as the bench's host-path baseline) give exactly the
+    single-threaded checkers' candidate lists and tables."""
+    g = gem.HostGraph.rmat(12, 8, seed=31).set_labels(4, seed=32)
+    for k, dens in ((3, gem.ANY), (5, gem.SPARSE), (8, gem.DENSE)):
+        for q in gem.gen_queries(g, k, dens, 3, seed=900 + k):
+            for T in (0, 1):
+                a = oracle.filter(g, q, threshold=T)
+                b = oracle.filter_mt(g, q, threshold=T, threads=threads)
+                assert all(np.array_equal(x, y) for x, y in zip(a, b))
+            cand = oracle.filter(g, q)
+            for u, w in q.edges.tolist():
+                for s, t in ((u, w), (w, u)):
+                    o1, v1 = oracle.edge_table(g, cand[s], cand[t])
+                    o2, v2 = oracle.edge_table_mt(g, cand[s], cand[t], threads=threads)
+                    assert np.array_equal(o1, o2) and np.array_equal(v1, v2)
