@@ -353,10 +353,13 @@ gem_status gem_index_probe(gem_ctx *ctx, const gem_query *q, uint32_t u,
  * vertices return GEM_ERR_LIMIT; more candidates than cand_cap return
  * GEM_ERR_OVERFLOW with exact counts.  All calls on a device share that
  * array, so calls whose work overlaps on the GPU race: order them on one
- * stream.  The first call on a device looks up the array's address (with
- * that device current) and should come before any stream capture.  stream
- * is a cudaStream_t (NULL = legacy default stream); the call returns after
- * the stream has finished its work. */
+ * stream.  Every call looks up the array's address in the caller's current
+ * context.  stream is a cudaStream_t (NULL = legacy default stream); the
+ * call blocks until the stream has finished its work (it reads each
+ * candidate count back), so it cannot be made during stream capture.  All
+ * four device pointers must be non-null; a neighbour id >= nv or offsets
+ * that decrease or run past offsets[nv] are skipped on the device and
+ * return GEM_ERR_ARG. */
 #define GEM_STATIC_SCRATCH_BYTES (4u << 20)
 #define GEM_STATIC_MAX_VERTICES 8000000u
 gem_status gem_filter_static(const uint64_t *d_offsets, const uint32_t *d_nbrs,

@@ -62,3 +62,40 @@ def test_filter_static_rejects_oversized_graph():
     st = gem.lib().gem_filter_static(one, one, one, 8_000_001, C.byref(qc), 0,
                                      counts.ctypes.data_as(C.POINTER(C.c_uint32)), one, 0, None)
     assert gem.STATUS[st] == "ERR_LIMIT"
+
+
+def test_filter_static_reports_malformed_graph():
+    """A neighbour id beyond the vertex count is skipped on the device (never
+    used as an index) and the call returns GEM_ERR_ARG; the next call on a
+    well-formed graph is exact again."""
+    import torch
+    g = gem.HostGraph.rmat(10, 8, seed=0x5A21).set_labels(3, 0.0, seed=0x5A22)
+    off, nbr, lab = g.arrays()
+    v = int(np.argmax(np.diff(off.astype(np.int64))))  # a vertex with neighbours
+    q = gem.Query([int(lab[v]), int(lab[nbr[off[v]]])], [(0, 1)])
+    bad_nbr = nbr.astype(np.uint32).copy()
+    bad_nbr[off[v]] = g.nv + 1000
+    d_off = _dev(off.astype(np.uint64), torch, np.int64)
+    d_lab = _dev(lab.astype(np.uint32), torch, np.int32)
+    L = gem.lib()
+    qc = q._c()
+    for arr, want in ((bad_nbr, "ERR_ARG"), (nbr.astype(np.uint32), "OK")):
+        d_nbr = _dev(arr, torch, np.int32)
+        d_cand = torch.full((2 * g.nv,), -1, dtype=torch.int32, device="cuda")
+        counts = np.zeros(q.nv, np.uint32)
+        torch.cuda.synchronize()
+        st = L.gem_filter_static(C.c_void_p(d_off.data_ptr()), C.c_void_p(d_nbr.data_ptr()),
+                                 C.c_void_p(d_lab.data_ptr()), g.nv, C.byref(qc), 0,
+                                 counts.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_void_p(d_cand.data_ptr()),
+                                 2 * g.nv, None)
+        assert gem.STATUS[st] == want
+
+
+def test_filter_static_rejects_null_adjacency():
+    q = gem.Query([0, 1], [(0, 1)])
+    qc = q._c()
+    counts = np.zeros(2, np.uint32)
+    one = C.c_void_p(1)  # never dereferenced: the argument check comes first
+    st = gem.lib().gem_filter_static(one, None, one, 16, C.byref(qc), 0,
+                                     counts.ctypes.data_as(C.POINTER(C.c_uint32)), one, 0, None)
+    assert gem.STATUS[st] == "ERR_ARG"
