@@ -81,7 +81,7 @@ def build(verbose=False, ptxas_info=False):
         _run(["g++"] + CXXFLAGS + [cli_src, "-o", CLI, "-L" + PKG, "-lgem",
                                    "-Wl,-rpath,$ORIGIN/..", "-L/usr/local/cuda/lib64", "-lcudart"], verbose)
     if _stale(ORACLE_LIB, [ORACLE_SRC]):
-        _run(["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-shared", "-fPIC", ORACLE_SRC, "-o", ORACLE_LIB], verbose)
+        _run(["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-shared", "-fPIC", ORACLE_SRC, "-o", ORACLE_LIB, "-lm"], verbose)
     return "\n".join(logs)
 
 

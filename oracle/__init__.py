@@ -37,6 +37,13 @@ def lib():
         L.oracle_count.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p, C.c_int,
                                    C.c_int, C.c_uint64, u64p, u64p, u64p]
         L.oracle_brute.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, u32p, u64p, u64p]
+        L.oracle_rmat.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64, u64p,
+                                  C.POINTER(u32p), u64p]
+        L.oracle_free.argtypes = [C.c_void_p]
+        L.oracle_free.restype = None
+        L.oracle_set_labels.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, u32p]
+        L.oracle_gen_queries.argtypes = [C.c_uint32, u64p, u32p, u32p, C.c_uint32, C.c_int, C.c_uint32, C.c_uint64,
+                                         C.c_uint32, u32p, u32p, u32p]
         _lib = L
     return _lib
 
@@ -157,3 +164,73 @@ def edge_table(g, cu, cw):
                                 _p32(vals), cap)
     assert r >= 0
     return offsets, vals[:r].copy()
+
+
+class Graph:
+    """A data graph as plain numpy CSR arrays (offsets u64[nv+1], nbrs u32[arcs], labels u32[nv]),
+    accepted wherever the functions above take a graph."""
+
+    def __init__(self, off, nbr, lab):
+        self.off, self.nbr, self.lab = off, nbr, lab
+
+    @property
+    def nv(self):
+        return int(self.lab.shape[0])
+
+    def arrays(self):
+        return self.off, self.nbr, self.lab
+
+
+class Query:
+    """A query: labels u32[nv] and undirected edges u32[ne, 2]."""
+
+    def __init__(self, labels, edges):
+        self.labels = np.ascontiguousarray(labels, dtype=np.uint32)
+        self.edges = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 2)
+
+    @property
+    def nv(self):
+        return int(self.labels.shape[0])
+
+    @property
+    def ne(self):
+        return int(self.edges.shape[0])
+
+
+def rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=None):
+    """Seeded R-MAT graph (oracle_rmat) with all labels 0; equal to gem_hgraph_rmat's."""
+    seed = (0x47454D00 + scale) if seed is None else seed
+    nv = 1 << scale
+    off = np.zeros(nv + 1, np.uint64)
+    pn = C.POINTER(C.c_uint32)()
+    na = C.c_uint64()
+    if lib().oracle_rmat(scale, edge_factor, a, b, c, seed, _p64(off), C.byref(pn), C.byref(na)) != 0:
+        raise MemoryError("oracle_rmat failed")
+    try:
+        nbr = np.ctypeslib.as_array(pn, shape=(max(na.value, 1),))[:na.value].copy()
+    finally:
+        lib().oracle_free(pn)
+    return Graph(off, nbr, np.zeros(nv, np.uint32))
+
+
+def set_labels(g, nlabels, zipf_s=0.0, seed=0x47454D4C):
+    """Seeded labels (oracle_set_labels), in place; equal to gem_hgraph_set_labels's."""
+    lab = np.zeros(g.nv, np.uint32)
+    if lib().oracle_set_labels(g.nv, nlabels, zipf_s, seed, _p32(lab)) != 0:
+        raise ValueError("oracle_set_labels rejected its arguments")
+    g.lab = lab
+    return g
+
+
+def gen_queries(g, k, density=0, count=1, seed=0x51000, max_e=496):
+    """Seeded random-walk queries (oracle_gen_queries); equal to gem_gen_queries's."""
+    off, nbr, lab = _graph(g)
+    ne = np.zeros(count, np.uint32)
+    ql = np.zeros(max(count * k, 1), np.uint32)
+    qe = np.zeros(max(count * 2 * max_e, 1), np.uint32)
+    r = lib().oracle_gen_queries(len(lab), _p64(off), _p32(nbr), _p32(lab), k, density, count, seed, max_e,
+                                 _p32(ne), _p32(ql), _p32(qe))
+    if r != 0:
+        raise ValueError(f"oracle_gen_queries failed ({r})")
+    return [Query(ql[i * k:(i + 1) * k].copy(),
+                  qe[i * 2 * max_e: i * 2 * max_e + 2 * int(ne[i])].reshape(-1, 2).copy()) for i in range(count)]

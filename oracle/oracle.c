@@ -24,6 +24,7 @@
  * golden vectors or fixtures; the committed fixtures under tests/golden/
  * hold hand-derived answers and counts printed by the reference binary.
  */
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -457,4 +458,242 @@ int oracle_brute(uint32_t nv, const uint64_t *off, const uint32_t *nbr, const ui
   *count_out = c;
   *hash_out = h;
   return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Seeded workload generators, restated so that the benchmark's reference arm
+ * builds its inputs without loading libgem.  They produce the same graphs and
+ * queries as gem_hgraph_rmat, gem_hgraph_set_labels and gem_gen_queries (a
+ * CPU test checks equality): counter-based splitmix64 draws, R-MAT quadrant
+ * descent, Zipf labels by inverse CDF, random-walk queries with induced
+ * edges.  The CSR of a simple undirected graph with sorted adjacency is
+ * unique, so any correct construction gives the same arrays.
+ * ------------------------------------------------------------------------ */
+static uint64_t or_rng_at(uint64_t s, uint64_t i) { return or_mix64(or_mix64(s) ^ (i * 0xD1B54A32D192ED03ull)); }
+static double or_u01(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
+
+/* LSD radix sort of n keys of `bits` bits (11-bit digits). */
+static int or_radix_sort(uint64_t *k, uint64_t n, uint32_t bits) {
+  uint64_t *tmp = (uint64_t *)malloc((n ? n : 1) * sizeof(uint64_t));
+  uint64_t *cnt = (uint64_t *)malloc(2048 * sizeof(uint64_t));
+  if (!tmp || !cnt) { free(tmp); free(cnt); return -1; }
+  for (uint32_t sh = 0; sh < bits; sh += 11) {
+    memset(cnt, 0, 2048 * sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; ++i) cnt[(k[i] >> sh) & 2047]++;
+    uint64_t s = 0;
+    for (uint32_t d = 0; d < 2048; ++d) { uint64_t c = cnt[d]; cnt[d] = s; s += c; }
+    for (uint64_t i = 0; i < n; ++i) tmp[cnt[(k[i] >> sh) & 2047]++] = k[i];
+    memcpy(k, tmp, n * sizeof(uint64_t));
+  }
+  free(tmp);
+  free(cnt);
+  return 0;
+}
+
+/*
+ * R-MAT: 2^scale vertices, edge_factor * 2^scale sampled edges; edge i draws
+ * one splitmix64 stream from (seed, i) and descends `scale` levels, taking
+ * quadrant (0,0), (0,1), (1,0) or (1,1) with probabilities a, b, c, 1-a-b-c
+ * compared on the draw's top 53 bits.  Self loops and duplicates are dropped,
+ * the rest symmetrised.  off gets nv+1 entries; *nbr_out is malloc'd (the
+ * caller frees it with oracle_free).  Returns 0, or -1 on bad arguments or
+ * memory.
+ */
+int oracle_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed, uint64_t *off,
+                uint32_t **nbr_out, uint64_t *n_arcs) {
+  if (scale == 0 || scale > 31 || edge_factor == 0 || !off || !nbr_out || !n_arcs) return -1;
+  const uint32_t nv = 1u << scale;
+  const uint64_t m = (uint64_t)edge_factor << scale;
+  const uint64_t ta = (uint64_t)(a * 9007199254740992.0), tb = (uint64_t)((a + b) * 9007199254740992.0),
+                 tc = (uint64_t)((a + b + c) * 9007199254740992.0);
+  uint64_t *keys = (uint64_t *)malloc(m * sizeof(uint64_t));
+  if (!keys) return -1;
+  const uint64_t drop = ~0ull;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)m; ++i) {
+    uint64_t s = or_rng_at(seed, (uint64_t)i);
+    uint32_t src = 0, dst = 0;
+    for (uint32_t l = 0; l < scale; ++l) {
+      s = or_mix64(s);
+      const uint64_t r = s >> 11;
+      const uint32_t bs = r >= tb, bd = (r >= ta && r < tb) || r >= tc;
+      src = (src << 1) | bs;
+      dst = (dst << 1) | bd;
+    }
+    keys[i] = src == dst ? drop : ((uint64_t)(src < dst ? src : dst) << scale) | (src < dst ? dst : src);
+  }
+  /* drop markers: move them out before sorting the 2*scale-bit keys */
+  uint64_t n = 0;
+  for (uint64_t i = 0; i < m; ++i)
+    if (keys[i] != drop) keys[n++] = keys[i];
+  if (or_radix_sort(keys, n, 2 * scale) != 0) { free(keys); return -1; }
+  uint64_t u = 0;
+  for (uint64_t i = 0; i < n; ++i)
+    if (u == 0 || keys[u - 1] != keys[i]) keys[u++] = keys[i];
+  const uint64_t mask = ((uint64_t)1 << scale) - 1;
+  uint64_t *lower = (uint64_t *)calloc((size_t)nv + 1, sizeof(uint64_t));
+  uint64_t *pos = (uint64_t *)malloc(((size_t)nv + 1) * sizeof(uint64_t));
+  uint64_t *lpos = (uint64_t *)malloc(((size_t)nv + 1) * sizeof(uint64_t));
+  uint32_t *nbr = (uint32_t *)malloc((2 * u ? 2 * u : 1) * sizeof(uint32_t));
+  if (!lower || !pos || !lpos || !nbr) { free(keys); free(lower); free(pos); free(lpos); free(nbr); return -1; }
+  for (uint32_t v = 0; v <= nv; ++v) off[v] = 0;
+  for (uint64_t i = 0; i < u; ++i) {
+    off[(keys[i] >> scale) + 1]++;  /* upper neighbour of lo */
+    off[(keys[i] & mask) + 1]++;    /* lower neighbour of hi */
+    lower[keys[i] & mask]++;
+  }
+  for (uint32_t v = 0; v < nv; ++v) off[v + 1] += off[v];
+  /* each list: its lower neighbours (< v) then its upper ones (> v); keys in
+     (lo, hi) order fill both parts in ascending order */
+  for (uint32_t v = 0; v < nv; ++v) { lpos[v] = off[v]; pos[v] = off[v] + lower[v]; }
+  for (uint64_t i = 0; i < u; ++i) {
+    const uint32_t lo = (uint32_t)(keys[i] >> scale), hi = (uint32_t)(keys[i] & mask);
+    nbr[pos[lo]++] = hi;
+    nbr[lpos[hi]++] = lo;
+  }
+  free(keys);
+  free(lower);
+  free(pos);
+  free(lpos);
+  *nbr_out = nbr;
+  *n_arcs = 2 * u;
+  return 0;
+}
+
+void oracle_free(void *p) { free(p); }
+
+/* Labels 0..nlabels-1 (uniform when zipf_s == 0, else P(l) ~ 1/(l+1)^s): vertex
+ * v draws u = u01(stream seed, draw v) and takes the first l with cdf[l] > u. */
+int oracle_set_labels(uint32_t nv, uint32_t nlabels, double zipf_s, uint64_t seed, uint32_t *lab) {
+  if (nlabels == 0 || zipf_s < 0 || !lab) return -1;
+  double *cdf = (double *)malloc(nlabels * sizeof(double));
+  if (!cdf) return -1;
+  double tot = 0;
+  for (uint32_t l = 0; l < nlabels; ++l) {
+    tot += zipf_s == 0 ? 1.0 : pow((double)(l + 1), -zipf_s);
+    cdf[l] = tot;
+  }
+  for (uint32_t l = 0; l < nlabels; ++l) cdf[l] /= tot;
+  cdf[nlabels - 1] = 1.0;
+#pragma omp parallel for schedule(static)
+  for (int64_t v = 0; v < (int64_t)nv; ++v) {
+    const double x = or_u01(or_rng_at(seed, (uint64_t)v));
+    uint32_t lo = 0, hi = nlabels;  /* first l with cdf[l] > x */
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) / 2;
+      if (cdf[mid] > x) hi = mid; else lo = mid + 1;
+    }
+    lab[v] = lo < nlabels ? lo : nlabels - 1;
+  }
+  free(cdf);
+  return 0;
+}
+
+/*
+ * Random-walk queries (density 0 any, 1 sparse = average degree <= 3, 2 dense
+ * = above 3).  Query qi draws from stream mix64(seed) ^ mix64(qi + 0x51).  Up
+ * to 4096 walks: a start vertex with neighbours, then uniform neighbour steps
+ * (at most 64k + 256) until k distinct vertices, numbered in visit order; the
+ * query keeps all induced edges.  The first walk that reaches k vertices is
+ * kept unless a later one meets the density.  An unsatisfied sparse request
+ * keeps the first-visit tree edges plus induced (i, j) edges in order while
+ * the average degree stays <= 3, sorted.  Outputs as gem_gen_queries:
+ * ne_out[qi], labels_out[qi*k ..), edges_out[qi*2*max_e ..).  Returns 0, -1
+ * (arguments), -2 (no walk reached k vertices) or -3 (more than max_e edges).
+ */
+int oracle_gen_queries(uint32_t nv, const uint64_t *off, const uint32_t *nbr, const uint32_t *lab, uint32_t k,
+                       int density, uint32_t count, uint64_t seed, uint32_t max_e, uint32_t *ne_out,
+                       uint32_t *labels_out, uint32_t *edges_out) {
+  if (k == 0 || k > OR_MAX_QV || k > nv || density < 0 || density > 2 || off[nv] == 0) return -1;
+  int fail = 0;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t qi = 0; qi < (int64_t)count; ++qi) {
+    const uint64_t stream = or_mix64(seed) ^ or_mix64((uint64_t)qi + 0x51ull);
+    uint64_t draw = 0;
+    uint32_t vis[OR_MAX_QV], best[OR_MAX_QV], tree[OR_MAX_QV][2], btree[OR_MAX_QV][2];
+    uint32_t nbest = 0, ntree = 0, nbtree = 0;
+    int done = 0;
+    for (uint32_t attempt = 0; attempt < 4096 && !done; ++attempt) {
+      uint32_t s;
+      do { s = (uint32_t)(or_rng_at(stream, draw++) % nv); } while (off[s + 1] == off[s]);
+      uint32_t nvis = 1, cur = s, cur_local = 0;
+      vis[0] = s;
+      ntree = 0;
+      for (uint64_t steps = 0, cap = 64ull * k + 256; nvis < k && steps < cap; ++steps) {
+        const uint64_t d = off[cur + 1] - off[cur];
+        const uint32_t nx = nbr[off[cur] + or_rng_at(stream, draw++) % d];
+        uint32_t j = 0;
+        while (j < nvis && vis[j] != nx) ++j;
+        if (j == nvis) {
+          vis[nvis++] = nx;
+          tree[ntree][0] = cur_local;
+          tree[ntree][1] = j;
+          ++ntree;
+        }
+        cur = nx;
+        cur_local = j;
+      }
+      if (nvis < k) continue;
+      uint32_t m = 0;
+      for (uint32_t i = 0; i < k; ++i)
+        for (uint32_t j = i + 1; j < k; ++j) m += (uint32_t)has_arc(off, nbr, vis[i], vis[j]);
+      const int dense = 2.0 * m / k > 3.0;
+      const int ok = density == 0 || (density == 1 && !dense) || (density == 2 && dense);
+      if (nbest == 0 || ok) {
+        memcpy(best, vis, k * sizeof(uint32_t));
+        memcpy(btree, tree, ntree * sizeof(tree[0]));
+        nbest = k;
+        nbtree = ntree;
+      }
+      if (ok) done = 1;
+    }
+    if (nbest == 0) {
+#pragma omp atomic write
+      fail = -2;
+      continue;
+    }
+    uint32_t ne = 0;
+    uint32_t *eo = edges_out + (size_t)qi * 2 * max_e;
+    if (done || density != 1) {
+      for (uint32_t i = 0; i < k; ++i)
+        for (uint32_t j = i + 1; j < k; ++j)
+          if (has_arc(off, nbr, best[i], best[j])) {
+            if (ne < max_e) { eo[2 * ne] = i; eo[2 * ne + 1] = j; }
+            ++ne;
+          }
+    } else {
+      uint32_t has[OR_MAX_QV] = {0};  /* has[i] bit j: tree edge (i, j), i < j */
+      uint32_t e[OR_MAX_QV * OR_MAX_QV][2];
+      for (uint32_t t = 0; t < nbtree; ++t) {
+        const uint32_t i = btree[t][0] < btree[t][1] ? btree[t][0] : btree[t][1];
+        const uint32_t j = btree[t][0] < btree[t][1] ? btree[t][1] : btree[t][0];
+        has[i] |= 1u << j;
+        e[ne][0] = i;
+        e[ne][1] = j;
+        ++ne;
+      }
+      for (uint32_t i = 0; i < k; ++i)
+        for (uint32_t j = i + 1; j < k; ++j) {
+          if (has[i] >> j & 1u) continue;
+          if (2.0 * (ne + 1) / k > 3.0) { i = k; break; }
+          if (has_arc(off, nbr, best[i], best[j])) { e[ne][0] = i; e[ne][1] = j; ++ne; }
+        }
+      /* sort (i, j) pairs */
+      for (uint32_t x = 1; x < ne; ++x)
+        for (uint32_t y = x; y > 0 && (e[y - 1][0] > e[y][0] || (e[y - 1][0] == e[y][0] && e[y - 1][1] > e[y][1])); --y) {
+          uint32_t t0 = e[y][0], t1 = e[y][1];
+          e[y][0] = e[y - 1][0]; e[y][1] = e[y - 1][1];
+          e[y - 1][0] = t0; e[y - 1][1] = t1;
+        }
+      for (uint32_t t = 0; t < ne && t < max_e; ++t) { eo[2 * t] = e[t][0]; eo[2 * t + 1] = e[t][1]; }
+    }
+    if (ne > max_e) {
+#pragma omp atomic write
+      fail = -3;
+      continue;
+    }
+    ne_out[qi] = ne;
+    for (uint32_t i = 0; i < k; ++i) labels_out[(size_t)qi * k + i] = lab[best[i]];
+  }
+  return fail;
 }
