@@ -2,39 +2,39 @@
 """Benchmark: exact subgraph-matching throughput on one B200 (queries/s and
 embeddings/s, batched vs plain, p50/p99 latency).
 
-Headline workload (default `rmat16`, the configuration whose every query
-completes exactly): R-MAT scale 16 (65,536 vertices), edge factor 8,
-(a,b,c,d) = (0.57,0.19,0.19,0.05), self loops and duplicates removed, uint32
-CSR with sorted adjacency, 8 uniform labels; 100 random-walk queries of 4
-vertices (seeded synthetic stand-ins; the reference's datasets are not used).
-A step is one gem_batch_run over the 100 queries (one persistent join launch
-per wave); `plain` runs the same queries one gem_query_run each.
+Headline workload (`--workload rmat22-mix`, the batched configuration):
+R-MAT scale 22 (4,194,304 vertices), edge factor 16, (a,b,c,d) =
+(0.57,0.19,0.19,0.05), self loops and duplicates removed, uint32 CSR with
+sorted adjacency, 16 labels Zipf(s=1.0); 1,000 random-walk queries whose
+sizes are drawn uniformly from {4, 8, 12, 16, 24, 32} vertices, alternately
+sparse (average degree <= 3) and dense (above 3; a 4-vertex query cannot
+exceed 3, so its "dense" draw keeps the walk's induced edges).  Seeded
+synthetic stand-ins; the reference's datasets are not used.  A step is one
+gem_batch_run over the 1,000 queries.  Every query runs under a per-query
+device time cap (`--cap-ms`): a query still running when the cap expires is
+reported as capped, never as an exact count, and the headline counts exact
+queries only.  `plain` runs a stratified sample of the same queries one
+gem_query_run each under the same cap.
 
-The scale-22 workload (`--workload rmat22`: 4,194,304 vertices, edge factor
-16, 16 labels Zipf(s=1.0), query sets 8 sparse / 8 dense / 16 sparse / 16
-dense) is reported in the `rmat22` section: its random-walk queries have
-10^13 to 10^17 embeddings each, so no exact method finishes them in a
-bounded step; the section reports, per query under a device time cap,
-whether it completed and the enumeration rate.  A query that exceeds the cap
-is reported as capped, never as an exact count.
+Section `config1` (`--workload rmat16` makes it the headline): R-MAT scale
+16, edge factor 8, 8 uniform labels, 100 random-walk 4-vertex queries, all
+exact; batched vs plain, every count and hash checked against the CPU oracle.
+Its `serving` part submits those queries through gem_submit / gem_poll under
+Poisson arrivals.
 
-Its `out_of_core` part runs one batch of 4-vertex queries on that graph in
-core, out of core with the adjacency streamed in partitions, and out of core
-reading the pinned adjacency in place, and reports each mode's table-build
-and wave times with equal counts.
+Section `rmat22`: the scale-22 graph with the 8s/8d/16s/16d query sets, each
+query plain under a device cap (status and prefix-match rate).  Its
+`out_of_core` part runs 4-vertex queries in core, out of core with streamed
+adjacency partitions and out of core reading the pinned adjacency in place.
 
-The `serving` section submits the headline queries one by one through
-gem_submit / gem_poll under Poisson arrivals (1,000 / 5,000 / 20,000 per
-second, one second each) and reports latency percentiles and the achieved
-rate; every result is checked against the batched count.
-
-`value` is device-timed (CUDA events around each batch, inputs resident in
-HBM), `e2e` is wall time around the C-ABI call from host buffers (query
-arrays in, results out).  L2 is flushed between steps (a 256 MiB write).
-With torchrun (N > 1) every rank runs an independent replica on its own share
-of the batches (the path has no exchange step); rank 0 reports the max time.
-`--impl reference` times the CPU restatement of the path (the reference has no
-CPU join) on the host cores with all threads.
+`value` is device-timed (CUDA events around each wave, inputs resident in
+HBM), `e2e` is wall time around the same C-ABI calls from host buffers
+(query arrays in, results out).  L2 is flushed between steps (a 256 MiB
+write).  With torchrun (N > 1) every rank runs an independent replica on its
+own queries (the path has no exchange step); rank 0 reports the max time.
+`--impl reference` times the CPU restatement of the path (the reference has
+no CPU join) on the host cores with all threads; it builds its inputs with
+the oracle's generators and never loads libgem.
 """
 import argparse
 import json
@@ -51,7 +51,17 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 SETS = ((8, 1), (8, 2), (16, 1), (16, 2))  # (k, density: 1 sparse, 2 dense)
+MIX_SIZES = (4, 8, 12, 16, 24, 32)
 METRIC = "queries/s & embeddings/s on 1 B200, batched vs plain, exact counts; p50/p99 ms"
+GRAPHS = {  # name: (scale, edge factor, labels, zipf s)
+    "rmat22-mix": (22, 16, 16, 1.0),
+    "rmat16": (16, 8, 8, 0.0),
+    "rmat22": (22, 16, 16, 1.0),
+}
+DEFAULTS = {  # per workload: batch, per-query cap (ms), plain sample, autotune
+    "rmat22-mix": dict(batch=1000, cap_ms=100, plain=200, autotune=0),
+    "rmat16": dict(batch=100, cap_ms=20000, plain=100, autotune=1),
+}
 
 
 def dist_env():
@@ -123,42 +133,72 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def parse_sets(spec):
-    """'8s,8d,16s,16d' -> ((8, 1), (8, 2), (16, 1), (16, 2)); a = any density."""
-    out = []
-    for tok in spec.split(","):
-        tok = tok.strip()
-        out.append((int(tok[:-1]), {"a": 0, "s": 1, "d": 2}[tok[-1]]))
-    return tuple(out)
+def _mix64(x):
+    """splitmix64 finaliser of x + golden gamma (the generators' mixer)."""
+    m = (1 << 64) - 1
+    x = (x + 0x9E3779B97F4A7C15) & m
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & m
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & m
+    return x ^ (x >> 31)
 
 
-def make_workload(gem, name, sets_spec=None):
-    if name == "rmat22":
-        t = time.time()
-        g = gem.HostGraph.rmat(22, 16, seed=0x47454D00 + 22).set_labels(16, 1.0, seed=(0x47454D00 + 22) ^ 0x4C)
-        gen_s = time.time() - t
-        desc = {"workload": "rmat22-ef16-zipf16", "scale": 22, "edge_factor": 16, "labels": 16, "zipf_s": 1.0}
-        sets = SETS
-    elif name == "rmat16":
-        t = time.time()
-        g = gem.HostGraph.rmat(16, 8, seed=0x47454D00 + 16).set_labels(8, 0.0, seed=(0x47454D00 + 16) ^ 0x4C)
-        gen_s = time.time() - t
-        desc = {"workload": "rmat16-ef8-uniform8", "scale": 16, "edge_factor": 8, "labels": 8, "zipf_s": 0.0}
-        sets = ((4, 0),)
+def make_graph(backend, name):
+    """The seeded data graph of a workload, built by `backend`: the libgem
+    binding (gem_b200) or the oracle's restated generators (same arrays)."""
+    scale, ef, nl, zs = GRAPHS[name]
+    seed = 0x47454D00 + scale
+    t = time.time()
+    if backend.__name__ == "oracle":
+        g = backend.set_labels(backend.rmat(scale, ef, seed=seed), nl, zs, seed=seed ^ 0x4C)
     else:
-        raise SystemExit(f"unknown workload {name}")
-    if sets_spec:
-        sets = parse_sets(sets_spec)
-    return g, desc, sets, gen_s
+        g = backend.HostGraph.rmat(scale, ef, seed=seed).set_labels(nl, zs, seed=seed ^ 0x4C)
+    return g, time.time() - t
 
 
-def query_pool(gem, g, sets, per_set):
-    pools = [gem.gen_queries(g, k, d, per_set, seed=0x51000 + i) for i, (k, d) in enumerate(sets)]
+def mix_pool(backend, g, n, seed=0x51003):
+    """Config-3 queries: query i has size MIX_SIZES[mix64(seed + i) % 6] and is
+    sparse for even i, dense for odd i; the queries of one (size, density)
+    come from one random-walk stream (seed << 8 | 4 size + density)."""
+    ks = [MIX_SIZES[_mix64(seed + i) % len(MIX_SIZES)] for i in range(n)]
+    ds = [1 + (i % 2) for i in range(n)]
+    need = {}
+    for k, d in zip(ks, ds):
+        need[(k, d)] = need.get((k, d), 0) + 1
+    made = {kd: backend.gen_queries(g, kd[0], kd[1], c, seed=(seed << 8) | (4 * kd[0] + kd[1]))
+            for kd, c in need.items()}
+    used = {kd: 0 for kd in need}
     out = []
-    for j in range(per_set):
-        for p in pools:
-            out.append(p[j])
+    for k, d in zip(ks, ds):
+        out.append(made[(k, d)][used[(k, d)]])
+        used[(k, d)] += 1
     return out
+
+
+def config1_pool(backend, g, n=100, seed=0x51000):
+    return backend.gen_queries(g, 4, 0, n, seed=seed)
+
+
+def workload_pool(backend, name, g, n):
+    if name == "rmat22-mix":
+        return mix_pool(backend, g, n)
+    if name == "rmat16":
+        return config1_pool(backend, g, n)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_config(name, args, world):
+    """The `config` object both arms print for a workload."""
+    scale, ef, nl, zs = GRAPHS[name]
+    c = {"workload": f"{name}-ef{ef}-{'zipf' if zs else 'uniform'}{nl}" if name != "rmat22-mix"
+         else "rmat22-ef16-zipf16-mix1000", "scale": scale, "edge_factor": ef, "labels": nl, "zipf_s": zs,
+         "batch": args.batch, "time_cap_ms": args.cap_ms, "parallelism": f"replicas{world}",
+         "l2": "flushed (256 MiB write)"}
+    if name == "rmat22-mix":
+        c["query_sizes"] = list(MIX_SIZES)
+        c["densities"] = "alternating sparse/dense"
+    else:
+        c["query_sizes"] = [4]
+    return c
 
 
 def flush_l2(torch_dev):
@@ -176,6 +216,13 @@ def pctl(xs, p):
     return xs[k]
 
 
+def waves_of(rs):
+    w = {}
+    for r in rs:
+        w.setdefault(r["wave"], r)
+    return list(w.values())
+
+
 def run_gem(args):
     import gem_b200 as gem
     rank, world, local = dist_env()
@@ -186,25 +233,27 @@ def run_gem(args):
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    g, desc, sets, gen_s = make_workload(gem, args.workload, args.sets)
-    pool = query_pool(gem, g, sets, args.per_set)
+    g, gen_s = make_graph(gem, args.workload)
     B = args.batch
+    pool = workload_pool(gem, args.workload, g, B * world)
     ctx = gem.Context(device=local, time_cap_ms=args.cap_ms)
     ctx.load_graph(g)
-    # the tuner runs the timed batch's queries (untimed); a wave's join lasts as long
-    # as its heaviest query, so a sample without it tunes for the wrong critical path
-    tuned = ctx.autotune(pool[: min(len(pool), args.batch)], trial_cap_ms=args.cap_ms) if args.autotune else {}
+    tuned = {}
+    if args.autotune:
+        # tuned on a disjoint sample of the same configuration (another query seed)
+        tune_pool = config1_pool(gem, g, B, seed=0x51080) if args.workload == "rmat16" else mix_pool(gem, g, B, 0x51083)
+        tuned = ctx.autotune(tune_pool, trial_cap_ms=args.cap_ms)
 
     def batch_of(step):
         return [pool[i] for i in batch_indices(step, rank, world, B, len(pool))]
 
-    # warm-up (compiles nothing; touches code paths and the arena)
     for s in range(args.warmup):
         ctx.batch(batch_of(s))
     steps = list(range(args.warmup, args.warmup + args.steps))
     dev_ms, wall_ms, res_all = [], [], []
-    h2d = d2h = launches = jbytes = n_joins = 0
-    jms = 0.0
+    h2d = d2h = launches = 0
+    jbytes = jms = tbytes = tpass_ms = 0.0
+    n_joins = n_tab = 0
     phase = {"filter": 0.0, "tables": 0.0, "index": 0.0, "join": 0.0}
     with Clocks(local) as clk:
         for s in steps:
@@ -213,98 +262,67 @@ def run_gem(args):
             if dist:
                 dist.barrier()
             torch.cuda.synchronize()
-            st, rs = ctx.batch(qs)
+            t0 = time.perf_counter()
+            st, rs = ctx.batch(qs)  # query arrays from host memory, results back in host memory
             torch.cuda.synchronize()
-            # device time of the batch: sum over its waves (first kernel .. last kernel, CUDA events)
-            waves = {}
-            for r in rs:
-                waves.setdefault(r["wave"], r)
-            dev_ms.append(sum(r["ms"]["total"] for r in waves.values()))
-            launches += sum(r["launches"] for r in waves.values())
-            jbytes += sum(r["bytes_alg"][3] for r in waves.values())
-            n_joins += len(waves)
-            jms += sum(r["ms"]["join"] for r in waves.values())
+            wall_ms.append((time.perf_counter() - t0) * 1e3)
+            ws = waves_of(rs)
+            dev_ms.append(sum(r["ms"]["total"] for r in ws))
+            launches += sum(r["launches"] for r in ws)
+            jbytes += sum(r["bytes_alg"][3] for r in ws)
+            jms += sum(r["ms"]["join"] for r in ws)
+            n_joins += len(ws)
+            for r in ws:
+                if r["table_pass_ms"][0] + r["table_pass_ms"][1] > 0:
+                    tbytes += r["bytes_alg"][2]
+                    tpass_ms += r["table_pass_ms"][0] + r["table_pass_ms"][1]
+                    n_tab += 1
             for k in phase:
-                phase[k] += sum(r["ms"][k] for r in waves.values())
+                phase[k] += sum(r["ms"][k] for r in ws)
+            h2d += sum(4 * q.nv + 8 * q.ne for q in qs)  # the queries' label and edge arrays
+            d2h += ctypes_result_bytes(gem) * len(qs)
             res_all.append(rs)
-    # end to end through the public API: query arrays in host memory, the
-    # counts and statuses read back, timed on the host (a separate pass over
-    # the same steps, so the device-timed pass keeps its per-wave records)
-    e2e_same, e2e_exact = True, 0
-    for i, s in enumerate(steps):
-        qs = batch_of(s)
-        flush_l2(dev)
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        st, counts, status = ctx.batch_counts(qs)
-        torch.cuda.synchronize()
-        wall_ms.append((time.perf_counter() - t0) * 1e3)
-        e2e_same &= all(int(c) == r["count"] for c, r in zip(counts, res_all[i]) if r["status"] == "OK")
-        e2e_exact += int((status == 0).sum())
-        h2d += sum(4 * q.nv + 8 * q.ne for q in qs)  # the queries' label and edge arrays
-        d2h += 64 * len(qs) + 1024  # per-query counters and the control block
     exact = sum(1 for rs in res_all for r in rs if r["status"] == "OK")
     capped = sum(1 for rs in res_all for r in rs if r["status"] == "ERR_TIMEOUT")
     emb = sum(r["count"] for rs in res_all for r in rs if r["status"] == "OK")
+    counts_stable = all(res_all[0][i]["count"] == rs[i]["count"] for rs in res_all[1:] for i in range(len(rs))
+                        if rs[i]["status"] == "OK" and res_all[0][i]["status"] == "OK") if world == 1 else None
     tdev = sum(dev_ms) / 1e3
     twall = sum(wall_ms) / 1e3
-    # join-kernel roofline from the batches' algorithmic bytes and join times
-    jb = jbytes
-    jt = jms / 1e3
+    e2e_exact = exact
     if dist:
-        tdev, twall, exact, emb, capped, e2e_exact = reduce_over_ranks(dist, tdev, twall, exact, emb, capped, e2e_exact)
-    # plain mode: the same queries, one gem_query_run each (rank 0)
+        tdev, twall, exact, emb, capped, e2e_exact = reduce_over_ranks(dist, tdev, twall, exact, emb, capped, exact)
     plain = {}
     if rank == 0 and args.plain > 0:
-        lat, pe, pn, pdev = [], 0, 0, 0.0
-        qs = batch_of(args.warmup)[: args.plain]
-        same = True
-        for q, rb in zip(qs, res_all[0]):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            r = ctx.run(q, raise_on_error=False)
-            torch.cuda.synchronize()
-            lat.append((time.perf_counter() - t0) * 1e3)
-            pdev += r["ms"]["total"] / 1e3
-            if r["status"] == "OK":
-                pn += 1
-                pe += r["count"]
-                same &= rb["status"] != "OK" or rb["count"] == r["count"]
-        plain = {"queries": len(lat), "exact": pn, "queries_per_s": pn / pdev if pdev else None,
-                 "queries_per_s_wall": pn / (sum(lat) / 1e3) if lat else None,
-                 "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99), "counts_equal_batched": same}
+        plain = plain_section(ctx, batch_of(args.warmup), res_all[0], args.plain)
     ctx.close()
-    serving = None
-    if rank == 0 and args.serve_seconds > 0:
-        ref = {i: r["count"] for i, r in enumerate(res_all[0])} if len(batch_of(args.warmup)) == len(pool) else {}
-        serving = serving_section(gem, args, local, g, pool, ref) if ref else None
-    c2 = None
+    sections = {}
+    if rank == 0 and args.workload != "rmat16" and args.config1:
+        sections["config1"] = config1_section(gem, args, local)
     if rank == 0 and (args.c2_sample > 0 or args.ooc_sample > 0):
-        t = time.time()
-        g22 = gem.HostGraph.rmat(22, 16, seed=0x47454D00 + 22).set_labels(16, 1.0, seed=(0x47454D00 + 22) ^ 0x4C)
-        gen22 = time.time() - t
+        if args.workload.startswith("rmat22"):
+            g22, gen22 = g, gen_s
+        else:
+            g22, gen22 = make_graph(gem, "rmat22")
         c2 = rmat22_section(gem, args, local, g22, gen22) if args.c2_sample > 0 else {"graph_gen_s": round(gen22, 2)}
         if args.ooc_sample > 0:
             c2["out_of_core"] = out_of_core_section(gem, args, local, g22)
+        sections["rmat22"] = c2
         del g22
     if dist:
         dist.destroy_process_group()
     if rank != 0:
         return
-    peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     except Exception:
         peak, peak_src = 6650.0, "fallback"
-    achieved = (jb / jt / 1e9) if jt > 0 else 0.0
-    set_names = ",".join(f"{k}{'s' if d == 1 else 'd' if d == 2 else 'a'}" for k, d in sets)
-    traffic, traffic_src = profiled_traffic(f"{args.workload} {set_names} batch {B}")
+    cfg = workload_config(args.workload, args, world)
+    value = exact / tdev if tdev > 0 else 0.0
     line = {
         "metric": METRIC,
-        "value": exact / tdev if tdev > 0 else 0.0,
+        "value": value,
         "unit": "queries/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -315,41 +333,170 @@ def run_gem(args):
         "vs_baseline": None,
         "dtype": "u32/u64",
         "data": "synthetic R-MAT graph and random-walk queries (seeded)",
-        "config": dict(desc, batch=B, query_sets=[f"{k}{'s' if d == 1 else 'd' if d == 2 else 'a'}" for k, d in sets],
-                       time_cap_ms=args.cap_ms, parallelism=f"replicas{world}", l2="flushed (256 MiB write)",
-                       exact_queries=exact, capped_queries=capped, graph_gen_s=round(gen_s, 2)),
+        "config": cfg,
+        "exact_queries": exact,
+        "capped_queries": capped,
+        "graph_gen_s": round(gen_s, 2),
         "embeddings_per_s": emb / tdev if tdev > 0 else 0.0,
-        "batched_over_plain": (exact / tdev) / plain["queries_per_s"] if plain.get("queries_per_s") else None,
+        "embeddings_note": "sum of the exact queries' counts per second; closed-form suffix levels are counted, "
+                           "not enumerated one by one",
+        "batched_over_plain": value / plain["queries_per_s"] if plain.get("queries_per_s") else None,
         "plain": plain,
-        "phase_ms": {k: round(v, 3) for k, v in phase.items()},
+        "counts_stable_across_steps": counts_stable,
+        "phase_ms_per_step": {k: round(v / args.steps, 3) for k, v in phase.items()},
         "autotune": tuned,
-        "serving": serving,
-        "rmat22": c2,
-        "e2e": {"value": e2e_exact / twall if twall > 0 else 0.0, "unit": "queries/s", "counts_equal": e2e_same,
-                "h2d_bytes_per_step": h2d // args.steps,
-                "d2h_bytes_per_step": d2h // args.steps},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if peak else None, "traffic": traffic, "traffic_source": traffic_src,
-                     "alg_bytes_per_launch": jb / n_joins if n_joins else None, "kernel": "join_kernel<COUNT>",
-                     "peak_source": peak_src},
+        "e2e": {"value": e2e_exact / twall if twall > 0 else 0.0, "unit": "queries/s",
+                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    # roofline of the dominant kernel: the edge-table passes or the join
+    t_tab = tpass_ms / n_tab if n_tab else 0.0
+    t_join = jms / n_joins if n_joins else 0.0
+    roof_tab = roofline(tbytes / n_tab if n_tab else 0.0, t_tab, peak, peak_src,
+                        "table_src_kernel<count>+<write> (edge-table passes)",
+                        profiled_traffic("tables", args.workload, B))
+    roof_join = roofline(jbytes / n_joins if n_joins else 0.0, t_join, peak, peak_src, "join_kernel<COUNT>",
+                         profiled_traffic("join", args.workload, B))
+    line["roofline"], line["roofline_other"] = (roof_tab, roof_join) if tpass_ms >= jms else (roof_join, roof_tab)
+    line["roofline"]["share_of_step"] = round((tpass_ms if tpass_ms >= jms else jms) / (tdev * 1e3), 3) if tdev else None
     if args.cpu_sample > 0:
+        line["parity"] = oracle_parity(g, batch_of(args.warmup), res_all[0], args.cpu_parity_cap, args.cpu_budget_s)
         line["cpu_baseline"] = cpu_baseline(g, pool, args)
-        line["host_path"] = host_path_baseline(g, pool[:B], (phase["filter"] + phase["tables"]) / args.steps)
+        qs0 = batch_of(args.warmup)
+        hstride = max(1, len(qs0) // args.host_path_queries)
+        line["host_path"] = host_path_baseline(g, qs0[::hstride], (phase["filter"] + phase["tables"]) / args.steps,
+                                               len(qs0), args.cpu_budget_s)
+    line.update(sections)
     print(json.dumps(line), flush=True)
+
+
+def ctypes_result_bytes(gem):
+    import ctypes
+    return ctypes.sizeof(gem._Result)
+
+
+def roofline(alg_bytes, ms, peak, peak_src, kernel, traffic):
+    achieved = alg_bytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    t, src = traffic
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if peak else None,
+            "traffic": t, "traffic_source": src, "alg_bytes_per_launch": alg_bytes, "ms_per_launch": ms,
+            "kernel": kernel, "peak_source": peak_src}
+
+
+def profiled_traffic(kind, workload, batch):
+    """DRAM bytes (read + write) of one launch of `kind` ("join" or "tables")
+    on workload `workload` with batch `batch`, from the committed ncu capture
+    summary whose `workload_key` line equals "<kind> <workload> batch
+    <batch>" and which states `dram_bytes_per_launch`, or (None, None)."""
+    import glob
+    import re
+    key = f"{kind} {workload} batch {batch}"
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        text = open(path).read()
+        k = re.search(r"^workload_key: (.+)$", text, re.M)
+        m = re.search(r"^dram_bytes_per_launch: (\d+)$", text, re.M)
+        if k and m and k.group(1).strip() == key:
+            return int(m.group(1)), os.path.relpath(path, ROOT) + " (ncu)"
+    return None, None
+
+
+def plain_section(ctx, qs_all, batch_res, n):
+    """The same queries one gem_query_run each (a stratified sample of n of
+    them: every len/n-th), same cap; device time from CUDA events, latency
+    on the host; counts compared with the batched run where both are exact."""
+    import torch
+    stride = max(1, len(qs_all) // n)
+    idx = list(range(0, len(qs_all), stride))[:n]
+    lat, pe, pn, pdev, same, capped = [], 0, 0, 0.0, True, 0
+    bexact = 0
+    for i in idx:
+        q = qs_all[i]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = ctx.run(q, raise_on_error=False)
+        torch.cuda.synchronize()
+        lat.append((time.perf_counter() - t0) * 1e3)
+        pdev += r["ms"]["total"] / 1e3
+        rb = batch_res[i]
+        bexact += rb["status"] == "OK"
+        if r["status"] == "OK":
+            pn += 1
+            pe += r["count"]
+            same &= rb["status"] != "OK" or rb["count"] == r["count"]
+        elif r["status"] == "ERR_TIMEOUT":
+            capped += 1
+    return {"queries": len(idx), "sample": f"every {stride}th query of the batch", "exact": pn, "capped": capped,
+            "batched_exact_same_queries": bexact,
+            "queries_per_s": pn / pdev if pdev else None, "queries_per_s_wall": pn / (sum(lat) / 1e3) if lat else None,
+            "embeddings_per_s": pe / pdev if pdev else None,
+            "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99), "counts_equal_batched": same}
+
+
+def config1_section(gem, args, local):
+    """Configuration 1 (R-MAT scale 16, 100 four-vertex queries): batched vs
+    plain, every count checked against the oracle, and serving."""
+    import torch
+    dev = torch.device("cuda", local)
+    g, gen_s = make_graph(gem, "rmat16")
+    pool = config1_pool(gem, g)
+    out = {"workload": "rmat16-ef8-uniform8", "queries": len(pool), "graph_gen_s": round(gen_s, 2)}
+    with gem.Context(device=local, time_cap_ms=20000) as c:
+        c.load_graph(g)
+        out["autotune"] = c.autotune(config1_pool(gem, g, 100, seed=0x51080), trial_cap_ms=20000)
+        for _ in range(3):
+            c.batch(pool)
+        ts, rs = [], None
+        for _ in range(args.c1_steps):
+            flush_l2(dev)
+            _, rs = c.batch(pool)
+            ts.append(sum(r["ms"]["total"] for r in waves_of(rs)))
+        exact = sum(r["status"] == "OK" for r in rs)
+        out["batched_queries_per_s"] = exact / (sum(ts) / len(ts) / 1e3)
+        out["batched_ms_per_step"] = statistics.median(ts)
+        out["plain"] = plain_section(c, pool, rs, len(pool))
+        out["batched_over_plain"] = (out["batched_queries_per_s"] / out["plain"]["queries_per_s"]
+                                     if out["plain"].get("queries_per_s") else None)
+        counts = [r["count"] if r["status"] == "OK" else None for r in rs]
+    out["parity"] = oracle_parity(g, pool, rs, 0, 120.0)
+    if args.serve_seconds > 0:
+        out["serving"] = serving_section(gem, args, local, g, pool, {i: x for i, x in enumerate(counts)})
+    return out
+
+
+def oracle_parity(g, qs, rs, work_cap, budget_s):
+    """The batched run's exact counts against the CPU oracle (each query under
+    `work_cap` scanned arcs, 0 = none; queries the oracle does not finish
+    are skipped and counted; stops starting queries after budget_s)."""
+    import oracle
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    checked = equal = skipped = 0
+    for q, r in zip(qs, rs):
+        if r["status"] != "OK":
+            continue
+        if time.perf_counter() - t0 > budget_s:
+            skipped += 1
+            continue
+        c, _, ok = oracle.count(g, q, threads=threads, want_hash=False, work_cap=work_cap)
+        if not ok:
+            skipped += 1
+            continue
+        checked += 1
+        equal += c == r["count"]
+    return {"checked": checked, "equal": equal, "not_finished_by_oracle": skipped,
+            "oracle_work_cap": work_cap, "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def serving_section(gem, args, local, g, pool, ref_counts):
     """Continuous batching through gem_submit / gem_poll under Poisson arrivals
-    of the headline queries (cycled), one stream per rate: latency from the
+    of the pool's queries (cycled), one stream per rate: latency from the
     arrival to the result being visible, achieved rate, and every count
     checked against the batched run's."""
     import collections
     import random
-    out = {"queries": "the headline pool, cycled", "seconds_per_rate": args.serve_seconds, "rates": []}
-    with gem.Context(device=local, time_cap_ms=args.cap_ms) as c:
+    out = {"queries": "the config-1 pool, cycled", "seconds_per_rate": args.serve_seconds, "rates": []}
+    with gem.Context(device=local, time_cap_ms=20000) as c:
         c.load_graph(g)
         for lam in [float(x) for x in args.serve_rates.split(",") if x]:
             rng = random.Random(0x5E12 + int(lam))
@@ -388,24 +535,11 @@ def serving_section(gem, args, local, g, pool, ref_counts):
     return out
 
 
-def profiled_traffic(key):
-    """DRAM bytes (read + write) of one join launch of the workload `key`
-    ("<workload> <query sets> batch <B>"), from the committed ncu capture
-    summary whose `workload_key` line equals it, or None."""
-    import glob
-    import re
-    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "join_*.md"))):
-        text = open(path).read()
-        k = re.search(r"^workload_key: (.+)$", text, re.M)
-        m = re.search(r"^dram_bytes_per_launch: (\d+)$", text, re.M)
-        if k and m and k.group(1).strip() == key:
-            return int(m.group(1)), os.path.relpath(path, ROOT) + " (ncu, one launch)"
-    return None, None
-
-
 def rmat22_section(gem, args, local, g, gen_s):
     """Scale-22 R-MAT with 16 Zipf(1.0) labels and the 8s/8d/16s/16d query sets:
-    per query, plain run under a device time cap (status, count, nodes/s)."""
+    per query, plain run under a device time cap (status, nodes/s).  A capped
+    query reports the partial embeddings it extended before the cap, not a
+    count."""
     per = max(1, args.c2_sample // len(SETS))
     out = {"workload": "rmat22-ef16-zipf16", "time_cap_ms": args.c2_cap_ms, "graph_gen_s": round(gen_s, 2),
            "queries": []}
@@ -417,8 +551,7 @@ def rmat22_section(gem, args, local, g, gen_s):
                 js = r["ms"]["join"] / 1e3
                 out["queries"].append({"set": f"{k}{'s' if d == 1 else 'd'}", "edges": q.ne, "status": r["status"],
                                        "count": r["count"] if r["status"] == "OK" else None,
-                                       "count_before_cap": r["count"] if r["status"] != "OK" else None,
-                                       "join_ms": round(r["ms"]["join"], 1),
+                                       "prefix_matches": r["nodes"], "join_ms": round(r["ms"]["join"], 1),
                                        "prefix_matches_per_s": r["nodes"] / js if js > 0 else None})
     out["exact"] = sum(1 for x in out["queries"] if x["status"] == "OK")
     return out
@@ -457,11 +590,9 @@ def out_of_core_section(gem, args, local, g):
             tab, tot = [], []
             for _ in range(3):
                 _, rs = c.batch(qs)
-                waves = {}
-                for r in rs:
-                    waves.setdefault(r["wave"], r)
-                tab.append(sum(w["ms"]["tables"] for w in waves.values()))
-                tot.append(sum(w["ms"]["total"] for w in waves.values()))
+                ws = waves_of(rs)
+                tab.append(sum(w["ms"]["tables"] for w in ws))
+                tot.append(sum(w["ms"]["total"] for w in ws))
             counts[name] = [r["count"] if r["status"] == "OK" else None for r in rs]
             m = {"tables_ms": round(sorted(tab)[1], 2), "wave_ms": round(sorted(tot)[1], 2)}
             if kw:
@@ -471,18 +602,22 @@ def out_of_core_section(gem, args, local, g):
     return out
 
 
-def host_path_baseline(g, qs, gpu_ms_per_step):
-    """The reference's host-side path for one batch: its out-of-core filter and
-    edge-table build (OpenMP, out-of-core/lib/filter/src/filter.cu:61-295 and
-    out-of-core/lib/structure/src/unifiedTrie.cu:1224-1427, restated in the
-    oracle with the reference's worker counts) on the host cores, beside the
-    GPU's filter + tables phases per step.  The reference builds both
-    directions of every query edge whose source has query degree > 1."""
+def host_path_baseline(g, qs, gpu_ms_per_step, step_queries, budget_s):
+    """The reference's host-side path for a sample of the batch: its
+    out-of-core filter and edge-table build (OpenMP, out-of-core/lib/filter/
+    src/filter.cu:61-295 and out-of-core/lib/structure/src/unifiedTrie.cu
+    :1224-1427, restated in the oracle with the reference's worker counts) on
+    the host cores, scaled to the step's queries, beside the GPU's filter +
+    tables phases per step.  The reference builds both directions of every
+    query edge whose source has query degree > 1."""
     import oracle
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    ntab = 0
+    ntab = done = 0
     for q in qs:
+        if time.perf_counter() - t0 > budget_s:
+            break
+        done += 1
         cand = oracle.filter_mt(g, q)
         deg = np.bincount(q.edges.reshape(-1), minlength=q.nv) if q.ne else np.zeros(q.nv, int)
         for a, b in q.edges.tolist():
@@ -491,19 +626,23 @@ def host_path_baseline(g, qs, gpu_ms_per_step):
                     oracle.edge_table_mt(g, cand[s], cand[t])
                     ntab += 1
     ms = (time.perf_counter() - t0) * 1e3
-    return {"filter_tables_ms_per_batch": round(ms, 2), "gpu_filter_tables_ms_per_step": round(gpu_ms_per_step, 3),
-            "gpu_speedup": round(ms / gpu_ms_per_step, 1) if gpu_ms_per_step > 0 else None,
-            "threads": {"filter": min(16, cores), "tables": min(4, cores)}, "queries": len(qs), "tables": ntab,
-            "kind": "port"}
+    per_step = ms * step_queries / max(1, done)
+    return {"filter_tables_ms_sample": round(ms, 2), "sample_queries": done,
+            "filter_tables_ms_per_step_est": round(per_step, 1),
+            "gpu_filter_tables_ms_per_step": round(gpu_ms_per_step, 3),
+            "gpu_speedup": round(per_step / gpu_ms_per_step, 1) if gpu_ms_per_step > 0 else None,
+            "threads": {"filter": min(16, cores), "tables": min(4, cores)}, "tables": ntab, "kind": "port"}
 
 
 def cpu_baseline(g, pool, args):
+    """The oracle on the host cores over a bounded sample of the pool."""
     import oracle
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
-    n_ok = 0
-    n = 0
+    n_ok = n = 0
     for q in pool[: args.cpu_sample]:
+        if time.perf_counter() - t0 > args.cpu_budget_s:
+            break
         c, h, ok = oracle.count(g, q, threads=threads, want_hash=False, work_cap=args.cpu_work_cap)
         n += 1
         n_ok += 1 if ok else 0
@@ -514,19 +653,19 @@ def cpu_baseline(g, pool, args):
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the path (the reference has
+    no CPU join) over a bounded sample per step, inputs from the oracle's
+    generators (libgem is never loaded)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import gem_b200 as gem
-    g, desc, sets, _ = make_workload(gem, args.workload, args.sets)
-    pool = query_pool(gem, g, sets, args.per_set)
     import oracle
+    g, _ = make_graph(oracle, args.workload)
+    pool = workload_pool(oracle, args.workload, g, args.batch)
     threads = os.cpu_count() or 1
-    B = args.batch
-    S = max(1, min(args.ref_sample, B))
+    S = max(1, min(args.ref_sample, len(pool)))
     times, exact, emb = [], 0, 0
     for s in range(args.warmup + args.steps):
-        # a bounded sample of the workload per step: S queries, cycling through the pool
         qs = [pool[(s * S + j) % len(pool)] for j in range(S)]
         t0 = time.perf_counter()
         for q in qs:
@@ -538,42 +677,55 @@ def run_reference(args):
             times.append(time.perf_counter() - t0)
     T = sum(times)
     v = exact / T if T > 0 else 0.0
+    cfg = workload_config(args.workload, args, world)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": T * 1e3 / max(1, args.steps), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64", "data": "synthetic (seeded)",
-        "config": dict(desc, batch=B, cpu_work_cap=args.cpu_work_cap),
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64", "data": "synthetic (seeded)", "config": cfg,
         "embeddings_per_s": emb / T if T > 0 else 0.0,
         "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
                          "sample": f"{S} queries per step, cycling through the {len(pool)}-query pool, each capped at "
-                                   f"{args.cpu_work_cap} scanned arcs"},
+                                   f"{args.cpu_work_cap} scanned arcs (a capped query is not counted as exact)"},
         "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
-def main():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gem", choices=["gem", "reference"])
-    ap.add_argument("--workload", default="rmat16")
-    ap.add_argument("--sets", default=None, help="query sets, e.g. '8s,8d,16s,16d' (s sparse, d dense, a any)")
-    ap.add_argument("--per-set", type=int, default=100)
-    ap.add_argument("--batch", type=int, default=100)
-    ap.add_argument("--cap-ms", type=int, default=20000)
-    ap.add_argument("--plain", type=int, default=100)
-    ap.add_argument("--autotune", type=int, default=1)
+    ap.add_argument("--workload", default="rmat22-mix", choices=sorted(DEFAULTS))
+    ap.add_argument("--batch", type=int, default=None, help="queries per step (default: the workload's)")
+    ap.add_argument("--cap-ms", type=int, default=None, help="per-query device time cap")
+    ap.add_argument("--plain", type=int, default=None, help="queries of the plain sample (0 = skip)")
+    ap.add_argument("--autotune", type=int, default=None)
+    ap.add_argument("--config1", type=int, default=1, help="run the config-1 section (headline rmat22-mix)")
+    ap.add_argument("--c1-steps", type=int, default=10)
     ap.add_argument("--c2-sample", type=int, default=8, help="scale-22 queries in the rmat22 section (0 = skip)")
     ap.add_argument("--ooc-sample", type=int, default=50,
                     help="4-vertex queries of the out-of-core comparison on the scale-22 graph (0 = skip)")
     ap.add_argument("--c2-cap-ms", type=int, default=1000)
     ap.add_argument("--cpu-sample", type=int, default=100, help="pool queries timed on the CPU oracle (0 = skip)")
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="wall-time bound of the CPU legs")
+    ap.add_argument("--cpu-parity-cap", type=int, default=200_000_000, help="oracle work cap of the parity check")
+    ap.add_argument("--host-path-queries", type=int, default=100)
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="per arrival rate in the serving section (0 = skip)")
     ap.add_argument("--serve-rates", default="1000,5000,20000", help="Poisson arrival rates (queries/s)")
-    ap.add_argument("--cpu-work-cap", type=int, default=1_000_000_000)
-    ap.add_argument("--ref-sample", type=int, default=8, help="queries per step of the reference arm (--impl reference)")
-    args = ap.parse_args()
+    ap.add_argument("--cpu-work-cap", type=int, default=200_000_000,
+                    help="scanned-arc cap per query of the CPU legs and the reference arm")
+    ap.add_argument("--ref-sample", type=int, default=4, help="queries per step of the reference arm (--impl reference)")
+    args = ap.parse_args(argv)
+    d = DEFAULTS[args.workload]
+    for k in ("batch", "cap_ms", "plain", "autotune"):
+        if getattr(args, k) is None:
+            setattr(args, k, d[k])
+    return args
+
+
+def main():
+    args = parse_args()
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -45,6 +45,7 @@ EXPORTS = (
     "gem_batch_run", "gem_embedding_hash", "gem_filter", "gem_edge_table", "gem_index_probe",
     "gem_submit", "gem_poll", "gem_autotune", "gem_filter_static", "gem_set_schedule", "gem_get_schedule",
     "gem_relaxed_sets", "gem_relaxed_run", "gem_ctx_ooc_stats", "gem_plan_query", "gem_hgraph_partitions",
+    "gem_estimate_bytes",
 )
 
 
@@ -86,7 +87,9 @@ class _Result(C.Structure):
     _fields_ = [("count", C.c_uint64), ("emb_hash", C.c_uint64), ("n_written", C.c_uint64),
                 ("status", C.c_uint32), ("n_tables", C.c_uint32), ("cand_total", C.c_uint64),
                 ("table_total", C.c_uint64), ("nodes", C.c_uint64), ("bytes_alg", C.c_uint64 * 4),
-                ("ms", C.c_float * 8), ("wave", C.c_uint32), ("launches", C.c_uint32)]
+                ("ms", C.c_float * 8), ("wave", C.c_uint32), ("launches", C.c_uint32),
+                ("table_pass_ms", C.c_float * 2), ("t_begin_ms", C.c_float), ("t_end_ms", C.c_float),
+                ("arena_bytes", C.c_uint64)]
 
 
 _lib = None
@@ -131,6 +134,7 @@ def lib():
                                      C.c_uint64, u64p, u64p]
         L.gem_index_probe.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_uint32, u32p, C.c_uint32, u32p]
         L.gem_submit.argtypes = [vp, C.POINTER(_Query), C.c_int, u64p]
+        L.gem_estimate_bytes.argtypes = [vp, C.POINTER(_Query), u64p]
         L.gem_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Result), C.POINTER(C.c_int)]
         L.gem_autotune.argtypes = [vp, C.POINTER(_Query), C.c_uint32, C.c_int, C.c_uint32, u32p]
         L.gem_relaxed_sets.argtypes = [C.POINTER(_Query), C.c_uint32, C.c_uint32, u64p, u32p]
@@ -357,7 +361,9 @@ class Result(dict):
                    status=STATUS.get(r.status, r.status), status_code=int(r.status), n_tables=int(r.n_tables),
                    cand_total=int(r.cand_total), table_total=int(r.table_total), nodes=int(r.nodes),
                    bytes_alg=[int(x) for x in r.bytes_alg], ms={p: float(r.ms[i]) for i, p in enumerate(PHASES)},
-                   wave=int(r.wave), launches=int(r.launches))
+                   wave=int(r.wave), launches=int(r.launches),
+                   table_pass_ms=[float(r.table_pass_ms[0]), float(r.table_pass_ms[1])],
+                   t_begin_ms=float(r.t_begin_ms), t_end_ms=float(r.t_end_ms), arena_bytes=int(r.arena_bytes))
         return d
 
 
@@ -494,6 +500,13 @@ class Context:
         st = _OocStats()
         _check(lib().gem_ctx_ooc_stats(self._h, C.byref(st)), self._h, "ooc_stats")
         return {k: int(getattr(st, k)) for k, _ in _OocStats._fields_ if k != "reserved0"}
+
+    def estimate_bytes(self, q):
+        """Device scratch bytes serving admission reserves for q (gem_estimate_bytes)."""
+        b = C.c_uint64()
+        qc = q._c()
+        _check(lib().gem_estimate_bytes(self._h, C.byref(qc), C.byref(b)), self._h, "estimate_bytes")
+        return b.value
 
     def submit(self, q, mode=MODE_COUNT):
         """Serving: returns a ticket, or None when admission is busy (retry later)."""

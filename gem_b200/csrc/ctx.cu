@@ -125,6 +125,20 @@ static gem_status aalloc(gem_ctx *ctx, uint64_t n, T **out) {
 // ---------------------------------------------------------------------------
 // Context and graph
 // ---------------------------------------------------------------------------
+// A context's own execution resources: stream, events, the join's control
+// block and task queue, the error words and the pinned staging buffer.
+static gem_status exec_init(gem_ctx *ctx) {
+  CU(cudaStreamCreateWithFlags(&ctx->s, cudaStreamNonBlocking));
+  for (auto &ev : ctx->ev) CU(cudaEventCreate(&ev));
+  CU(cudaMalloc(&ctx->d_ctl, sizeof(JControl)));
+  CU(cudaMalloc(&ctx->d_queue, sizeof(JTask) * TASK_CAP));
+  CU(cudaMalloc(&ctx->d_qends, sizeof(JQueueEnds) * QUEUE_SUBQ));
+  CU(cudaMalloc(&ctx->d_err, sizeof(uint32_t) * 4));
+  CU(cudaHostAlloc(&ctx->h_small, H_SMALL_BYTES, cudaHostAllocDefault));
+  ctx->device_bytes += sizeof(JControl) + sizeof(JTask) * TASK_CAP + sizeof(JQueueEnds) * QUEUE_SUBQ + 16;
+  return GEM_OK;
+}
+
 extern "C" gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out) {
   if (!out) return GEM_ERR_ARG;
   *out = nullptr;
@@ -139,22 +153,53 @@ extern "C" gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out) {
   }
   if (ctx->opts.device < 0 || ctx->opts.device >= ndev) return GEM_ERR_ARG;
   CU(cudaSetDevice(ctx->opts.device));
-  CU(cudaStreamCreateWithFlags(&ctx->s, cudaStreamNonBlocking));
-  for (auto &ev : ctx->ev) CU(cudaEventCreate(&ev));
   size_t fr = 0, tot = 0;
   CU(cudaMemGetInfo(&fr, &tot));
   ctx->budget = ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : (uint64_t)(fr * 0.9);
   if (ctx->budget > fr) ctx->budget = fr;
   CU(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->opts.device));
   for (uint32_t m = 0; m < 3; ++m) ctx->join_bps[m] = join_blocks_per_sm(m);
-  // persistent small buffers
-  CU(cudaMalloc(&ctx->d_ctl, sizeof(JControl)));
-  CU(cudaMalloc(&ctx->d_queue, sizeof(JTask) * TASK_CAP));
-  CU(cudaMalloc(&ctx->d_qends, sizeof(JQueueEnds) * QUEUE_SUBQ));
-  CU(cudaMalloc(&ctx->d_err, sizeof(uint32_t) * 4));
-  CU(cudaHostAlloc(&ctx->h_small, H_SMALL_BYTES, cudaHostAllocDefault));
-  ctx->device_bytes += sizeof(JControl) + sizeof(JTask) * TASK_CAP + sizeof(JQueueEnds) * QUEUE_SUBQ + 16;
+  CU(cudaEventCreate(&ctx->ev_ref));
+  ST(exec_init(ctx));
   *out = c.release();
+  return GEM_OK;
+}
+
+// Serving lane over root's resident graph: everything a wave runs on of its
+// own (stream, events, arena, control block, task queue, pinned staging),
+// the graph and its derived indexes borrowed, the tuned schedules copied.
+gem_status lane_create(gem_ctx *root, uint64_t budget, gem_ctx **out) {
+  *out = nullptr;
+  if (!root->loaded || root->opts.ooc) return GEM_ERR_STATE;
+  std::unique_ptr<gem_ctx> c(new gem_ctx());
+  gem_ctx *ctx = c.get();
+  ctx->opts = root->opts;
+  ctx->sms = root->sms;
+  for (uint32_t m = 0; m < 3; ++m) ctx->join_bps[m] = root->join_bps[m];
+  ctx->budget = budget;
+  ctx->loaded = true;
+  ctx->borrowed_graph = true;
+  ctx->g = root->g;
+  ctx->vnh_off = root->vnh_off;
+  ctx->vnh_slots = root->vnh_slots;
+  ctx->label_freq = root->label_freq;
+  ctx->label_arcs = root->label_arcs;
+  ctx->label_pair_arcs = root->label_pair_arcs;
+  for (int b = 0; b < 6; ++b) ctx->tune[b] = root->tune[b];
+  ctx->donate_max_level = root->donate_max_level;
+  ctx->closed_form_suffix = root->closed_form_suffix;
+  ctx->wave_max_rows = root->wave_max_rows;
+  ctx->ev_ref = root->ev_ref;
+  ctx->ev_ref_recorded = root->ev_ref_recorded;
+  c.release();
+  gem_status st = cudaSetDevice(ctx->opts.device) == cudaSuccess ? exec_init(ctx) : GEM_ERR_CUDA;
+  if (st != GEM_OK) {
+    cudaGetLastError();
+    gem_ctx_destroy(ctx);  // its own resources only: the graph is borrowed
+    return st;
+  }
+  ctx->budget += ctx->device_bytes;
+  *out = ctx;
   return GEM_OK;
 }
 
@@ -198,7 +243,8 @@ extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
   cudaSetDevice(ctx->opts.device);
   cudaStreamSynchronize(ctx->s);
   ctx->arena.release(ctx);
-  free_graph(ctx);
+  if (!ctx->borrowed_graph) free_graph(ctx);
+  if (ctx->ev_ref && !ctx->borrowed_graph) cudaEventDestroy(ctx->ev_ref);
   destroy_join_graph(ctx->jgraph);
   if (ctx->d_ctl) cudaFree(ctx->d_ctl);
   if (ctx->d_queue) cudaFree(ctx->d_queue);
@@ -410,11 +456,31 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   }
   ctx->g = g;
   ctx->loaded = true;
+  CU(cudaEventRecord(ctx->ev_ref, ctx->s));
+  ctx->ev_ref_recorded = true;
   ctx->label_freq.assign(L, 0);
   ctx->label_arcs.assign(L, 0);
   for (uint32_t v = 0; v < nv; ++v) {
     ctx->label_freq[hg->lab[v]]++;
     ctx->label_arcs[hg->lab[v]] += hg->off[v + 1] - hg->off[v];
+  }
+  // arcs per (source label, target label): the largest any edge table between
+  // vertices of those labels can be (bounds the serving admission estimate)
+  ctx->label_pair_arcs.clear();
+  if (L && L <= NLC_MAX_LABELS) {
+    std::vector<uint64_t> pa((size_t)L * L, 0);
+#pragma omp parallel
+    {
+      std::vector<uint64_t> mine((size_t)L * L, 0);
+#pragma omp for schedule(dynamic, 4096) nowait
+      for (int64_t v = 0; v < (int64_t)nv; ++v) {
+        uint64_t *row = mine.data() + (size_t)hg->lab[v] * L;
+        for (uint64_t i = hg->off[v]; i < hg->off[v + 1]; ++i) row[hg->lab[hg->nbr[i]]]++;
+      }
+#pragma omp critical
+      for (size_t i = 0; i < pa.size(); ++i) pa[i] += mine[i];
+    }
+    ctx->label_pair_arcs.swap(pa);
   }
   return GEM_OK;
 }
@@ -992,16 +1058,29 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
     }
     return GEM_OK;
   };
+  CU(cudaEventRecord(ctx->ev[8], ctx->s));
   ST(table_pass(false));
+  CU(cudaEventRecord(ctx->ev[9], ctx->s));
   launch_scan(d_mask, SCAN_POPC_U32, tiles, d_vp, d_tmp2, ctx->s);
-  uint64_t nvals = 0;
-  CU(d2h_sync(ctx, &nvals, d_vp + tiles, 8));
+  // every table's first value position and the total (table sizes order the
+  // wave's queries by estimated join work)
+  uint64_t *d_ebase;
+  ST(aalloc(ctx, edge.size() + 1, &d_ebase));
+  launch_edge_value_bases(d_edge, (uint32_t)edge.size(), d_vp, tiles, d_ebase, ctx->s);
+  std::vector<uint64_t> ebase(edge.size() + 1);
+  CU(d2h_sync(ctx, ebase.data(), d_ebase, 8 * ebase.size()));
   CU(cudaGetLastError());
+  const uint64_t nvals = ebase[edge.size()];
+  w.edge_vals.resize(edge.size());
+  for (size_t e = 0; e < edge.size(); ++e) w.edge_vals[e] = ebase[e + 1] - ebase[e];
   ST(aalloc(ctx, nvals ? nvals : 1, &w.d_values));
   w.d_vkey = nullptr;
   if (key_map) ST(aalloc(ctx, nvals ? nvals : 1, &w.d_vkey));
   launch_table_offsets(d_src, d_edge, (uint32_t)edge.size(), d_tp, d_vp, offs, ctx->s);
+  CU(cudaEventRecord(ctx->ev[10], ctx->s));
   ST(table_pass(true));
+  CU(cudaEventRecord(ctx->ev[11], ctx->s));
+  w.table_passes = true;
   CU(cudaGetLastError());
   w.edges = edge;
   w.table_values = nvals;
@@ -1083,6 +1162,32 @@ static gem_status wave_index(gem_ctx *ctx, Wave &w) {
   return GEM_OK;
 }
 
+// Estimated join work of query qi (partial embeddings the DFS visits), from
+// the sizes of its tables: level k multiplies the matches of the levels
+// before it by the average length of its shortest backward list, times, per
+// further backward list, the chance that a candidate of u_k is in it
+// (average length / |C(u_k)|); a closed-form suffix adds its levels' work
+// per prefix match.
+static double join_cost(const Wave &w, size_t qi) {
+  const Plan &p = w.plan[qi];
+  double est = (double)w.cnt[w.row_of[qi][p.order[0]]], cost = est;
+  for (uint32_t k = 1; k < p.n_enum; ++k) {
+    const double ck = std::max(1.0, (double)w.cnt[w.row_of[qi][p.order[k]]]);
+    double best = 1e300, sel = 1.0;
+    for (uint32_t j : p.back[k]) {
+      const uint32_t ei = w.edge_of[qi][j * QV + k];
+      if (ei >= w.edge_vals.size()) continue;
+      const double keys = std::max(1.0, (double)w.cnt[w.row_of[qi][p.order[j]]]);
+      const double avg = (double)w.edge_vals[ei] / keys;
+      sel *= std::min(1.0, avg / ck);
+      best = std::min(best, avg);
+    }
+    if (best < 1e300) est *= best * std::max(sel, 1e-300) / std::min(1.0, best / ck);
+    cost += est;
+  }
+  return cost + est * (double)(p.n - p.n_enum);
+}
+
 static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, uint64_t emb_cap) {
   std::vector<JQuery> jq;
   std::vector<JBack> jb;
@@ -1091,8 +1196,19 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   uint64_t lp_roots = 0;
   w.jq_index.assign(w.q.size(), UINT32_MAX);
   uint64_t roots = 0;
-  for (size_t qi = 0; qi < w.q.size(); ++qi) {
-    if (!w.active[qi]) continue;
+  // Queries take the grid's warps in order of estimated work, cheapest
+  // first: under a time cap the queries that can finish do so before the
+  // expensive ones take the warps, and a wave's result for a query does not
+  // depend on the order.
+  std::vector<size_t> order;
+  std::vector<double> cost(w.q.size(), 0.0);
+  for (size_t qi = 0; qi < w.q.size(); ++qi)
+    if (w.active[qi]) {
+      order.push_back(qi);
+      cost[qi] = join_cost(w, qi);
+    }
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cost[x] < cost[y]; });
+  for (const size_t qi : order) {
     const Plan &p = w.plan[qi];
     JQuery J;
     std::memset(&J, 0, sizeof J);
@@ -1227,6 +1343,7 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   a.n_terms = (uint32_t)terms.size();
   int bps = ctx->join_bps[mode];
   if (tu.blocks_per_sm && (int)tu.blocks_per_sm < bps) bps = (int)tu.blocks_per_sm;
+  bps = std::max(1, bps / (int)std::max(1u, ctx->join_grid_div));
   CU(cudaEventRecord(ctx->ev[6], ctx->s));
   CU(launch_join_graph(ctx->jgraph, a, cap_ms * 1000000ull, (uint32_t)(ctx->sms * bps), ctx->s));
   CU(cudaEventRecord(ctx->ev[7], ctx->s));
@@ -1345,6 +1462,15 @@ gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_
   w.tables_ms = ev_ms(ctx->ev[1], ctx->ev[2]);
   w.index_ms = ev_ms(ctx->ev[2], ctx->ev[3]);
   w.total_ms = ev_ms(ctx->ev[0], ctx->ev[4]);
+  if (w.table_passes) {
+    w.table_pass_ms[0] = ev_ms(ctx->ev[8], ctx->ev[9]);
+    w.table_pass_ms[1] = ev_ms(ctx->ev[10], ctx->ev[11]);
+  }
+  if (ctx->ev_ref_recorded) {
+    w.t_begin_ms = ev_ms(ctx->ev_ref, ctx->ev[0]);
+    w.t_end_ms = ev_ms(ctx->ev_ref, ctx->ev[4]);
+  }
+  w.arena_bytes = ctx->arena.in_use;
   w.launches = (uint32_t)(g_launches.load() - launches0);
   return GEM_OK;
 }
@@ -1378,6 +1504,11 @@ void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r) {
   r->ms[GEM_PH_TOTAL] = w.total_ms;
   r->ms[GEM_PH_HOST] = (float)w.plan_ms;
   r->launches = w.launches;
+  r->table_pass_ms[0] = w.table_pass_ms[0];
+  r->table_pass_ms[1] = w.table_pass_ms[1];
+  r->t_begin_ms = w.t_begin_ms;
+  r->t_end_ms = w.t_end_ms;
+  r->arena_bytes = w.arena_bytes;
   (void)ctx;
 }
 

@@ -71,6 +71,7 @@ struct Wave {
   std::vector<uint64_t> c_base;   // list start per row
   uint64_t cand_total = 0;
   std::vector<gem::TabEdge> edges;
+  std::vector<uint64_t> edge_vals;  // values per table (edges[e])
   uint32_t *d_values = nullptr;
   uint64_t table_values = 0, table_tiles = 0;
   const gem::CuckooTable *ck_tabs = nullptr;
@@ -80,6 +81,10 @@ struct Wave {
   uint64_t join_nodes = 0, join_scanned = 0, join_probes = 0, emb_written = 0;
   uint32_t join_err = 0;
   float filter_ms = 0, tables_ms = 0, index_ms = 0, join_ms = 0, total_ms = 0;
+  float table_pass_ms[2] = {0, 0};  // the table kernels' count and write passes
+  float t_begin_ms = 0, t_end_ms = 0;  // first and last event of the wave against the context's ev_ref
+  uint64_t arena_bytes = 0;            // arena bytes the wave used
+  bool table_passes = false;        // the passes ran (their events were recorded)
   double plan_ms = 0;
   uint64_t bytes_filter = 0, bytes_tables = 0, bytes_index = 0, bytes_join = 0;
   uint32_t launches = 0;
@@ -106,7 +111,7 @@ constexpr size_t H_SMALL_BYTES = 4u << 20;  // pinned staging per context
 struct gem_ctx {
   gem_opts opts{};
   cudaStream_t s = nullptr;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[12] = {};
   int sms = 148;
   int join_bps[3] = {1, 1, 1};
   uint64_t budget = 0, device_bytes = 0;
@@ -134,6 +139,7 @@ struct gem_ctx {
   uint64_t graph_bytes = 0;
   std::vector<uint64_t> label_freq;  // vertices per label
   std::vector<uint64_t> label_arcs;  // sum of degrees per label
+  std::vector<uint64_t> label_pair_arcs;  // [s * nlabels + t]: arcs from label-s to label-t vertices (<= 64 labels)
   Server *server = nullptr;          // serving thread (gem_submit / gem_poll)
   // scratch
   Arena arena;
@@ -150,7 +156,18 @@ struct gem_ctx {
   uint32_t donate_max_level = 30;
   bool closed_form_suffix = true;
   uint32_t wave_max_rows = 4096;
+  uint32_t join_grid_div = 1;        // the join grid takes blocks_per_sm / this per SM (serving lanes: 2)
+  // device timeline: waves report their first and last event against ev_ref
+  // (recorded when the graph is loaded; serving lanes share their root's)
+  cudaEvent_t ev_ref = nullptr;
+  bool ev_ref_recorded = false;
+  bool borrowed_graph = false;       // a serving lane: the graph belongs to another context
 };
+
+// A serving lane: a context with its own stream, events, arena, control
+// block and task queue that borrows `root`'s resident graph (in-core only),
+// so that waves of two lanes run on the device at the same time.
+gem_status lane_create(gem_ctx *root, uint64_t budget, gem_ctx **out);
 
 gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_t *emb_dev, uint64_t emb_cap);
 void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r);

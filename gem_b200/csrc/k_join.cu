@@ -84,6 +84,27 @@ __device__ __forceinline__ bool inb(const JoinArgs &a, uint32_t site, uint64_t i
   return false;
 }
 
+// Warp-uniform: true once the error word is set or the time cap has passed
+// (the cap then sets the error word, so every warp stops at its next look).
+__device__ __forceinline__ bool stop_now(const JoinArgs &a, uint64_t deadline) {
+  int stop = 0;
+  if (lane_id() == 0) {
+    if (ld_vol(&a.ctl->err) != DERR_NONE) {
+      stop = 1;
+    } else if (globaltimer_ns() > deadline) {
+      set_error(&a.ctl->err, DERR_TIMEOUT);
+      stop = 1;
+    }
+  }
+  return __shfl_sync(FULL, stop, 0) != 0;
+}
+
+// Warp-uniform: the error word is set (a count cut short by the cap may
+// have been added since the last look).
+__device__ __forceinline__ bool err_set(const JoinArgs &a) {
+  return __shfl_sync(FULL, lane_id() == 0 ? (int)(ld_vol(&a.ctl->err) != DERR_NONE) : 0, 0) != 0;
+}
+
 // Range [lo, hi) of table entry b at key position kidx (checked).
 __device__ __forceinline__ void table_range(const JoinArgs &a, const JBack *b, uint32_t kidx, uint64_t &lo,
                                             uint64_t &hi) {
@@ -856,13 +877,7 @@ __device__ __forceinline__ bool flat_lane_chunk(const JoinArgs &a, const LaneCtx
   // ---- stage 2: blocks dealt round-robin; partial counts summed per job
   uint32_t cur_j = 0, cur_c = 0;
   for (uint32_t base = 0; base < total; base += 32) {
-    if (((base >> 5) & 63u) == 63u) {
-      const int late = __shfl_sync(FULL, lane == 0 ? (int)(globaltimer_ns() > x.deadline) : 0, 0);
-      if (late) {
-        if (lane == 0) set_error(&a.ctl->err, DERR_TIMEOUT);
-        break;
-      }
-    }
+    if (((base >> 5) & 15u) == 15u && stop_now(a, x.deadline)) break;
     const uint32_t bid = base + lane;
     if (bid < total) {
       uint32_t lo = cur_j, hi = njobs;  // last job whose start <= bid (jobs only move forward)
@@ -1030,15 +1045,10 @@ __device__ uint64_t warp_subset_count(const JoinArgs &a, const LaneCtx &x, uint3
   uint64_t cnt = 0;
   uint32_t step = 0;
   for (uint64_t cp = s_lo; cp < s_hi; cp += 32) {
-    // long merges look at the time cap every 64 steps; past it, the partial
-    // count is dropped with the query (the error word marks it incomplete)
-    if ((++step & 63u) == 0) {
-      const int late = __shfl_sync(FULL, lane == 0 ? (int)(globaltimer_ns() > x.deadline) : 0, 0);
-      if (late) {
-        if (lane == 0) set_error(&a.ctl->err, DERR_TIMEOUT);
-        break;
-      }
-    }
+    // merges look at the time cap and the error word first and every 16
+    // steps; past the cap the partial count is dropped with the query (the
+    // error word marks it incomplete wherever the count is retired)
+    if ((step++ & 15u) == 0 && stop_now(a, x.deadline)) break;
     const uint64_t e = cp + lane;
     bool ok = e < s_hi;
     const uint32_t v = !ok ? 0xFFFFFFFFu
@@ -1448,6 +1458,17 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
         if (lane == 0 && k) atomicAdd(&a.out[qh].count, (unsigned long long)k);
       }
       if (lane == 0) st.nodes += (a.lp_roots - base) < 32 ? (a.lp_roots - base) : 32;
+      if (err_set(a)) {
+        // a count of this chunk may have been cut short: its queries and every
+        // unclaimed root of the pool are incomplete
+        if (lane == 0) {
+          const unsigned long long r0 = atomicExch(&ctl->lp_next, (unsigned long long)a.lp_roots);
+          const unsigned long long from = base < r0 ? base : r0;
+          for (uint32_t k = find_query(a.lp_prefix, a.lp_nq, from); k < a.lp_nq; ++k)
+            atomicOr(&a.out[a.lp_query[k]].pad[0], 1ull);
+        }
+        break;
+      }
     }
   }
 
@@ -1539,6 +1560,17 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
       if (lane == 0) {
         if (cnt) atomicAdd(&a.out[q].count, (unsigned long long)cnt);
         st.nodes += __popc(m);
+      }
+      if (err_set(a)) {
+        // this chunk's count may have been cut short: its query and every
+        // unclaimed chunk's are incomplete
+        if (lane == 0) {
+          const unsigned long long r0 = atomicExch(&ctl->lp2_next, (unsigned long long)total);
+          const unsigned long long from = base < r0 ? base : r0;
+          for (uint32_t k = find_query(a.lp2_prefix, a.lp2_nq, from); k < a.lp2_nq; ++k)
+            atomicOr(&a.out[a.lp2_query[k]].pad[0], 1ull);
+        }
+        break;
       }
     }
   }
@@ -1901,7 +1933,11 @@ __global__ void __launch_bounds__(256, 2) join_kernel(JoinArgs a) {
       th += __shfl_xor_sync(FULL, th, d);
     }
     const bool release = abort || !from_root || rb_cur >= rb_end;
+    // a count of this task may have been cut short by the cap since the last
+    // look: with the error word set, its query is incomplete
+    const bool cut = !abort && err_set(a);
     if (lane == 0) {
+      if (cut) atomicOr(&a.out[q].pad[0], 1ull);
       if (abort) {
         abandon(a, q);
         if (from_root && rb_cur < rb_end) {

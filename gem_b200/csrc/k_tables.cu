@@ -279,6 +279,18 @@ void launch_tile_scatter(const uint32_t *tpart, uint64_t ntile, uint32_t nparts,
   }
 }
 
+__global__ void edge_value_bases_kernel(const TabEdge *__restrict__ edges, uint32_t nedge,
+                                       const uint64_t *__restrict__ vp, uint64_t tiles, uint64_t *__restrict__ out) {
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e <= nedge; e += gridDim.x * blockDim.x)
+    out[e] = vp[e < nedge ? edges[e].tile_base : tiles];
+}
+
+void launch_edge_value_bases(const TabEdge *d_edge, uint32_t nedge, const uint64_t *vp, uint64_t tiles,
+                             uint64_t *out, cudaStream_t s) {
+  count_launch();
+  edge_value_bases_kernel<<<(nedge + 256) / 256, 256, 0, s>>>(d_edge, nedge, vp, tiles, out);
+}
+
 __device__ __forceinline__ uint32_t find_edge_off(const TabEdge *__restrict__ e, uint32_t ne, uint64_t i) {
   uint32_t lo = 0, hi = ne;
   while (hi - lo > 1) {

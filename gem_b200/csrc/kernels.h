@@ -141,6 +141,11 @@ void launch_tile_scatter(const uint32_t *tpart, uint64_t ntile, uint32_t nparts,
 // out[i] = tp[d_src[i].key_base] for i < nsrc, out[nsrc] = tp[nkeys].
 void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp,
                               uint64_t *out, cudaStream_t s);
+// out[e] = vp[edges[e].tile_base] for e < nedge and out[nedge] = vp[tiles]:
+// the first value position of every table (and the total), so that table e
+// holds out[e + 1] - out[e] values.
+void launch_edge_value_bases(const TabEdge *d_edge, uint32_t nedge, const uint64_t *vp, uint64_t tiles,
+                             uint64_t *out, cudaStream_t s);
 void launch_table_offsets(const TabSource *d_src, const TabEdge *d_edge, uint32_t nedge,
                           const uint64_t *tp, const uint64_t *vp, uint64_t total_offsets,
                           cudaStream_t s);

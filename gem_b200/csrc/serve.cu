@@ -1,14 +1,20 @@
 // Serving: continuous batching with memory-based admission.
 //
 // No counterpart in the reference (one query per process).  gem_submit
-// admits a query when its estimated device bytes fit the admission budget,
-// and a server thread owned by the context turns everything admitted so far
-// into one wave (shared filter/table launches and one persistent join launch).
-// Requests that arrive while a wave is on the GPU are admitted as budget
-// frees and run in the next wave, together with everything else waiting.
-// Results are identical to gem_query_run's: every query of a wave has its own
-// plan, tables and counters.  While the server runs, only gem_submit and
-// gem_poll may be used on the context (other calls return GEM_ERR_STATE).
+// admits a query when its estimated device bytes fit the admission budget.
+// Worker threads, one per serving lane, each turn everything admitted and
+// not yet taken into a wave (shared filter/table launches and one persistent
+// join launch) on their lane.  An in-core context serves on two lanes: the
+// context itself and a lane context that borrows its resident graph (its own
+// stream, arena, control block and task queue).  While one lane's wave is on
+// the GPU the other lane takes the requests that arrived meanwhile, so their
+// work overlaps on the device; each lane's join grid takes half of the SMs'
+// blocks so that two joins fit side by side.  An out-of-core context serves
+// on one lane (its partition staging buffers are not shared).  Results are
+// identical to gem_query_run's: every query of a wave has its own plan,
+// tables and counters.  While the server runs, only gem_submit and gem_poll
+// may be used on the context (other calls return GEM_ERR_STATE).
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -24,7 +30,9 @@ using namespace gem;
 struct Server {
   std::mutex mu;
   std::condition_variable cv;
-  std::thread th;
+  std::vector<std::thread> th;
+  std::vector<gem_ctx *> lanes;  // lanes[0] is the context itself
+  uint64_t saved_budget = 0;     // the context's device budget before serving split it
   bool stop = false;
   struct Req {
     uint64_t ticket;
@@ -39,33 +47,62 @@ struct Server {
   uint64_t waves = 0;
 };
 
-// Device bytes a query is expected to need: one rank-bitmap row per query
-// vertex, its candidate list (bounded by the label's frequency) and, per
-// query edge, the label-restricted arcs of the source candidates.
+// Upper bound of the device scratch one query's wave can take, from the
+// graph's label statistics alone (the plan is not known at admission): per
+// query vertex its rank-bitmap row with the row scan, its candidate list
+// (at most the label's vertices) and, as an edge-table source, its keys'
+// tile bookkeeping (tiles <= vertices + arcs / 32 of the label) and an
+// index; per query edge the larger direction's table: per-tile masks and
+// positions, offsets per key, values and key positions (at most the arcs
+// between the two labels); per query the join's descriptors.
 static uint64_t estimate_bytes(const gem_ctx *ctx, const HostQuery &q) {
   const uint64_t nwords = (ctx->g.nv + 31) / 32;
+  const size_t L = ctx->label_freq.size();
+  auto freq = [&](uint32_t l) -> uint64_t { return l < L ? ctx->label_freq[l] : 0; };
+  auto tiles = [&](uint32_t l) -> uint64_t { return l < L ? ctx->label_freq[l] + ctx->label_arcs[l] / 32 + 1 : 1; };
+  auto pair_arcs = [&](uint32_t s, uint32_t t) -> uint64_t {
+    if (s >= L || t >= L) return 0;
+    return ctx->label_pair_arcs.empty() ? ctx->label_arcs[s] : ctx->label_pair_arcs[(size_t)s * L + t];
+  };
+  auto al = [](uint64_t b) -> uint64_t { return (b + 255) & ~(uint64_t)255; };
   uint64_t b = 0;
   for (uint32_t u = 0; u < q.nv; ++u) {
-    const uint64_t f = q.lab[u] < ctx->label_freq.size() ? ctx->label_freq[q.lab[u]] : 0;
-    b += nwords * 8 * 3 + f * 4;
+    const uint64_t f = freq(q.lab[u]), t = tiles(q.lab[u]);
+    b += al(8 * nwords) + al(8 * (nwords + 1)) + al(8 * (nwords / 2048 + 2)) + al(4 * f + 4);  // row, scan, list
+    b += al(4 * f) + al(8 * (f + 1)) + al(8 * (f / 2048 + 2)) + 2 * al(4 * t);  // source: key tiles, tile map
+    b += al(16 * f + 1024);                                                    // index
   }
-  const double nv = ctx->g.nv ? (double)ctx->g.nv : 1.0;
   for (uint32_t e = 0; e < q.ne; ++e) {
-    const uint32_t a = q.edges[2 * e], c = q.edges[2 * e + 1];
+    uint64_t most = 0;
     for (int dir = 0; dir < 2; ++dir) {
-      const uint32_t s = dir ? c : a, t = dir ? a : c;
-      const double arcs = q.lab[s] < ctx->label_arcs.size() ? (double)ctx->label_arcs[q.lab[s]] : 0.0;
-      const double pt = q.lab[t] < ctx->label_freq.size() ? (double)ctx->label_freq[q.lab[t]] / nv : 0.0;
-      b += (uint64_t)(arcs * (4.0 / 32 + 8.0 / 32 + pt * 4.0)) + 16;
+      const uint32_t s = q.lab[q.edges[2 * e + dir]], t = q.lab[q.edges[2 * e + 1 - dir]];
+      const uint64_t ts = tiles(s), f = freq(s), v = pair_arcs(s, t);
+      most = std::max<uint64_t>(most, al(4 * ts) + al(8 * (ts + 1)) + al(8 * (ts / 2048 + 2)) + al(8 * (f + 1)) +
+                                2 * al(4 * v + 4));
     }
+    b += most;
   }
-  return b + (1u << 20);
+  return b + (64ull << 10) * (q.nv + 1) + (1ull << 20);
 }
 
-static void server_loop(gem_ctx *ctx) {
-  Server &S = *ctx->server;
+extern "C" gem_status gem_estimate_bytes(const gem_ctx *ctx, const gem_query *q, uint64_t *bytes) {
+  if (!ctx || !q || !bytes) return GEM_ERR_ARG;
+  if (!ctx->loaded) return GEM_ERR_STATE;
+  HostQuery hq;
+  std::string err;
+  const gem_status st = make_host_query(q, hq, err);
+  if (st != GEM_OK) return st;
+  *bytes = estimate_bytes(ctx, hq);
+  return GEM_OK;
+}
+
+// One lane's worker: takes the longest run of pending requests of one mode
+// that fits a wave, runs it on the lane, publishes the results.
+static void server_loop(gem_ctx *root, gem_ctx *lane) {
+  Server &S = *root->server;
   for (;;) {
     std::vector<Server::Req> batch;
+    uint64_t wave_no = 0;
     {
       std::unique_lock<std::mutex> lk(S.mu);
       S.cv.wait(lk, [&] { return S.stop || !S.pending.empty(); });
@@ -73,22 +110,27 @@ static void server_loop(gem_ctx *ctx) {
       uint32_t rows = 0;
       const int mode = S.pending.front().mode;
       while (!S.pending.empty() && S.pending.front().mode == mode &&
-             (batch.empty() || rows + S.pending.front().q.nv <= ctx->wave_max_rows)) {
+             (batch.empty() || rows + S.pending.front().q.nv <= lane->wave_max_rows)) {
         rows += S.pending.front().q.nv;
         batch.push_back(std::move(S.pending.front()));
         S.pending.pop_front();
       }
+      wave_no = S.waves++;
     }
     Wave w;
     for (auto &r : batch) w.q.push_back(r.q);
-    ctx->arena.reset();
-    gem_status st = run_wave(ctx, w, 0, batch[0].mode, nullptr, 0);
+    lane->arena.reset();
+    gem_status st = run_wave(lane, w, 0, batch[0].mode, nullptr, 0);
+    if (st != GEM_OK) {
+      cudaStreamSynchronize(lane->s);
+      cudaGetLastError();
+    }
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < batch.size(); ++i) {
       gem_result r;
       if (st == GEM_OK) {
-        wave_result(ctx, w, i, &r);
-        r.wave = (uint32_t)S.waves;
+        wave_result(lane, w, i, &r);
+        r.wave = (uint32_t)wave_no;
       } else {
         std::memset(&r, 0, sizeof r);
         r.status = st;
@@ -96,20 +138,49 @@ static void server_loop(gem_ctx *ctx) {
       S.done[batch[i].ticket] = r;
       S.in_flight -= batch[i].est;
     }
-    ++S.waves;
   }
 }
 
 void server_shutdown(gem_ctx *ctx) {
   if (!ctx->server) return;
+  Server *S = ctx->server;
   {
-    std::lock_guard<std::mutex> lk(ctx->server->mu);
-    ctx->server->stop = true;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
   }
-  ctx->server->cv.notify_all();
-  if (ctx->server->th.joinable()) ctx->server->th.join();
-  delete ctx->server;
+  S->cv.notify_all();
+  for (auto &t : S->th)
+    if (t.joinable()) t.join();
+  for (size_t i = 1; i < S->lanes.size(); ++i) gem_ctx_destroy(S->lanes[i]);
+  ctx->join_grid_div = 1;
+  if (S->saved_budget) ctx->budget = S->saved_budget;
+  delete S;
   ctx->server = nullptr;
+}
+
+// Starts the server: a second lane for in-core contexts (the remaining
+// device budget split between the two), one worker thread per lane.
+static gem_status server_start(gem_ctx *ctx) {
+  Server *S = new Server();
+  ctx->server = S;
+  const uint64_t cap = ctx->opts.admit_gb ? (uint64_t)ctx->opts.admit_gb << 30 : 120ull << 30;
+  const uint64_t room = ctx->budget > ctx->device_bytes ? ctx->budget - ctx->device_bytes : 0;
+  S->budget = cap < room ? cap : room;
+  S->lanes.push_back(ctx);
+  if (!ctx->opts.ooc) {
+    gem_ctx *lane = nullptr;
+    if (lane_create(ctx, room / 2, &lane) == GEM_OK) {
+      S->saved_budget = ctx->budget;
+      ctx->budget = ctx->device_bytes + room / 2;
+      ctx->join_grid_div = 2;
+      lane->join_grid_div = 2;
+      S->lanes.push_back(lane);
+    } else {
+      cudaGetLastError();
+    }
+  }
+  for (gem_ctx *lane : S->lanes) S->th.emplace_back(server_loop, ctx, lane);
+  return GEM_OK;
 }
 
 extern "C" gem_status gem_submit(gem_ctx *ctx, const gem_query *q, int mode, uint64_t *ticket) {
@@ -121,11 +192,8 @@ extern "C" gem_status gem_submit(gem_ctx *ctx, const gem_query *q, int mode, uin
   gem_status st = make_host_query(q, hq, err);
   if (st != GEM_OK) return st;
   if (!ctx->server) {
-    ctx->server = new Server();
-    const uint64_t cap = ctx->opts.admit_gb ? (uint64_t)ctx->opts.admit_gb << 30 : 120ull << 30;
-    const uint64_t room = ctx->budget > ctx->device_bytes ? ctx->budget - ctx->device_bytes : 0;
-    ctx->server->budget = cap < room ? cap : room;
-    ctx->server->th = std::thread(server_loop, ctx);
+    const gem_status ss = server_start(ctx);
+    if (ss != GEM_OK) return ss;
   }
   Server &S = *ctx->server;
   const uint64_t est = estimate_bytes(ctx, hq);

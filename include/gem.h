@@ -213,6 +213,10 @@ typedef struct gem_result {
   float ms[8];           /* GEM_PH_* (batch: times of the wave that ran this query) */
   uint32_t wave;         /* batch: index of the wave that ran this query */
   uint32_t launches;     /* kernels launched for this query's wave */
+  float table_pass_ms[2]; /* device time of the wave's edge-table count pass and write pass */
+  float t_begin_ms;      /* device timeline of the wave: its first and last event, in ms after */
+  float t_end_ms;        /* an event recorded when the context loaded its graph */
+  uint64_t arena_bytes;  /* device scratch bytes the wave used */
 } gem_result;
 
 /* Run one query end to end on the device (filter -> index -> edge tables ->
@@ -375,6 +379,10 @@ gem_status gem_filter_static(const uint64_t *d_offsets, const uint32_t *d_nbrs,
 /* until gem_ctx_destroy.  Admitted requests run in waves: everything        */
 /* admitted while a wave is on the GPU forms the next wave.                  */
 /* ------------------------------------------------------------------------ */
+/* Device scratch bytes gem_submit reserves for q under the admission budget
+ * (host only, no counterpart in the reference): an upper bound of what a
+ * wave of q alone takes, from the resident graph's label statistics. */
+gem_status gem_estimate_bytes(const gem_ctx *ctx, const gem_query *q, uint64_t *bytes);
 /* Submit a query; returns GEM_ERR_OOM when its estimated device bytes do not
  * fit the admission budget right now (caller retries later). */
 gem_status gem_submit(gem_ctx *ctx, const gem_query *q, int mode,

@@ -1,0 +1,74 @@
+"""The benchmark's workloads on the GPU against the CPU oracle, bit-exact.
+
+* Configuration 1 exactly as bench.py builds it (R-MAT scale 16, edge factor
+  8, 8 uniform labels, the 100 random-walk 4-vertex queries): every query's
+  count and embedding hash from one batch, and every plain count.
+* The configuration-3 mix (query sizes 4 to 32, alternately sparse and
+  dense) on a scale-10 graph with 16 Zipf labels, where the oracle finishes
+  most of them: one batch in hash mode and one in count mode (closed-form
+  suffixes), every query the oracle finishes compared.
+* A batch under a time cap: the cheap queries of the wave finish exactly
+  while an expensive one runs into the cap.
+"""
+import numpy as np
+import pytest
+
+import bench
+import gem_b200 as gem
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def test_config1_pool_matches_oracle():
+    g, _ = bench.make_graph(gem, "rmat16")
+    pool = bench.config1_pool(gem, g)
+    assert len(pool) == 100
+    with gem.Context(time_cap_ms=60000) as c:
+        c.load_graph(g)
+        st, rh = c.batch(pool, mode=gem.MODE_HASH)
+        assert st == 0
+        st, rc = c.batch(pool)
+        assert st == 0
+        plain = [c.run(q)["count"] for q in pool]
+    for i, q in enumerate(pool):
+        cnt, h, ok = oracle.count(g, q, want_hash=True)
+        assert ok
+        assert rh[i]["status"] == "OK" and rh[i]["count"] == cnt and rh[i]["emb_hash"] == h, i
+        assert rc[i]["status"] == "OK" and rc[i]["count"] == cnt, i
+        assert plain[i] == cnt, i
+
+
+def test_mixed_size_batch_matches_oracle():
+    g = gem.HostGraph.rmat(10, 8, seed=0x47454D0A).set_labels(16, 1.0, seed=0x47454D0A ^ 0x4C)
+    pool = bench.mix_pool(gem, g, 120)
+    assert {q.nv for q in pool} == set(bench.MIX_SIZES)
+    with gem.Context(time_cap_ms=60000) as c:
+        c.load_graph(g)
+        st, rh = c.batch(pool, mode=gem.MODE_HASH)
+        st2, rc = c.batch(pool)
+    checked, sizes = 0, set()
+    for i, q in enumerate(pool):
+        cnt, h, ok = oracle.count(g, q, want_hash=True, work_cap=100_000_000)
+        if not ok:
+            continue
+        checked += 1
+        sizes.add(q.nv)
+        assert rh[i]["status"] == "OK" and rh[i]["count"] == cnt and rh[i]["emb_hash"] == h, (i, q.nv)
+        assert rc[i]["status"] == "OK" and rc[i]["count"] == cnt, (i, q.nv)
+    assert checked >= 50 and {24, 32} <= sizes, (checked, sizes)
+
+
+def test_capped_wave_keeps_cheap_queries_exact():
+    g, _ = bench.make_graph(gem, "rmat16")
+    cheap = bench.config1_pool(gem, g, 40)
+    heavy = gem.gen_queries(g, 32, gem.SPARSE, 1, seed=0x5EA)
+    qs = heavy + cheap  # the expensive query first in the batch
+    with gem.Context(time_cap_ms=300) as c:
+        c.load_graph(g)
+        assert c.run(heavy[0], raise_on_error=False)["status"] == "ERR_TIMEOUT"
+        _, rs = c.batch(qs)
+    assert rs[0]["status"] == "ERR_TIMEOUT"
+    for q, r in zip(cheap, rs[1:]):
+        cnt, _, ok = oracle.count(g, q, want_hash=False)
+        assert ok and r["status"] == "OK" and r["count"] == cnt
