@@ -297,6 +297,12 @@ def run_gem(args):
         plain = plain_section(ctx, batch_of(args.warmup), res_all[0], args.plain)
     ctx.close()
     sections = {}
+    if rank == 0 and args.workload == "rmat22-mix" and args.serve5_seconds > 0:
+        ref5 = {i: r["count"] for i, r in enumerate(res_all[0]) if r["status"] == "OK"}
+        sections["serving"] = serving_section(gem, local, g, batch_of(args.warmup), ref5,
+                                              [float(x) for x in args.serve5_rates.split(",") if x],
+                                              args.serve5_seconds, args.cap_ms, 120,
+                                              label="the scale-22 mixed-size pool")
     if rank == 0 and args.workload != "rmat16" and args.config1:
         sections["config1"] = config1_section(gem, args, local)
     if rank == 0 and (args.c2_sample > 0 or args.ooc_sample > 0):
@@ -309,6 +315,8 @@ def run_gem(args):
             c2["out_of_core"] = out_of_core_section(gem, args, local, g22)
         sections["rmat22"] = c2
         del g22
+    if rank == 0 and args.ooc26:
+        sections["out_of_core_scale26"] = ooc26_section(gem, args, local)
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -460,7 +468,9 @@ def config1_section(gem, args, local):
         counts = [r["count"] if r["status"] == "OK" else None for r in rs]
     out["parity"] = oracle_parity(g, pool, rs, 0, 120.0)
     if args.serve_seconds > 0:
-        out["serving"] = serving_section(gem, args, local, g, pool, {i: x for i, x in enumerate(counts)})
+        out["serving"] = serving_section(gem, local, g, pool, {i: x for i, x in enumerate(counts)},
+                                         [float(x) for x in args.serve_rates.split(",") if x], args.serve_seconds,
+                                         20000, label="the config-1 pool")
     return out
 
 
@@ -488,25 +498,27 @@ def oracle_parity(g, qs, rs, work_cap, budget_s):
             "oracle_work_cap": work_cap, "seconds": round(time.perf_counter() - t0, 1)}
 
 
-def serving_section(gem, args, local, g, pool, ref_counts):
+def serving_section(gem, local, g, pool, ref_counts, rates, seconds, cap_ms, admit_gb=0, label="the pool"):
     """Continuous batching through gem_submit / gem_poll under Poisson arrivals
     of the pool's queries (cycled), one stream per rate: latency from the
-    arrival to the result being visible, achieved rate, and every count
-    checked against the batched run's."""
+    arrival to the result being visible, achieved rate, exact and capped
+    results, and every exact count checked against the batched run's."""
     import collections
     import random
-    out = {"queries": "the config-1 pool, cycled", "seconds_per_rate": args.serve_seconds, "rates": []}
-    with gem.Context(device=local, time_cap_ms=20000) as c:
+    out = {"queries": f"{label}, cycled", "seconds_per_rate": seconds, "time_cap_ms": cap_ms,
+           "admission_budget_gib": admit_gb or 120, "rates": []}
+    with gem.Context(device=local, time_cap_ms=cap_ms, admit_gb=admit_gb) as c:
         c.load_graph(g)
-        for lam in [float(x) for x in args.serve_rates.split(",") if x]:
+        for lam in rates:
             rng = random.Random(0x5E12 + int(lam))
             arr, t = [], 0.0
             while True:
                 t += rng.expovariate(lam)
-                if t > args.serve_seconds:
+                if t > seconds:
                     break
                 arr.append(t)
             pending, lat, same, busy, i = collections.deque(), [], True, 0, 0
+            exact = capped = checked = 0
             t0 = time.perf_counter()
             while i < len(arr) or pending:
                 now = time.perf_counter() - t0
@@ -524,14 +536,23 @@ def serving_section(gem, args, local, g, pool, ref_counts):
                     if r is None:
                         break
                     lat.append((time.perf_counter() - t0 - ta) * 1e3)
-                    same &= r["status"] == "OK" and r["count"] == ref_counts[qi]
+                    if r["status"] == "OK":
+                        exact += 1
+                        if ref_counts.get(qi) is not None:
+                            checked += 1
+                            same &= r["count"] == ref_counts[qi]
+                    elif r["status"] == "ERR_TIMEOUT":
+                        capped += 1
+                    else:
+                        same = False
                     pending.popleft()
-                if not pending and i < len(arr):
-                    time.sleep(max(0.0, arr[i] - (time.perf_counter() - t0)))
+                if pending or i < len(arr):
+                    time.sleep(0.0002 if pending else max(0.0, arr[i] - (time.perf_counter() - t0)))
             wall = time.perf_counter() - t0
             out["rates"].append({"lambda_qps": lam, "queries": len(lat), "achieved_qps": len(lat) / wall,
-                                 "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99), "counts_equal_batched": same,
-                                 "admission_busy": busy})
+                                 "exact": exact, "capped": capped, "exact_qps": exact / wall,
+                                 "p50_ms": pctl(lat, 50), "p99_ms": pctl(lat, 99),
+                                 "counts_checked": checked, "counts_equal_batched": same, "admission_busy": busy})
     return out
 
 
@@ -599,6 +620,45 @@ def out_of_core_section(gem, args, local, g):
                 m["stats"] = c.ooc_stats()
             out["modes"][name] = m
     out["counts_equal"] = all(v == counts["in_core"] for v in counts.values()) and None not in counts["in_core"]
+    return out
+
+
+def ooc26_section(gem, args, local):
+    """Configuration 4: R-MAT scale 26 (67,108,864 vertices), edge factor 16,
+    32 labels Zipf(1.2), the adjacency in pinned host memory and a 24 GiB
+    device budget.  100 dense 12-vertex random-walk queries in one batch
+    under the per-query cap (waves split to fit the budget), and 4-vertex
+    queries run out of core and in core (the 8.6 GB adjacency also fits the
+    device) with equal counts."""
+    t = time.time()
+    g = gem.HostGraph.rmat(26, 16, seed=0x47454D00 + 26).set_labels(32, 1.2, seed=(0x47454D00 + 26) ^ 0x4C)
+    out = {"workload": "rmat26-ef16-zipf32(1.2)", "graph_gen_s": round(time.time() - t, 1),
+           "adjacency_bytes": 4 * int(g.info()["n_arcs"]), "device_budget_gib": 24, "time_cap_ms": args.ooc26_cap_ms}
+    q12 = gem.gen_queries(g, 12, gem.DENSE, 100, seed=0x51400)
+    q4 = gem.gen_queries(g, 4, gem.ANY, args.ooc26_small, seed=0x51404)
+    with gem.Context(device=local, time_cap_ms=args.ooc26_cap_ms, ooc=True, budget_bytes=24 << 30) as c:
+        t = time.time()
+        c.load_graph(g)
+        out["load_s"] = round(time.time() - t, 1)
+        t = time.time()
+        _, rs = c.batch(q12)
+        ws = waves_of(rs)
+        out["dense12"] = {"queries": len(q12), "wall_s": round(time.time() - t, 2), "waves": len(ws),
+                          "exact": sum(r["status"] == "OK" for r in rs),
+                          "capped": sum(r["status"] == "ERR_TIMEOUT" for r in rs),
+                          "other": sorted({r["status"] for r in rs} - {"OK", "ERR_TIMEOUT"}),
+                          "phase_ms": {k: round(sum(w["ms"][k] for w in ws), 1) for k in ("filter", "tables", "join")}}
+        _, r4 = c.batch(q4)
+        ws4 = waves_of(r4)
+        out["small4_out_of_core"] = {"queries": len(q4), "waves": len(ws4),
+                                     "wave_ms": round(sum(w["ms"]["total"] for w in ws4), 1),
+                                     "exact": sum(r["status"] == "OK" for r in r4)}
+        out["ooc_stats"] = c.ooc_stats()
+    with gem.Context(device=local, time_cap_ms=args.ooc26_cap_ms) as c:
+        c.load_graph(g)
+        _, r4i = c.batch(q4)
+        out["small4_in_core_wave_ms"] = round(sum(w["ms"]["total"] for w in waves_of(r4i)), 1)
+    out["small4_counts_equal"] = [(r["status"], r["count"]) for r in r4] == [(r["status"], r["count"]) for r in r4i]
     return out
 
 
@@ -711,8 +771,15 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="wall-time bound of the CPU legs")
     ap.add_argument("--cpu-parity-cap", type=int, default=200_000_000, help="oracle work cap of the parity check")
     ap.add_argument("--host-path-queries", type=int, default=100)
-    ap.add_argument("--serve-seconds", type=float, default=1.0, help="per arrival rate in the serving section (0 = skip)")
-    ap.add_argument("--serve-rates", default="1000,5000,20000", help="Poisson arrival rates (queries/s)")
+    ap.add_argument("--serve-seconds", type=float, default=1.0,
+                    help="per arrival rate in the config-1 serving section (0 = skip)")
+    ap.add_argument("--serve-rates", default="1000,5000,20000", help="Poisson arrival rates (queries/s), config 1")
+    ap.add_argument("--serve5-seconds", type=float, default=3.0,
+                    help="per arrival rate in the scale-22 serving section (0 = skip)")
+    ap.add_argument("--serve5-rates", default="50,200,1000", help="Poisson arrival rates (queries/s), scale 22")
+    ap.add_argument("--ooc26", type=int, default=0, help="run the scale-26 out-of-core section (minutes)")
+    ap.add_argument("--ooc26-cap-ms", type=int, default=1000)
+    ap.add_argument("--ooc26-small", type=int, default=20, help="4-vertex queries compared in and out of core")
     ap.add_argument("--cpu-work-cap", type=int, default=200_000_000,
                     help="scanned-arc cap per query of the CPU legs and the reference arm")
     ap.add_argument("--ref-sample", type=int, default=4, help="queries per step of the reference arm (--impl reference)")

@@ -70,7 +70,8 @@ class _Opts(C.Structure):
 class _OocStats(C.Structure):
     _fields_ = [("partitions", C.c_uint32), ("reserved0", C.c_uint32), ("max_part_bytes", C.c_uint64),
                 ("waves_streamed", C.c_uint64), ("waves_in_place", C.c_uint64), ("parts_streamed", C.c_uint64),
-                ("bytes_streamed", C.c_uint64)]
+                ("bytes_streamed", C.c_uint64), ("waves_spilled", C.c_uint64), ("bytes_spilled", C.c_uint64),
+                ("resident_bytes", C.c_uint64)]
 
 
 class _Schedule(C.Structure):

@@ -258,6 +258,7 @@ extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
     if (ctx->ev_free[b]) cudaEventDestroy(ctx->ev_free[b]);
   }
   if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
+  if (ctx->spill_host) cudaFreeHost(ctx->spill_host);
   if (ctx->s) cudaStreamDestroy(ctx->s);
   delete ctx;
 }
@@ -349,6 +350,9 @@ extern "C" gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out) 
   if (!ctx || !out) return GEM_ERR_ARG;
   if (ctx->server) return GEM_ERR_STATE;  // the serving thread updates the counters
   *out = ctx->ooc;
+  uint64_t arena = 0;
+  for (const auto &c : ctx->arena.chunks) arena += c.size;
+  out->resident_bytes = ctx->device_bytes - arena;
   return GEM_OK;
 }
 
@@ -420,11 +424,12 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   if (stride) launch_nlc(g, d_nlc, stride, ctx->s);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(ctx->s));
-  // Neighbourhood hash for arc tests in the join: in-core graphs only (it
-  // is read at random), and only when it fits the budget with a quarter of
-  // the remaining budget left for the waves; otherwise the join searches
-  // the sorted adjacency instead.
-  if (!ooc && na) {
+  // Neighbourhood hash for arc tests in the join, when it fits the device
+  // budget with a quarter of the remaining budget left for the waves;
+  // otherwise the join searches the sorted table lists instead.  Out of core
+  // it is built from the mapped adjacency (one read over the host link) and
+  // lives on the device like the tables the join reads.
+  if (na) {
     std::vector<uint64_t> hoff(nv + 1);
     uint64_t n_slots = 0;
     for (uint32_t v = 0; v < nv; ++v) {
@@ -869,6 +874,33 @@ static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   return GEM_OK;
 }
 
+// Mapped pinned host memory of at least `bytes` for spilled table values
+// (kept between waves, grown when needed, within the pinned budget).
+static gem_status spill_buffer(gem_ctx *ctx, uint64_t bytes) {
+  if (ctx->spill_bytes >= bytes) return GEM_OK;
+  const uint64_t pinned_nbr = ctx->pinned_nbr ? 4ull * ctx->g.narcs : 0;
+  if (ctx->opts.pinned_budget_bytes && pinned_nbr + bytes > ctx->opts.pinned_budget_bytes) {
+    ctx->err = "edge tables exceed both the device and the pinned budget";
+    return GEM_ERR_OOM;
+  }
+  if (ctx->spill_host) {
+    CU(cudaStreamSynchronize(ctx->s));
+    cudaFreeHost(ctx->spill_host);
+    ctx->spill_host = ctx->spill_dev = nullptr;
+    ctx->spill_bytes = 0;
+  }
+  const uint64_t sz = std::max<uint64_t>(bytes, 1ull << 30);
+  if (cudaHostAlloc(&ctx->spill_host, sz, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->spill_host = nullptr;
+    ctx->err = "pinned host memory for spilled edge tables unavailable";
+    return GEM_ERR_OOM;
+  }
+  CU(cudaHostGetDevicePointer(&ctx->spill_dev, ctx->spill_host, 0));
+  ctx->spill_bytes = sz;
+  return GEM_OK;
+}
+
 static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   // sources and edges of every active query
   std::vector<TabSource> src;
@@ -1073,9 +1105,25 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   const uint64_t nvals = ebase[edge.size()];
   w.edge_vals.resize(edge.size());
   for (size_t e = 0; e < edge.size(); ++e) w.edge_vals[e] = ebase[e + 1] - ebase[e];
-  ST(aalloc(ctx, nvals ? nvals : 1, &w.d_values));
+  // The values (and key positions) of the wave's tables.  Out of core, a
+  // single query whose tables do not fit the device budget keeps them in
+  // mapped pinned host memory, which the write pass and the join reach over
+  // the host link; a batch wave that does not fit is split instead.
   w.d_vkey = nullptr;
-  if (key_map) ST(aalloc(ctx, nvals ? nvals : 1, &w.d_vkey));
+  const uint64_t nv_alloc = nvals ? nvals : 1;
+  gem_status vst = aalloc(ctx, nv_alloc, &w.d_values);
+  if (vst == GEM_OK && key_map) vst = aalloc(ctx, nv_alloc, &w.d_vkey);
+  if (vst == GEM_ERR_OOM && ctx->opts.ooc && w.q.size() == 1) {
+    const uint64_t need = 4 * nv_alloc * (key_map ? 2 : 1);
+    ST(spill_buffer(ctx, need));
+    w.d_values = static_cast<uint32_t *>(ctx->spill_dev);
+    w.d_vkey = key_map ? w.d_values + nv_alloc : nullptr;
+    ctx->err.clear();
+    ctx->ooc.waves_spilled += 1;
+    ctx->ooc.bytes_spilled += need;
+  } else if (vst != GEM_OK) {
+    return vst;
+  }
   launch_table_offsets(d_src, d_edge, (uint32_t)edge.size(), d_tp, d_vp, offs, ctx->s);
   CU(cudaEventRecord(ctx->ev[10], ctx->s));
   ST(table_pass(true));
@@ -1162,30 +1210,20 @@ static gem_status wave_index(gem_ctx *ctx, Wave &w) {
   return GEM_OK;
 }
 
-// Estimated join work of query qi (partial embeddings the DFS visits), from
-// the sizes of its tables: level k multiplies the matches of the levels
-// before it by the average length of its shortest backward list, times, per
-// further backward list, the chance that a candidate of u_k is in it
-// (average length / |C(u_k)|); a closed-form suffix adds its levels' work
-// per prefix match.
+// Join-work rank of query qi: enumerated levels first (the enumeration's
+// exponent), then query vertices, then the values of the tables it reads.
+// An estimate that multiplies per-level selectivities as if the levels were
+// independent ranks dense queries on skewed graphs as cheap, which they are
+// not; the prefix length is the robust part of the cost.
 static double join_cost(const Wave &w, size_t qi) {
   const Plan &p = w.plan[qi];
-  double est = (double)w.cnt[w.row_of[qi][p.order[0]]], cost = est;
-  for (uint32_t k = 1; k < p.n_enum; ++k) {
-    const double ck = std::max(1.0, (double)w.cnt[w.row_of[qi][p.order[k]]]);
-    double best = 1e300, sel = 1.0;
+  double vals = 0;
+  for (uint32_t k = 1; k < p.n; ++k)
     for (uint32_t j : p.back[k]) {
       const uint32_t ei = w.edge_of[qi][j * QV + k];
-      if (ei >= w.edge_vals.size()) continue;
-      const double keys = std::max(1.0, (double)w.cnt[w.row_of[qi][p.order[j]]]);
-      const double avg = (double)w.edge_vals[ei] / keys;
-      sel *= std::min(1.0, avg / ck);
-      best = std::min(best, avg);
+      if (ei < w.edge_vals.size()) vals += (double)w.edge_vals[ei];
     }
-    if (best < 1e300) est *= best * std::max(sel, 1e-300) / std::min(1.0, best / ck);
-    cost += est;
-  }
-  return cost + est * (double)(p.n - p.n_enum);
+  return ((double)p.n_enum * 64.0 + (double)p.n) * 1e15 + std::min(vals, 1e15 - 1);
 }
 
 static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, uint64_t emb_cap) {
@@ -1361,13 +1399,14 @@ static gem_status wave_join(gem_ctx *ctx, Wave &w, int mode, uint32_t *emb_dev, 
   // Donated tasks still queued when the grid stopped (deadline) were never
   // run: their queries are incomplete.
   if (hc.pending) {
+    // one copy of the queue ends and one of the cells, then the host walks them
     std::vector<JQueueEnds> ends(QUEUE_SUBQ);
+    std::vector<JTask> cells((size_t)QUEUE_SUBQ * QUEUE_SUBQ_CAP);
     CU(cudaMemcpy(ends.data(), ctx->d_qends, sizeof(JQueueEnds) * QUEUE_SUBQ, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(cells.data(), ctx->d_queue, sizeof(JTask) * cells.size(), cudaMemcpyDeviceToHost));
     for (uint32_t sq = 0; sq < QUEUE_SUBQ; ++sq)
       for (unsigned long long t = ends[sq].head; t < ends[sq].tail && t < ends[sq].head + QUEUE_SUBQ_CAP; ++t) {
-        uint32_t qq = 0;
-        CU(cudaMemcpy(&qq, &ctx->d_queue[sq * QUEUE_SUBQ_CAP + (t & (QUEUE_SUBQ_CAP - 1))].q, 4,
-                      cudaMemcpyDeviceToHost));
+        const uint32_t qq = cells[(size_t)sq * QUEUE_SUBQ_CAP + (t & (QUEUE_SUBQ_CAP - 1))].q;
         if (qq < out.size()) out[qq].pad[0] = 1;
       }
   }

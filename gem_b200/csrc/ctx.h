@@ -136,6 +136,9 @@ struct gem_ctx {
   cudaStream_t s_copy = nullptr;
   cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
   gem_ooc_stats ooc{};
+  void *spill_host = nullptr;        // out-of-core: mapped pinned values of tables that exceed the budget
+  void *spill_dev = nullptr;
+  uint64_t spill_bytes = 0;
   uint64_t graph_bytes = 0;
   std::vector<uint64_t> label_freq;  // vertices per label
   std::vector<uint64_t> label_arcs;  // sum of degrees per label

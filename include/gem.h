@@ -169,6 +169,11 @@ typedef struct gem_ooc_stats {
   uint64_t waves_in_place;      /* table builds that read the mapped adjacency */
   uint64_t parts_streamed;      /* partition copies issued (two table passes per build) */
   uint64_t bytes_streamed;      /* bytes those copies moved */
+  uint64_t waves_spilled;       /* single-query waves whose edge-table values exceeded the device
+                                   budget and were kept in mapped pinned host memory */
+  uint64_t bytes_spilled;       /* bytes of those values (and key positions) */
+  uint64_t resident_bytes;      /* device bytes the context holds outside its wave scratch (graph,
+                                   partitions, join queue), counted against its device budget */
 } gem_ooc_stats;
 /* GEM_ERR_STATE while the context serves (gem_submit): its waves update the counters. */
 gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out);

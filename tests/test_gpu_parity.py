@@ -340,6 +340,33 @@ def test_out_of_core_partition_streaming_same_counts(small):
         assert sc["waves_streamed"] == 0 and sc["waves_in_place"] == len(qs) and sc["bytes_streamed"] == 0
 
 
+def test_out_of_core_spills_tables_beyond_the_device_budget(small):
+    """Out of core, a single query whose edge-table values do not fit the
+    device budget keeps them in mapped pinned host memory: same count and
+    hash as in core, and the spill is counted."""
+    qs = [q for q in gem.gen_queries(small, 4, gem.ANY, 8, seed=6300)
+          if oracle.count(small, q, want_hash=False, work_cap=100_000_000)[2]]
+    q = qs[0]
+    with gem.Context(time_cap_ms=30000) as a:
+        a.load_graph(small)
+        ra = a.run(q, mode=gem.MODE_HASH)
+    with gem.Context(time_cap_ms=30000, ooc=True, budget_bytes=2 << 30) as b:
+        b.load_graph(small)
+        rb = b.run(q, mode=gem.MODE_HASH)
+        resident = b.ooc_stats()["resident_bytes"]
+    assert (rb["count"], rb["emb_hash"]) == (ra["count"], ra["emb_hash"])
+    values = 4 * rb["table_total"]
+    assert values >= 1 << 16
+    # a budget that holds everything of the wave but half of the values
+    budget = resident + rb["arena_bytes"] - values // 2
+    with gem.Context(time_cap_ms=30000, ooc=True, budget_bytes=budget) as c:
+        c.load_graph(small)
+        rc = c.run(q, mode=gem.MODE_HASH)
+        st = c.ooc_stats()
+    assert (rc["count"], rc["emb_hash"]) == (ra["count"], ra["emb_hash"])
+    assert st["waves_spilled"] == 1 and st["bytes_spilled"] >= values
+
+
 def test_batch_splits_waves_under_a_tight_budget(small, gctx):
     """A wave whose tables exceed the device budget is split and retried: at the
     smallest budget that runs the batch, every result equals the plain run's and

@@ -43,20 +43,22 @@ def test_mixed_size_batch_matches_oracle():
     g = gem.HostGraph.rmat(10, 8, seed=0x47454D0A).set_labels(16, 1.0, seed=0x47454D0A ^ 0x4C)
     pool = bench.mix_pool(gem, g, 120)
     assert {q.nv for q in pool} == set(bench.MIX_SIZES)
+    # the queries the oracle finishes (under a work cap), all sizes, in one batch
+    checked = []
+    for q in pool:
+        cnt, h, ok = oracle.count(g, q, want_hash=True, work_cap=100_000_000)
+        if ok:
+            checked.append((q, cnt, h))
+    assert len(checked) >= 50 and {24, 32} <= {q.nv for q, _, _ in checked}, len(checked)
+    qs = [q for q, _, _ in checked]
     with gem.Context(time_cap_ms=60000) as c:
         c.load_graph(g)
-        st, rh = c.batch(pool, mode=gem.MODE_HASH)
-        st2, rc = c.batch(pool)
-    checked, sizes = 0, set()
-    for i, q in enumerate(pool):
-        cnt, h, ok = oracle.count(g, q, want_hash=True, work_cap=100_000_000)
-        if not ok:
-            continue
-        checked += 1
-        sizes.add(q.nv)
+        st, rh = c.batch(qs, mode=gem.MODE_HASH)
+        st2, rc = c.batch(qs)
+    assert st == 0 and st2 == 0
+    for i, (q, cnt, h) in enumerate(checked):
         assert rh[i]["status"] == "OK" and rh[i]["count"] == cnt and rh[i]["emb_hash"] == h, (i, q.nv)
         assert rc[i]["status"] == "OK" and rc[i]["count"] == cnt, (i, q.nv)
-    assert checked >= 50 and {24, 32} <= sizes, (checked, sizes)
 
 
 def test_capped_wave_keeps_cheap_queries_exact():
