@@ -27,8 +27,9 @@ query plain under a device cap (status and prefix-match rate).  Its
 `out_of_core` part runs 4-vertex queries in core, out of core with streamed
 adjacency partitions and out of core reading the pinned adjacency in place.
 
-`value` is device-timed (CUDA events around each wave, inputs resident in
-HBM), `e2e` is wall time around the same C-ABI calls from host buffers
+`value` is device-timed (CUDA events, from each step's first kernel to its
+last, inputs resident in HBM), `e2e` is wall time around the same C-ABI
+calls from host buffers
 (query arrays in, results out).  L2 is flushed between steps (a 256 MiB
 write).  With torchrun (N > 1) every rank runs an independent replica on its
 own queries (the path has no exchange step); rank 0 reports the max time.
@@ -252,7 +253,7 @@ def run_gem(args):
     steps = list(range(args.warmup, args.warmup + args.steps))
     dev_ms, wall_ms, res_all = [], [], []
     h2d = d2h = launches = 0
-    jbytes = jms = tbytes = tpass_ms = 0.0
+    jbytes = jms = tbytes = tpass_ms = busy_ms = 0.0
     n_joins = n_tab = 0
     phase = {"filter": 0.0, "tables": 0.0, "index": 0.0, "join": 0.0}
     with Clocks(local) as clk:
@@ -267,7 +268,11 @@ def run_gem(args):
             torch.cuda.synchronize()
             wall_ms.append((time.perf_counter() - t0) * 1e3)
             ws = waves_of(rs)
-            dev_ms.append(sum(r["ms"]["total"] for r in ws))
+            # device time of the step: its first wave's first event to its last
+            # wave's last event (CUDA events on one timeline), so a wave retried
+            # after an out-of-memory split and the gaps between waves count too
+            dev_ms.append(max(r["t_end_ms"] for r in ws) - min(r["t_begin_ms"] for r in ws))
+            busy_ms += sum(r["ms"]["total"] for r in ws)
             launches += sum(r["launches"] for r in ws)
             jbytes += sum(r["bytes_alg"][3] for r in ws)
             jms += sum(r["ms"]["join"] for r in ws)
@@ -352,6 +357,7 @@ def run_gem(args):
         "plain": plain,
         "counts_stable_across_steps": counts_stable,
         "phase_ms_per_step": {k: round(v / args.steps, 3) for k, v in phase.items()},
+        "waves_busy_ms_per_step": round(busy_ms / args.steps, 3),
         "autotune": tuned,
         "e2e": {"value": e2e_exact / twall if twall > 0 else 0.0, "unit": "queries/s",
                 "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
@@ -458,7 +464,8 @@ def config1_section(gem, args, local):
         for _ in range(args.c1_steps):
             flush_l2(dev)
             _, rs = c.batch(pool)
-            ts.append(sum(r["ms"]["total"] for r in waves_of(rs)))
+            ws = waves_of(rs)
+            ts.append(max(r["t_end_ms"] for r in ws) - min(r["t_begin_ms"] for r in ws))
         exact = sum(r["status"] == "OK" for r in rs)
         out["batched_queries_per_s"] = exact / (sum(ts) / len(ts) / 1e3)
         out["batched_ms_per_step"] = statistics.median(ts)

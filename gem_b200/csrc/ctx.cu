@@ -1605,28 +1605,37 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
     vs[i] = make_host_query(&qs[i], all[i], e);
     res[i].status = vs[i];
   }
-  // waves: as many queries as the per-wave row limit allows; a wave whose
-  // tables do not fit the device budget is split in halves and retried, down
-  // to single queries
-  const uint32_t max_rows = ctx->wave_max_rows;
-  std::deque<std::vector<uint32_t>> todo;
-  for (uint32_t i = 0; i < n;) {
-    std::vector<uint32_t> ids;
-    uint32_t rows = 0;
-    while (i < n && (ids.empty() || rows + all[i].nv <= max_rows)) {
-      if (vs[i] == GEM_OK) {
-        ids.push_back(i);
-        rows += all[i].nv;
-      }
-      ++i;
-    }
-    if (!ids.empty()) todo.push_back(std::move(ids));
-  }
-  uint32_t wave_no = 0;
+  // Waves are packed as the batch runs: as many pending queries as the row
+  // limit allows.  A wave that does not fit the device budget is split in
+  // halves and retried (down to single queries) with a released arena, and
+  // the context's limit drops to half the rows that failed, so later waves
+  // (and later batches) are packed to a size that fits.
+  std::deque<std::vector<uint32_t>> retry;
+  uint32_t next = 0, wave_no = 0;
   gem_status first_err = GEM_OK;
-  while (!todo.empty()) {
-    std::vector<uint32_t> ids = std::move(todo.front());
-    todo.pop_front();
+  auto rows_of = [&](const std::vector<uint32_t> &ids) {
+    uint64_t r = 0;
+    for (uint32_t id : ids) r += all[id].nv;
+    return r;
+  };
+  while (!retry.empty() || next < n) {
+    std::vector<uint32_t> ids;
+    if (!retry.empty()) {
+      ids = std::move(retry.front());
+      retry.pop_front();
+    } else {
+      uint64_t cap = ctx->wave_max_rows;
+      if (ctx->wave_rows_cap) cap = std::min<uint64_t>(cap, ctx->wave_rows_cap);
+      uint64_t rows = 0;
+      while (next < n && (ids.empty() || rows + all[next].nv <= cap)) {
+        if (vs[next] == GEM_OK) {
+          ids.push_back(next);
+          rows += all[next].nv;
+        }
+        ++next;
+      }
+      if (ids.empty()) continue;
+    }
     Wave w;
     for (uint32_t id : ids) w.q.push_back(all[id]);
     ctx->arena.reset();
@@ -1635,9 +1644,12 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
       cudaStreamSynchronize(ctx->s);  // the failed wave's copies and kernels are done before reuse
       cudaGetLastError();
       if (st == GEM_ERR_OOM && ids.size() > 1) {
+        const uint64_t r = rows_of(ids);
+        ctx->wave_rows_cap = (uint32_t)std::max<uint64_t>(1, r / 2);
+        ctx->arena.release(ctx);  // a fresh arena: chunks sized for the smaller waves
         const size_t h = ids.size() / 2;
-        todo.push_front(std::vector<uint32_t>(ids.begin() + h, ids.end()));
-        todo.push_front(std::vector<uint32_t>(ids.begin(), ids.begin() + h));
+        retry.push_front(std::vector<uint32_t>(ids.begin() + h, ids.end()));
+        retry.push_front(std::vector<uint32_t>(ids.begin(), ids.begin() + h));
         continue;
       }
       for (uint32_t id : ids) res[id].status = st;

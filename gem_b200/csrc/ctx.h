@@ -159,6 +159,9 @@ struct gem_ctx {
   uint32_t donate_max_level = 30;
   bool closed_form_suffix = true;
   uint32_t wave_max_rows = 4096;
+  // batch packing learnt from earlier waves: half the rows of the last wave
+  // that did not fit the device budget (0 = none yet)
+  uint32_t wave_rows_cap = 0;
   uint32_t join_grid_div = 1;        // the join grid takes blocks_per_sm / this per SM (serving lanes: 2)
   // device timeline: waves report their first and last event against ev_ref
   // (recorded when the graph is loaded; serving lanes share their root's)

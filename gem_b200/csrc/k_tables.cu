@@ -129,6 +129,47 @@ __global__ void __launch_bounds__(256) table_src_kernel(TabPass P, const TabSour
       xv[i] = tv && arc < a1;
       x[i] = xv[i] ? __ldg(P.nbr + (arc - P.arc_shift)) : 0u;
     }
+    // Common case: the warp's tiles all belong to one source (a source has
+    // many tiles).  Then each table of the source is read once for all of
+    // them, and its TILE_UNROLL membership probes (count) or mask / position
+    // loads (write) are issued together.
+    bool same = base + TILE_UNROLL <= P.t1;
+#pragma unroll
+    for (int i = 1; i < TILE_UNROLL; ++i) same = same && sx[i] == sx[0];
+    if (same) {
+      const uint32_t e0 = __ldg(sedge + 2 * sx[0]), ne = __ldg(sedge + 2 * sx[0] + 1);
+      for (uint32_t e = e0; e < e0 + ne; ++e) {
+        const uint64_t tb = edges[e].tile_base;
+        if (!WRITE) {
+          const uint64_t *rb = edges[e].rb_w;
+          bool hit[TILE_UNROLL];
+#pragma unroll
+          for (int i = 0; i < TILE_UNROLL; ++i) hit[i] = xv[i] && dev::rank_member(rb, x[i]);
+#pragma unroll
+          for (int i = 0; i < TILE_UNROLL; ++i) {
+            const uint32_t m = __ballot_sync(dev::FULL, hit[i]);
+            if (lane == 0) mask[tb + lt[i]] = m;
+          }
+        } else {
+          uint32_t m[TILE_UNROLL];
+          uint64_t vb[TILE_UNROLL];
+#pragma unroll
+          for (int i = 0; i < TILE_UNROLL; ++i) {
+            m[i] = __ldg(mask + tb + lt[i]);
+            vb[i] = __ldg(vp + tb + lt[i]);
+          }
+          const bool km = (edges[e].flags & TAB_KEY_MAP) != 0;
+#pragma unroll
+          for (int i = 0; i < TILE_UNROLL; ++i)
+            if (m[i] & (1u << lane)) {
+              const uint64_t pos = vb[i] + __popc(m[i] & ((1u << lane) - 1u));
+              values[pos] = x[i];
+              if (km) vkey[pos] = kx[i];
+            }
+        }
+      }
+      continue;
+    }
 #pragma unroll
     for (int i = 0; i < TILE_UNROLL; ++i) {
       if (base + i >= P.t1) break;  // the same in every lane

@@ -41,6 +41,16 @@ struct Server {
     uint64_t est;
   };
   std::deque<Req> pending;
+  // tickets at which a wave that did not fit was halved: a wave ends before them
+  std::vector<uint64_t> split_at;
+  bool is_split_point(uint64_t t) {
+    for (size_t i = 0; i < split_at.size(); ++i)
+      if (split_at[i] == t) {
+        split_at.erase(split_at.begin() + (long)i);
+        return true;
+      }
+    return false;
+  }
   std::map<uint64_t, gem_result> done;
   uint64_t next_ticket = 1;
   uint64_t in_flight = 0, budget = 0;
@@ -110,7 +120,8 @@ static void server_loop(gem_ctx *root, gem_ctx *lane) {
       uint32_t rows = 0;
       const int mode = S.pending.front().mode;
       while (!S.pending.empty() && S.pending.front().mode == mode &&
-             (batch.empty() || rows + S.pending.front().q.nv <= lane->wave_max_rows)) {
+             (batch.empty() || rows + S.pending.front().q.nv <= lane->wave_max_rows) &&
+             (batch.empty() || !S.is_split_point(S.pending.front().ticket))) {
         rows += S.pending.front().q.nv;
         batch.push_back(std::move(S.pending.front()));
         S.pending.pop_front();
@@ -124,6 +135,17 @@ static void server_loop(gem_ctx *root, gem_ctx *lane) {
     if (st != GEM_OK) {
       cudaStreamSynchronize(lane->s);
       cudaGetLastError();
+    }
+    if (st == GEM_ERR_OOM && batch.size() > 1) {
+      // the wave's tables do not fit the lane's budget: its requests go back
+      // to the front of the queue in halves, with a fresh arena
+      lane->arena.release(lane);
+      std::lock_guard<std::mutex> lk(S.mu);
+      const size_t h = batch.size() / 2;
+      S.split_at.push_back(batch[h].ticket);
+      for (size_t i = batch.size(); i-- > 0;) S.pending.push_front(std::move(batch[i]));
+      S.cv.notify_all();
+      continue;
     }
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < batch.size(); ++i) {
