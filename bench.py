@@ -665,7 +665,10 @@ def ooc26_section(gem, args, local):
         c.load_graph(g)
         _, r4i = c.batch(q4)
         out["small4_in_core_wave_ms"] = round(sum(w["ms"]["total"] for w in waves_of(r4i)), 1)
-    out["small4_counts_equal"] = [(r["status"], r["count"]) for r in r4] == [(r["status"], r["count"]) for r in r4i]
+    both = [(a["count"], b["count"]) for a, b in zip(r4, r4i) if a["status"] == "OK" and b["status"] == "OK"]
+    out["small4_in_core_exact"] = sum(r["status"] == "OK" for r in r4i)
+    out["small4_both_exact"] = len(both)
+    out["small4_counts_equal"] = all(a == b for a, b in both)
     return out
 
 

@@ -19,6 +19,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -78,7 +79,21 @@ gem_status Arena::alloc(gem_ctx *ctx, uint64_t bytes, void **out) {
   }
   uint64_t sz = std::max<uint64_t>(bytes, 512ull << 20);
   if (ctx->device_bytes + sz > ctx->budget) {
-    sz = bytes;
+    // chunks this wave has not used (too small for what it asked) go back
+    // to the budget before the new one is taken
+    size_t k = 0;
+    for (size_t i = 0; i < chunks.size(); ++i) {
+      if (chunks[i].used == 0) {
+        cudaFree(chunks[i].base);
+        ctx->device_bytes -= chunks[i].size;
+      } else {
+        chunks[k++] = chunks[i];
+      }
+    }
+    chunks.resize(k);
+    cur = chunks.size();
+    sz = std::max<uint64_t>(bytes, 512ull << 20);
+    if (ctx->device_bytes + sz > ctx->budget) sz = bytes;
     if (ctx->device_bytes + sz > ctx->budget) {
       ctx->err = "device budget exceeded: need " + std::to_string(bytes) + " more bytes";
       return GEM_ERR_OOM;
@@ -237,9 +252,20 @@ static void free_graph(gem_ctx *ctx) {
   ctx->loaded = false;
 }
 
+// The batch lane (a second context over this context's graph) and the
+// budget it took; dropped before the graph changes or the context goes.
+void drop_batch_lane(gem_ctx *ctx) {
+  if (!ctx->batch_lane) return;
+  gem_ctx_destroy(ctx->batch_lane);
+  ctx->batch_lane = nullptr;
+  if (ctx->batch_saved_budget) ctx->budget = ctx->batch_saved_budget;
+  ctx->batch_saved_budget = 0;
+}
+
 extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
   if (!ctx) return;
   server_shutdown(ctx);
+  drop_batch_lane(ctx);
   cudaSetDevice(ctx->opts.device);
   cudaStreamSynchronize(ctx->s);
   ctx->arena.release(ctx);
@@ -359,6 +385,7 @@ extern "C" gem_status gem_ctx_ooc_stats(const gem_ctx *ctx, gem_ooc_stats *out) 
 extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
   if (!ctx || !hg) return GEM_ERR_ARG;
   if (ctx->server) return GEM_ERR_STATE;
+  drop_batch_lane(ctx);
   CU(cudaSetDevice(ctx->opts.device));
   CU(cudaStreamSynchronize(ctx->s));
   ctx->arena.reset();
@@ -856,7 +883,8 @@ static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   ST(aalloc(ctx, rows + 1, &d_cbase));
   CU(h2d(ctx, d_cbase, w.c_base.data(), 8ull * (rows + 1)));
   ST(aalloc(ctx, total ? total : 1, &w.d_cand));
-  launch_compact(w.d_rb, d_ex, rows, nwords, d_cbase, w.d_cand, ctx->s);
+  ST(aalloc(ctx, nbits, &w.d_bits));
+  launch_compact(w.d_rb, d_ex, rows, nwords, d_cbase, w.d_cand, ctx->s, w.d_bits);
   CU(cudaGetLastError());
   w.cand_total = total;
   // algorithmic bytes, per descriptor: labels + degrees of every vertex, the
@@ -982,6 +1010,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
     e.src = rq.s;
     e.flags = flags;
     e.rb_w = w.d_rb + (uint64_t)tgt * w.nwords;
+    e.bits_w = w.d_bits + (uint64_t)tgt * w.nwords;
     e.tile_base = tiles;
     e.ntiles = stb[rq.s + 1] - stb[rq.s];
     e.off_base = offs;
@@ -1605,62 +1634,117 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
     vs[i] = make_host_query(&qs[i], all[i], e);
     res[i].status = vs[i];
   }
-  // Waves are packed as the batch runs: as many pending queries as the row
-  // limit allows.  A wave that does not fit the device budget is split in
-  // halves and retried (down to single queries) with a released arena, and
-  // the context's limit drops to half the rows that failed, so later waves
-  // (and later batches) are packed to a size that fits.
+  // Waves are packed as the batch runs: as many pending queries as the
+  // lane's row limit allows.  A wave that does not fit the lane's device
+  // budget is split in halves and retried (down to single queries) with a
+  // released arena, and the lane's limit drops to half the rows that failed,
+  // so later waves (and later batches) are packed to a size that fits
+  // (the limit does not grow back: a retried wave costs its filter and
+  // table build).
+  //
+  // An in-core batch of more rows than one wave takes runs on two lanes: the
+  // context and a lane context borrowing its graph (created once, kept), one
+  // host thread each, the device budget left after the graph split between
+  // them and each join grid on half of the blocks per SM.  One wave's join
+  // then runs beside the next wave's filter and table kernels.
+  std::mutex mu;
   std::deque<std::vector<uint32_t>> retry;
   uint32_t next = 0, wave_no = 0;
   gem_status first_err = GEM_OK;
+  std::string lane_err;
   auto rows_of = [&](const std::vector<uint32_t> &ids) {
     uint64_t r = 0;
     for (uint32_t id : ids) r += all[id].nv;
     return r;
   };
-  while (!retry.empty() || next < n) {
-    std::vector<uint32_t> ids;
-    if (!retry.empty()) {
-      ids = std::move(retry.front());
-      retry.pop_front();
-    } else {
-      uint64_t cap = ctx->wave_max_rows;
-      if (ctx->wave_rows_cap) cap = std::min<uint64_t>(cap, ctx->wave_rows_cap);
-      uint64_t rows = 0;
-      while (next < n && (ids.empty() || rows + all[next].nv <= cap)) {
-        if (vs[next] == GEM_OK) {
-          ids.push_back(next);
-          rows += all[next].nv;
+  uint64_t total_rows = 0;
+  for (uint32_t i = 0; i < n; ++i)
+    if (vs[i] == GEM_OK) total_rows += all[i].nv;
+  auto worker = [&](gem_ctx *lane) {
+    for (;;) {
+      std::vector<uint32_t> ids;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!retry.empty()) {
+          ids = std::move(retry.front());
+          retry.pop_front();
+        } else {
+          uint64_t cap = lane->wave_max_rows;
+          if (lane->wave_rows_cap) cap = std::min<uint64_t>(cap, lane->wave_rows_cap);
+          uint64_t rows = 0;
+          while (next < n && (ids.empty() || rows + all[next].nv <= cap)) {
+            if (vs[next] == GEM_OK) {
+              ids.push_back(next);
+              rows += all[next].nv;
+            }
+            ++next;
+          }
         }
-        ++next;
       }
-      if (ids.empty()) continue;
-    }
-    Wave w;
-    for (uint32_t id : ids) w.q.push_back(all[id]);
-    ctx->arena.reset();
-    gem_status st = run_wave(ctx, w, 0, mode, nullptr, 0);
-    if (st != GEM_OK) {
-      cudaStreamSynchronize(ctx->s);  // the failed wave's copies and kernels are done before reuse
-      cudaGetLastError();
-      if (st == GEM_ERR_OOM && ids.size() > 1) {
-        const uint64_t r = rows_of(ids);
-        ctx->wave_rows_cap = (uint32_t)std::max<uint64_t>(1, r / 2);
-        ctx->arena.release(ctx);  // a fresh arena: chunks sized for the smaller waves
-        const size_t h = ids.size() / 2;
-        retry.push_front(std::vector<uint32_t>(ids.begin() + h, ids.end()));
-        retry.push_front(std::vector<uint32_t>(ids.begin(), ids.begin() + h));
+      if (ids.empty()) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (retry.empty() && next >= n) return;
         continue;
       }
-      for (uint32_t id : ids) res[id].status = st;
-      if (first_err == GEM_OK) first_err = st;
-      continue;
+      Wave w;
+      for (uint32_t id : ids) w.q.push_back(all[id]);
+      lane->arena.reset();
+      const gem_status st = run_wave(lane, w, 0, mode, nullptr, 0);
+      if (st != GEM_OK) {
+        cudaStreamSynchronize(lane->s);  // the failed wave's copies and kernels are done before reuse
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(mu);
+        if (st == GEM_ERR_OOM && ids.size() > 1) {
+          lane->wave_rows_cap = (uint32_t)std::max<uint64_t>(1, rows_of(ids) / 2);
+          lane->arena.release(lane);  // a fresh arena: chunks sized for the smaller waves
+          const size_t h = ids.size() / 2;
+          retry.push_front(std::vector<uint32_t>(ids.begin() + h, ids.end()));
+          retry.push_front(std::vector<uint32_t>(ids.begin(), ids.begin() + h));
+          continue;
+        }
+        for (uint32_t id : ids) res[id].status = st;
+        if (first_err == GEM_OK) first_err = st;
+        if (lane != ctx && lane_err.empty()) lane_err = lane->err;
+        continue;
+      }
+      uint32_t my_wave;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        my_wave = wave_no++;
+      }
+      for (size_t k = 0; k < ids.size(); ++k) {
+        wave_result(lane, w, k, &res[ids[k]]);
+        res[ids[k]].wave = my_wave;
+      }
     }
-    for (size_t k = 0; k < ids.size(); ++k) {
-      wave_result(ctx, w, k, &res[ids[k]]);
-      res[ids[k]].wave = wave_no;
+  };
+  gem_ctx *second = nullptr;
+  if (!ctx->opts.ooc && total_rows > ctx->wave_max_rows) {
+    if (!ctx->batch_lane) {
+      // the graph's remaining budget, split evenly: the context's arena is
+      // released so each lane grows its own within its half
+      ctx->arena.release(ctx);
+      const uint64_t room = ctx->budget > ctx->device_bytes ? ctx->budget - ctx->device_bytes : 0;
+      if (lane_create(ctx, room / 2, &ctx->batch_lane) == GEM_OK) {
+        ctx->batch_saved_budget = ctx->budget;
+        ctx->budget = ctx->device_bytes + room / 2;
+      } else {
+        ctx->batch_lane = nullptr;
+        cudaGetLastError();
+      }
     }
-    ++wave_no;
+    second = ctx->batch_lane;
+  }
+  if (second) {
+    for (int b = 0; b < 6; ++b) second->tune[b] = ctx->tune[b];
+    ctx->join_grid_div = second->join_grid_div = 2;
+    std::thread t(worker, second);
+    worker(ctx);
+    t.join();
+    ctx->join_grid_div = 1;
+    if (!lane_err.empty() && ctx->err.empty()) ctx->err = lane_err;
+  } else {
+    worker(ctx);
   }
   for (uint32_t k = 0; k < n; ++k)
     if (res[k].status != GEM_OK && first_err == GEM_OK) first_err = (gem_status)res[k].status;

@@ -66,6 +66,7 @@ struct Wave {
   uint32_t *d_vkey = nullptr;       // key positions of the pool queries' root-table values
   uint32_t nrows = 0, nwords = 0, nsrc = 0;
   uint64_t *d_rb = nullptr;       // rank bitmaps, nrows x nwords
+  uint32_t *d_bits = nullptr;     // their membership bits alone, nrows x nwords
   uint32_t *d_cand = nullptr;     // candidate lists back to back
   std::vector<uint32_t> cnt;      // |C| per row
   std::vector<uint64_t> c_base;   // list start per row
@@ -168,12 +169,16 @@ struct gem_ctx {
   cudaEvent_t ev_ref = nullptr;
   bool ev_ref_recorded = false;
   bool borrowed_graph = false;       // a serving lane: the graph belongs to another context
+  gem_ctx *batch_lane = nullptr;     // second lane of multi-wave batches (kept until the graph changes)
+  uint64_t batch_saved_budget = 0;   // the device budget before the batch lane took its half
 };
 
 // A serving lane: a context with its own stream, events, arena, control
 // block and task queue that borrows `root`'s resident graph (in-core only),
 // so that waves of two lanes run on the device at the same time.
 gem_status lane_create(gem_ctx *root, uint64_t budget, gem_ctx **out);
+// Destroys the context's batch lane, if any, and gives its budget back.
+void drop_batch_lane(gem_ctx *ctx);
 
 gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_t *emb_dev, uint64_t emb_cap);
 void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r);

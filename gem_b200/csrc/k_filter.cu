@@ -93,13 +93,15 @@ void launch_filter(const DevGraph &g, const FilterDesc *d_desc, uint32_t nquery,
 }
 
 __global__ void compact_kernel(uint64_t *__restrict__ rb, const uint64_t *__restrict__ ex, uint32_t nrows,
-                               uint32_t nwords, const uint64_t *__restrict__ c_base, uint32_t *__restrict__ cand) {
+                               uint32_t nwords, const uint64_t *__restrict__ c_base, uint32_t *__restrict__ cand,
+                               uint32_t *__restrict__ bit_rows) {
   const uint64_t n = (uint64_t)nrows * nwords;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t r = (uint32_t)(i / nwords), w = (uint32_t)(i % nwords);
     const uint32_t bits = (uint32_t)rb[i];
     const uint64_t rank = ex[i] - ex[(uint64_t)r * nwords];
     rb[i] = (rank << 32) | bits;
+    if (bit_rows) bit_rows[i] = bits;
     uint32_t m = bits, j = 0;
     uint32_t *dst = cand + c_base[r] + rank;
     while (m) {
@@ -111,13 +113,13 @@ __global__ void compact_kernel(uint64_t *__restrict__ rb, const uint64_t *__rest
 }
 
 void launch_compact(uint64_t *rb, const uint64_t *ex, uint32_t nrows, uint32_t nwords, const uint64_t *c_base,
-                    uint32_t *cand, cudaStream_t s) {
+                    uint32_t *cand, cudaStream_t s, uint32_t *bit_rows) {
   uint64_t n = (uint64_t)nrows * nwords;
   if (n == 0) return;
   uint64_t blocks = (n + 255) / 256;
   if (blocks > 148ull * 32) blocks = 148ull * 32;
   count_launch();
-  compact_kernel<<<(uint32_t)blocks, 256, 0, s>>>(rb, ex, nrows, nwords, c_base, cand);
+  compact_kernel<<<(uint32_t)blocks, 256, 0, s>>>(rb, ex, nrows, nwords, c_base, cand, bit_rows);
 }
 
 }  // namespace gem

@@ -141,10 +141,10 @@ __global__ void __launch_bounds__(256) table_src_kernel(TabPass P, const TabSour
       for (uint32_t e = e0; e < e0 + ne; ++e) {
         const uint64_t tb = edges[e].tile_base;
         if (!WRITE) {
-          const uint64_t *rb = edges[e].rb_w;
+          const uint32_t *bw = edges[e].bits_w;
           bool hit[TILE_UNROLL];
 #pragma unroll
-          for (int i = 0; i < TILE_UNROLL; ++i) hit[i] = xv[i] && dev::rank_member(rb, x[i]);
+          for (int i = 0; i < TILE_UNROLL; ++i) hit[i] = xv[i] && ((__ldg(bw + (x[i] >> 5)) >> (x[i] & 31u)) & 1u);
 #pragma unroll
           for (int i = 0; i < TILE_UNROLL; ++i) {
             const uint32_t m = __ballot_sync(dev::FULL, hit[i]);
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(256) table_src_kernel(TabPass P, const TabSour
       for (uint32_t e = e0; e < e0 + ne; ++e) {
         const uint64_t et = edges[e].tile_base + lt[i];
         if (!WRITE) {
-          const bool hit = xv[i] && dev::rank_member(edges[e].rb_w, x[i]);
+          const bool hit = xv[i] && ((__ldg(edges[e].bits_w + (x[i] >> 5)) >> (x[i] & 31u)) & 1u);
           const uint32_t m = __ballot_sync(dev::FULL, hit);
           if (lane == 0) mask[et] = m;
         } else {

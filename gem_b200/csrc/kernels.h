@@ -86,8 +86,10 @@ void launch_filter(const DevGraph &g, const FilterDesc *d_desc, uint32_t nquery,
 // Given ex = exclusive scan of popcounts over all rows, writes the per-word
 // ranks into the high halves of rb and the sorted candidate lists
 // cand[c_base[row] ...].
+// bit_rows (optional, nrows x nwords u32): the membership bits alone, half
+// the bytes of rb for tests that need no rank.
 void launch_compact(uint64_t *rb, const uint64_t *ex, uint32_t nrows, uint32_t nwords,
-                    const uint64_t *c_base, uint32_t *cand, cudaStream_t s);
+                    const uint64_t *c_base, uint32_t *cand, cudaStream_t s, uint32_t *bit_rows = nullptr);
 
 // ---------------------------------------------------------------------------
 // Edge-candidate tables
@@ -101,7 +103,8 @@ struct TabSource {           // a (query, query vertex) whose candidates are tab
 struct TabEdge {             // a directed table T(u -> w)
   uint32_t src;              // index into TabSource
   uint32_t flags;            // TAB_KEY_MAP: the write pass also records each value's key position
-  const uint64_t *rb_w;      // rank bitmap row of the target w (membership)
+  const uint64_t *rb_w;      // rank bitmap row of the target w
+  const uint32_t *bits_w;    // membership bits of w alone (32 vertices per word)
   uint64_t tile_base;        // first tile of this edge in the flattened edge-tile space
   uint64_t ntiles;
   uint64_t off_base;         // first entry of this edge in the flattened offsets space

@@ -183,6 +183,7 @@ void server_shutdown(gem_ctx *ctx) {
 // Starts the server: a second lane for in-core contexts (the remaining
 // device budget split between the two), one worker thread per lane.
 static gem_status server_start(gem_ctx *ctx) {
+  drop_batch_lane(ctx);  // serving splits the budget between lanes of its own
   Server *S = new Server();
   ctx->server = S;
   const uint64_t cap = ctx->opts.admit_gb ? (uint64_t)ctx->opts.admit_gb << 30 : 120ull << 30;

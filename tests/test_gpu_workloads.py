@@ -74,3 +74,26 @@ def test_capped_wave_keeps_cheap_queries_exact():
     for q, r in zip(cheap, rs[1:]):
         cnt, _, ok = oracle.count(g, q, want_hash=False)
         assert ok and r["status"] == "OK" and r["count"] == cnt
+
+
+def test_two_lane_batch_matches_plain():
+    """A batch of more query vertices than one wave takes runs its waves on
+    two lanes (their joins beside the other lane's table builds): every count
+    equals the plain run's and the oracle's, and waves of both lanes overlap
+    on the device timeline."""
+    g, _ = bench.make_graph(gem, "rmat16")
+    pool = bench.config1_pool(gem, g)
+    qs = pool * 12  # 4,800 query vertices: more than one wave
+    expect = [oracle.count(g, q, want_hash=False)[0] for q in pool]
+    with gem.Context(time_cap_ms=60000) as c:
+        c.load_graph(g)
+        for _ in range(2):  # the second batch reuses the lane
+            st, rs = c.batch(qs)
+            assert st == 0
+            for i, r in enumerate(rs):
+                assert r["status"] == "OK" and r["count"] == expect[i % len(pool)], i
+        plain = [c.run(q)["count"] for q in pool]
+    assert plain == expect
+    iv = sorted({r["wave"]: (r["t_begin_ms"], r["t_end_ms"]) for r in rs}.values())
+    assert len(iv) >= 2
+    assert any(iv[b][0] < iv[a][1] for a in range(len(iv)) for b in range(a + 1, len(iv)))
