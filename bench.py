@@ -156,11 +156,11 @@ def make_graph(backend, name):
     return g, time.time() - t
 
 
-def mix_pool(backend, g, n, seed=0x51003):
+def mix_pool(backend, g, n, seed=0x51003, sizes=MIX_SIZES):
     """Config-3 queries: query i has size MIX_SIZES[mix64(seed + i) % 6] and is
     sparse for even i, dense for odd i; the queries of one (size, density)
     come from one random-walk stream (seed << 8 | 4 size + density)."""
-    ks = [MIX_SIZES[_mix64(seed + i) % len(MIX_SIZES)] for i in range(n)]
+    ks = [sizes[_mix64(seed + i) % len(sizes)] for i in range(n)]
     ds = [1 + (i % 2) for i in range(n)]
     need = {}
     for k, d in zip(ks, ds):
@@ -179,9 +179,9 @@ def config1_pool(backend, g, n=100, seed=0x51000):
     return backend.gen_queries(g, 4, 0, n, seed=seed)
 
 
-def workload_pool(backend, name, g, n):
+def workload_pool(backend, name, g, n, sizes=MIX_SIZES):
     if name == "rmat22-mix":
-        return mix_pool(backend, g, n)
+        return mix_pool(backend, g, n, sizes=sizes)
     if name == "rmat16":
         return config1_pool(backend, g, n)
     raise SystemExit(f"unknown workload {name}")
@@ -195,7 +195,7 @@ def workload_config(name, args, world):
          "batch": args.batch, "time_cap_ms": args.cap_ms, "parallelism": f"replicas{world}",
          "l2": "flushed (256 MiB write)"}
     if name == "rmat22-mix":
-        c["query_sizes"] = list(MIX_SIZES)
+        c["query_sizes"] = list(args.sizes)
         c["densities"] = "alternating sparse/dense"
     else:
         c["query_sizes"] = [4]
@@ -236,8 +236,8 @@ def run_gem(args):
     dev = torch.device("cuda", local)
     g, gen_s = make_graph(gem, args.workload)
     B = args.batch
-    pool = workload_pool(gem, args.workload, g, B * world)
-    ctx = gem.Context(device=local, time_cap_ms=args.cap_ms)
+    pool = workload_pool(gem, args.workload, g, B * world, args.sizes)
+    ctx = gem.Context(device=local, time_cap_ms=args.cap_ms, batch_lanes=args.lanes)
     ctx.load_graph(g)
     tuned = {}
     if args.autotune:
@@ -392,26 +392,28 @@ def ctypes_result_bytes(gem):
 
 def roofline(alg_bytes, ms, peak, peak_src, kernel, traffic):
     achieved = alg_bytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
-    t, src = traffic
+    ratio, src = traffic
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if peak else None,
-            "traffic": t, "traffic_source": src, "alg_bytes_per_launch": alg_bytes, "ms_per_launch": ms,
+            "traffic": int(ratio * alg_bytes) if ratio is not None else None,
+            "traffic_source": src, "alg_bytes_per_launch": alg_bytes, "ms_per_launch": ms,
             "kernel": kernel, "peak_source": peak_src}
 
 
-def profiled_traffic(kind, workload, batch):
-    """DRAM bytes (read + write) of one launch of `kind` ("join" or "tables")
-    on workload `workload` with batch `batch`, from the committed ncu capture
-    summary whose `workload_key` line equals "<kind> <workload> batch
-    <batch>" and which states `dram_bytes_per_launch`, or (None, None)."""
+def profiled_traffic(kind, workload, batch=None):
+    """DRAM bytes (read + write) per algorithmic byte of `kind` ("join" or
+    "tables") on `workload`, from the committed ncu capture summary whose
+    `workload_key` line is "<kind> <workload>" and which states
+    `dram_per_alg_byte` (the ratio does not depend on the wave's size, so a
+    capture of a smaller wave scales to the bench's launches), or (None, None)."""
     import glob
     import re
-    key = f"{kind} {workload} batch {batch}"
+    key = f"{kind} {workload}"
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         text = open(path).read()
         k = re.search(r"^workload_key: (.+)$", text, re.M)
-        m = re.search(r"^dram_bytes_per_launch: (\d+)$", text, re.M)
+        m = re.search(r"^dram_per_alg_byte: ([0-9.]+)$", text, re.M)
         if k and m and k.group(1).strip() == key:
-            return int(m.group(1)), os.path.relpath(path, ROOT) + " (ncu)"
+            return float(m.group(1)), os.path.relpath(path, ROOT) + " (ncu DRAM bytes / algorithmic bytes of a capture)"
     return None, None
 
 
@@ -731,7 +733,7 @@ def run_reference(args):
         return
     import oracle
     g, _ = make_graph(oracle, args.workload)
-    pool = workload_pool(oracle, args.workload, g, args.batch)
+    pool = workload_pool(oracle, args.workload, g, args.batch, args.sizes)
     threads = os.cpu_count() or 1
     S = max(1, min(args.ref_sample, len(pool)))
     times, exact, emb = [], 0, 0
@@ -768,10 +770,13 @@ def parse_args(argv=None):
     ap.add_argument("--impl", default="gem", choices=["gem", "reference"])
     ap.add_argument("--workload", default="rmat22-mix", choices=sorted(DEFAULTS))
     ap.add_argument("--batch", type=int, default=None, help="queries per step (default: the workload's)")
+    ap.add_argument("--sizes", default=None,
+                    help="query sizes of the scale-22 mix, e.g. '4' (default: 4,8,12,16,24,32)")
     ap.add_argument("--cap-ms", type=int, default=None, help="per-query device time cap")
     ap.add_argument("--plain", type=int, default=None, help="queries of the plain sample (0 = skip)")
     ap.add_argument("--autotune", type=int, default=None)
     ap.add_argument("--config1", type=int, default=1, help="run the config-1 section (headline rmat22-mix)")
+    ap.add_argument("--lanes", type=int, default=0, help="batch lanes: 0 = two for multi-wave batches, 1 = one")
     ap.add_argument("--c1-steps", type=int, default=10)
     ap.add_argument("--c2-sample", type=int, default=8, help="scale-22 queries in the rmat22 section (0 = skip)")
     ap.add_argument("--ooc-sample", type=int, default=50,
@@ -794,6 +799,7 @@ def parse_args(argv=None):
                     help="scanned-arc cap per query of the CPU legs and the reference arm")
     ap.add_argument("--ref-sample", type=int, default=4, help="queries per step of the reference arm (--impl reference)")
     args = ap.parse_args(argv)
+    args.sizes = tuple(int(x) for x in args.sizes.split(",")) if args.sizes else MIX_SIZES
     d = DEFAULTS[args.workload]
     for k in ("batch", "cap_ms", "plain", "autotune"):
         if getattr(args, k) is None:
