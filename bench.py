@@ -375,7 +375,7 @@ def run_gem(args):
     line["roofline"], line["roofline_other"] = (roof_tab, roof_join) if tpass_ms >= jms else (roof_join, roof_tab)
     line["roofline"]["share_of_step"] = round((tpass_ms if tpass_ms >= jms else jms) / (tdev * 1e3), 3) if tdev else None
     if args.cpu_sample > 0:
-        line["parity"] = oracle_parity(g, batch_of(args.warmup), res_all[0], args.cpu_parity_cap, args.cpu_budget_s)
+        line["parity"] = oracle_parity(g, batch_of(args.warmup), res_all[0], args.cpu_parity_cap, args.parity_budget_s)
         line["cpu_baseline"] = cpu_baseline(g, pool, args)
         qs0 = batch_of(args.warmup)
         hstride = max(1, len(qs0) // args.host_path_queries)
@@ -784,7 +784,8 @@ def parse_args(argv=None):
     ap.add_argument("--c2-cap-ms", type=int, default=1000)
     ap.add_argument("--cpu-sample", type=int, default=100, help="pool queries timed on the CPU oracle (0 = skip)")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="wall-time bound of the CPU legs")
-    ap.add_argument("--cpu-parity-cap", type=int, default=200_000_000, help="oracle work cap of the parity check")
+    ap.add_argument("--parity-budget-s", type=float, default=60.0, help="wall-time bound of the oracle parity check")
+    ap.add_argument("--cpu-parity-cap", type=int, default=2_000_000_000, help="oracle work cap of the parity check")
     ap.add_argument("--host-path-queries", type=int, default=100)
     ap.add_argument("--serve-seconds", type=float, default=1.0,
                     help="per arrival rate in the config-1 serving section (0 = skip)")
@@ -795,9 +796,9 @@ def parse_args(argv=None):
     ap.add_argument("--ooc26", type=int, default=0, help="run the scale-26 out-of-core section (minutes)")
     ap.add_argument("--ooc26-cap-ms", type=int, default=1000)
     ap.add_argument("--ooc26-small", type=int, default=20, help="4-vertex queries compared in and out of core")
-    ap.add_argument("--cpu-work-cap", type=int, default=200_000_000,
+    ap.add_argument("--cpu-work-cap", type=int, default=1_000_000_000,
                     help="scanned-arc cap per query of the CPU legs and the reference arm")
-    ap.add_argument("--ref-sample", type=int, default=4, help="queries per step of the reference arm (--impl reference)")
+    ap.add_argument("--ref-sample", type=int, default=2, help="queries per step of the reference arm (--impl reference)")
     args = ap.parse_args(argv)
     args.sizes = tuple(int(x) for x in args.sizes.split(",")) if args.sizes else MIX_SIZES
     d = DEFAULTS[args.workload]

@@ -323,6 +323,8 @@ typedef struct {
   int want_hash;
   uint64_t node_cap;
   volatile int *abort_flag;
+  const uint32_t *lastc;          /* count mode, a last level keyed by one neighbour only: per data vertex
+                                     its neighbours with that level's label and least degree (else null) */
   uint32_t f[OR_MAX_QV];          /* by level */
   uint64_t hsum[OR_MAX_QV + 1];   /* prefix sums of per-vertex hash terms */
 } or_walker;
@@ -332,6 +334,22 @@ static void walk(or_walker *w, uint32_t k) {
   const uint32_t u = p->order[k];
   const uint32_t par = w->f[p->parent[k]];
   const uint32_t last = (k + 1 == p->n);
+  if (last && w->lastc) {
+    /* The last level counted without listing it, as the reference's last
+       join step does (only the count of each row's extensions, in-core/lib/
+       join/src/join_trie.cu:1204): the parent's neighbours with the label
+       and degree, minus the earlier matches among them (injectivity). */
+    uint64_t c = w->lastc[par];
+    for (uint32_t j = 0; j < k; ++j) {
+      const uint32_t y = w->f[j];
+      if (w->lab[y] == p->label[k] && (uint32_t)(w->off[y + 1] - w->off[y]) >= p->qdeg[k] &&
+          has_arc(w->off, w->nbr, par, y))
+        --c;
+    }
+    w->count += c;
+    w->work += 1 + k;
+    return;
+  }
   w->work += w->off[par + 1] - w->off[par];
   if (w->node_cap && w->work > w->node_cap) { *w->abort_flag = 1; return; }
   if (*w->abort_flag) return;
@@ -381,12 +399,31 @@ int oracle_count(uint32_t nv, const uint64_t *off, const uint32_t *nbr, const ui
 #else
   nt = 1;
 #endif
+  /* count mode: a last level whose only backward neighbour is its parent is
+     counted from per-vertex neighbour counts instead of being listed */
+  uint32_t *lastc = NULL;
+  if (!want_hash && qn >= 2 && p.nback[qn - 1] == 0) {
+    lastc = (uint32_t *)malloc((size_t)nv * sizeof(uint32_t));
+    if (lastc) {
+      const uint32_t L = p.label[qn - 1], D = p.qdeg[qn - 1];
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(nt)
+      for (int64_t v = 0; v < (int64_t)nv; ++v) {
+        uint32_t c = 0;
+        for (uint64_t i = off[v]; i < off[v + 1]; ++i) {
+          const uint32_t x = nbr[i];
+          c += lab[x] == L && (uint32_t)(off[x + 1] - off[x]) >= D;
+        }
+        lastc[v] = c;
+      }
+    }
+  }
 #pragma omp parallel num_threads(nt) reduction(+ : count, hash, nodes)
   {
     or_walker w;
     w.off = off; w.nbr = nbr; w.lab = lab; w.p = &p;
     w.count = 0; w.hash = 0; w.nodes = 0; w.work = 0; w.want_hash = want_hash;
     w.node_cap = node_cap; w.abort_flag = &abort_flag;
+    w.lastc = lastc;
     w.hsum[0] = 0;
 #pragma omp for schedule(dynamic, 64)
     for (int64_t v = 0; v < (int64_t)nv; ++v) {
@@ -416,6 +453,7 @@ int oracle_count(uint32_t nv, const uint64_t *off, const uint32_t *nbr, const ui
     hash += w.hash;
     nodes += w.nodes;
   }
+  free(lastc);
   *count_out = count;
   if (hash_out) *hash_out = hash;
   if (nodes_out) *nodes_out = nodes;

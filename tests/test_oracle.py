@@ -165,3 +165,22 @@ def test_threaded_filter_and_tables_equal_the_checkers(threads):
                     o1, v1 = oracle.edge_table(g, cand[s], cand[t])
                     o2, v2 = oracle.edge_table_mt(g, cand[s], cand[t], threads=threads)
                     assert np.array_equal(o1, o2) and np.array_equal(v1, v2)
+
+
+def test_count_mode_last_level_shortcut_equals_listing():
+    """In count mode the oracle counts a last level keyed by one neighbour from
+    per-vertex neighbour counts (the reference's count-only last join step);
+    the count equals listing every embedding (hash mode) and brute force."""
+    import gem_b200 as gem
+    checked = 0
+    for sc in (6, 9):
+        g = oracle.set_labels(oracle.rmat(sc, 8, seed=0x77 + sc), 3, 0.0, seed=sc)
+        for k in (2, 3, 4, 5):
+            for q in oracle.gen_queries(g, k, 0, 8, seed=0x99 + 7 * k + sc):
+                a = oracle.count(g, q, want_hash=False)[0]
+                b = oracle.count(g, q, want_hash=True)[0]
+                assert a == b, (sc, k)
+                if sc == 6 and k <= 5:
+                    assert a == oracle.brute(g, q)[0]
+                checked += 1
+    assert checked >= 60
