@@ -64,7 +64,7 @@ class _Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("device_budget_bytes", C.c_uint64), ("pinned_budget_bytes", C.c_uint64),
                 ("ooc", C.c_int), ("time_cap_ms", C.c_uint32), ("index_kind", C.c_uint32),
                 ("admit_gb", C.c_uint32), ("ooc_part_kib", C.c_uint32), ("ooc_stream", C.c_uint32),
-                ("reserved", C.c_uint32 * 3)]
+                ("batch_lanes", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 class _OocStats(C.Structure):
@@ -372,13 +372,14 @@ class Context:
     """One GPU with a resident data graph (gem_ctx)."""
 
     def __init__(self, device=0, budget_bytes=0, time_cap_ms=0, index_kind=IDX_AUTO, ooc=False, pinned_bytes=0,
-                 admit_gb=0, ooc_part_kib=0, ooc_stream=0):
+                 admit_gb=0, ooc_part_kib=0, ooc_stream=0, batch_lanes=0):
         """ooc_part_kib / ooc_stream: out-of-core adjacency partition size (KiB, 0 = 16 MiB) and whether
         table builds stream partitions (0 = when the sources fill them enough, 1 = always, 2 = never)."""
         o = _Opts()
         o.admit_gb = admit_gb
         o.ooc_part_kib = ooc_part_kib
         o.ooc_stream = ooc_stream
+        o.batch_lanes = batch_lanes
         o.device = device
         o.device_budget_bytes = budget_bytes
         o.pinned_budget_bytes = pinned_bytes

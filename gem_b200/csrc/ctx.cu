@@ -180,12 +180,39 @@ extern "C" gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out) {
   return GEM_OK;
 }
 
+// A lane's own out-of-core staging: two buffers of the root's largest
+// partition, a copy stream and its events (the partition bounds on the
+// device are the root's).
+static gem_status lane_staging(gem_ctx *ctx, const gem_ctx *root) {
+  const uint64_t b_st = (root->ooc.max_part_bytes + 255) & ~255ull;
+  char *p = nullptr;
+  if (ctx->device_bytes + 2 * b_st > ctx->budget || cudaMalloc(&p, 2 * b_st) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->err = "out-of-core staging buffers of a lane do not fit the device budget";
+    return GEM_ERR_OOM;
+  }
+  ctx->part_mem = p;
+  ctx->part_bytes = 2 * b_st;
+  ctx->device_bytes += 2 * b_st;
+  ctx->d_part_v = root->d_part_v;
+  ctx->d_stage[0] = (uint32_t *)p;
+  ctx->d_stage[1] = (uint32_t *)(p + b_st);
+  CU(cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking));
+  for (int b = 0; b < 2; ++b) {
+    CU(cudaEventCreateWithFlags(&ctx->ev_ready[b], cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&ctx->ev_free[b], cudaEventDisableTiming));
+  }
+  ctx->ooc.partitions = root->ooc.partitions;
+  ctx->ooc.max_part_bytes = root->ooc.max_part_bytes;
+  return GEM_OK;
+}
+
 // Serving lane over root's resident graph: everything a wave runs on of its
 // own (stream, events, arena, control block, task queue, pinned staging),
 // the graph and its derived indexes borrowed, the tuned schedules copied.
 gem_status lane_create(gem_ctx *root, uint64_t budget, gem_ctx **out) {
   *out = nullptr;
-  if (!root->loaded || root->opts.ooc) return GEM_ERR_STATE;
+  if (!root->loaded) return GEM_ERR_STATE;
   std::unique_ptr<gem_ctx> c(new gem_ctx());
   gem_ctx *ctx = c.get();
   ctx->opts = root->opts;
@@ -206,8 +233,15 @@ gem_status lane_create(gem_ctx *root, uint64_t budget, gem_ctx **out) {
   ctx->wave_max_rows = root->wave_max_rows;
   ctx->ev_ref = root->ev_ref;
   ctx->ev_ref_recorded = root->ev_ref_recorded;
+  // out of core: the pinned adjacency and the partition bounds are the
+  // root's; the two staging buffers and the copy stream are the lane's own
+  ctx->pinned_nbr = nullptr;
+  ctx->host_nbr = root->host_nbr;
+  ctx->part_v = root->part_v;
+  ctx->part_a = root->part_a;
   c.release();
   gem_status st = cudaSetDevice(ctx->opts.device) == cudaSuccess ? exec_init(ctx) : GEM_ERR_CUDA;
+  if (st == GEM_OK && root->opts.ooc && !root->part_v.empty()) st = lane_staging(ctx, root);
   if (st != GEM_OK) {
     cudaGetLastError();
     gem_ctx_destroy(ctx);  // its own resources only: the graph is borrowed
@@ -223,6 +257,7 @@ static void free_graph(gem_ctx *ctx) {
     cudaFreeHost(ctx->pinned_nbr);
     ctx->pinned_nbr = nullptr;
   }
+  ctx->host_nbr = nullptr;
   if (ctx->part_mem) {
     cudaFree(ctx->part_mem);
     ctx->device_bytes -= ctx->part_bytes;
@@ -254,6 +289,18 @@ static void free_graph(gem_ctx *ctx) {
 
 // The batch lane (a second context over this context's graph) and the
 // budget it took; dropped before the graph changes or the context goes.
+// Adds a lane's out-of-core counters to its root's and clears them.
+void merge_ooc_stats(gem_ctx *root, gem_ctx *lane) {
+  root->ooc.waves_streamed += lane->ooc.waves_streamed;
+  root->ooc.waves_in_place += lane->ooc.waves_in_place;
+  root->ooc.parts_streamed += lane->ooc.parts_streamed;
+  root->ooc.bytes_streamed += lane->ooc.bytes_streamed;
+  root->ooc.waves_spilled += lane->ooc.waves_spilled;
+  root->ooc.bytes_spilled += lane->ooc.bytes_spilled;
+  lane->ooc.waves_streamed = lane->ooc.waves_in_place = lane->ooc.parts_streamed = 0;
+  lane->ooc.bytes_streamed = lane->ooc.waves_spilled = lane->ooc.bytes_spilled = 0;
+}
+
 void drop_batch_lane(gem_ctx *ctx) {
   if (!ctx->batch_lane) return;
   gem_ctx_destroy(ctx->batch_lane);
@@ -270,6 +317,7 @@ extern "C" void gem_ctx_destroy(gem_ctx *ctx) {
   cudaStreamSynchronize(ctx->s);
   ctx->arena.release(ctx);
   if (!ctx->borrowed_graph) free_graph(ctx);
+  else if (ctx->part_mem) cudaFree(ctx->part_mem);  // a lane's own staging buffers
   if (ctx->ev_ref && !ctx->borrowed_graph) cudaEventDestroy(ctx->ev_ref);
   destroy_join_graph(ctx->jgraph);
   if (ctx->d_ctl) cudaFree(ctx->d_ctl);
@@ -429,6 +477,7 @@ extern "C" gem_status gem_ctx_load_graph(gem_ctx *ctx, const gem_hgraph *hg) {
     void *h = nullptr;
     CU(cudaHostAlloc(&h, na ? 4ull * na : 4, cudaHostAllocMapped | cudaHostAllocPortable));
     ctx->pinned_nbr = h;
+    ctx->host_nbr = h;
     if (na) std::memcpy(h, hg->nbr.data(), 4ull * na);
     CU(cudaHostGetDevicePointer((void **)&d_nbr, h, 0));
     const gem_status pst = ooc_partitions(ctx, hg);
@@ -1099,7 +1148,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
       const int b = (int)(k++ & 1u);
       const uint64_t a0 = ctx->part_a[p], bytes = 4 * (ctx->part_a[p + 1] - a0);
       CU(cudaStreamWaitEvent(ctx->s_copy, ctx->ev_free[b], 0));
-      CU(cudaMemcpyAsync(ctx->d_stage[b], static_cast<const uint32_t *>(ctx->pinned_nbr) + a0, bytes,
+      CU(cudaMemcpyAsync(ctx->d_stage[b], static_cast<const uint32_t *>(ctx->host_nbr) + a0, bytes,
                          cudaMemcpyHostToDevice, ctx->s_copy));
       CU(cudaEventRecord(ctx->ev_ready[b], ctx->s_copy));
       CU(cudaStreamWaitEvent(ctx->s, ctx->ev_ready[b], 0));
@@ -1719,7 +1768,7 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
     }
   };
   gem_ctx *second = nullptr;
-  if (!ctx->opts.ooc && total_rows > ctx->wave_max_rows) {
+  if (ctx->opts.batch_lanes != 1 && total_rows > ctx->wave_max_rows) {
     if (!ctx->batch_lane) {
       // the graph's remaining budget, split evenly: the context's arena is
       // released so each lane grows its own within its half
@@ -1742,6 +1791,7 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
     worker(ctx);
     t.join();
     ctx->join_grid_div = 1;
+    merge_ooc_stats(ctx, second);
     if (!lane_err.empty() && ctx->err.empty()) ctx->err = lane_err;
   } else {
     worker(ctx);

@@ -125,7 +125,8 @@ struct gem_ctx {
   uint64_t vnh_bytes = 0;
   const uint64_t *vnh_off = nullptr;
   const uint32_t *vnh_slots = nullptr;
-  void *pinned_nbr = nullptr;        // out-of-core: mapped pinned adjacency
+  void *pinned_nbr = nullptr;        // out-of-core: mapped pinned adjacency (owned)
+  void *host_nbr = nullptr;          // the same, as the host-side source of partition copies (lanes borrow it)
   // out-of-core partition streaming: vertex ranges of at most ooc_part_kib
   // KiB of adjacency, two device staging buffers and a side copy stream
   std::vector<uint32_t> part_v;      // partition vertex bounds (partitions + 1)
@@ -179,6 +180,8 @@ struct gem_ctx {
 gem_status lane_create(gem_ctx *root, uint64_t budget, gem_ctx **out);
 // Destroys the context's batch lane, if any, and gives its budget back.
 void drop_batch_lane(gem_ctx *ctx);
+// Adds a lane's out-of-core counters to its root's and clears them.
+void merge_ooc_stats(gem_ctx *root, gem_ctx *lane);
 
 gem_status run_wave(gem_ctx *ctx, Wave &w, uint32_t threshold, int mode, uint32_t *emb_dev, uint64_t emb_cap);
 void wave_result(const gem_ctx *ctx, const Wave &w, size_t qi, gem_result *r);

@@ -9,8 +9,9 @@
 // stream, arena, control block and task queue).  While one lane's wave is on
 // the GPU the other lane takes the requests that arrived meanwhile, so their
 // work overlaps on the device; each lane's join grid takes half of the SMs'
-// blocks so that two joins fit side by side.  An out-of-core context serves
-// on one lane (its partition staging buffers are not shared).  Results are
+// blocks so that two joins fit side by side.  Out of core, each lane has
+// its own partition staging buffers and copy stream, so one lane's
+// partition copies run beside the other lane's join.  Results are
 // identical to gem_query_run's: every query of a wave has its own plan,
 // tables and counters.  While the server runs, only gem_submit and gem_poll
 // may be used on the context (other calls return GEM_ERR_STATE).
@@ -173,7 +174,10 @@ void server_shutdown(gem_ctx *ctx) {
   S->cv.notify_all();
   for (auto &t : S->th)
     if (t.joinable()) t.join();
-  for (size_t i = 1; i < S->lanes.size(); ++i) gem_ctx_destroy(S->lanes[i]);
+  for (size_t i = 1; i < S->lanes.size(); ++i) {
+    merge_ooc_stats(ctx, S->lanes[i]);
+    gem_ctx_destroy(S->lanes[i]);
+  }
   ctx->join_grid_div = 1;
   if (S->saved_budget) ctx->budget = S->saved_budget;
   delete S;
@@ -190,7 +194,7 @@ static gem_status server_start(gem_ctx *ctx) {
   const uint64_t room = ctx->budget > ctx->device_bytes ? ctx->budget - ctx->device_bytes : 0;
   S->budget = cap < room ? cap : room;
   S->lanes.push_back(ctx);
-  if (!ctx->opts.ooc) {
+  {
     gem_ctx *lane = nullptr;
     if (lane_create(ctx, room / 2, &lane) == GEM_OK) {
       S->saved_budget = ctx->budget;

@@ -143,7 +143,9 @@ typedef struct gem_opts {
   uint32_t ooc_stream;          /* out-of-core table builds: 0 = stream partitions when the wave's
                                    sources fill them enough, 1 = always stream, 2 = never (read the
                                    mapped adjacency in place) */
-  uint32_t reserved[3];
+  uint32_t batch_lanes;         /* in-core batches of more than one wave: 0 = run on two lanes (one
+                                   wave's join beside the next wave's table build), 1 = one lane */
+  uint32_t reserved[2];
 } gem_opts;
 
 gem_status gem_ctx_create(const gem_opts *opts, gem_ctx **out);

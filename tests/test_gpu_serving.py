@@ -69,3 +69,4 @@ def test_admission_estimate_bounds_wave_bytes():
                     ratios.append(est / r["arena_bytes"])
     assert len(ratios) >= 150
     assert float(np.median(ratios)) < 16.0, float(np.median(ratios))
+
