@@ -368,7 +368,7 @@ def run_gem(args):
     t_tab = tpass_ms / n_tab if n_tab else 0.0
     t_join = jms / n_joins if n_joins else 0.0
     roof_tab = roofline(tbytes / n_tab if n_tab else 0.0, t_tab, peak, peak_src,
-                        "table_src_kernel<count>+<write> (edge-table passes)",
+                        "table_vtx_kernel<count>+<write> (edge-table passes over vertex tiles)",
                         profiled_traffic("tables", args.workload, B))
     roof_join = roofline(jbytes / n_joins if n_joins else 0.0, t_join, peak, peak_src, "join_kernel<COUNT>",
                          profiled_traffic("join", args.workload, B))

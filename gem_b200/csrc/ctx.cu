@@ -1014,15 +1014,31 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   ST(aalloc(ctx, nkeys ? nkeys : 1, &d_tiles));
   ST(aalloc(ctx, nkeys + 1, &d_tp));
   ST(aalloc(ctx, scan_tmp_words(nkeys), &d_tmp));
-  ST(aalloc(ctx, src.size() + 1, &d_stb));
+  ST(aalloc(ctx, src.size() + 2, &d_stb));
   launch_key_tiles(ctx->g, d_src, (uint32_t)src.size(), nkeys, d_tiles, ctx->s);
   launch_scan(d_tiles, SCAN_U32, nkeys, d_tp, d_tmp, ctx->s);
   launch_source_tile_bases(d_src, (uint32_t)src.size(), nkeys, d_tp, d_stb, ctx->s);
-  std::vector<uint64_t> stb(src.size() + 1);
+  // Vertex tiles: which sources hold each vertex (the source membership
+  // columns, WS words per vertex) and the 32-arc tiles of every vertex that
+  // some source holds; the table passes walk those tiles once for all sources.
+  const uint32_t nv = ctx->g.nv;
+  const uint32_t WS = (uint32_t)((src.size() + 31) / 32);
+  uint32_t *d_srow, *d_S, *d_vtiles;
+  uint64_t *d_vtp, *d_tmp3;
+  ST(aalloc(ctx, src.size(), &d_srow));
+  CU(h2d(ctx, d_srow, src_row.data(), 4 * src_row.size()));
+  ST(aalloc(ctx, (uint64_t)nv * WS, &d_S));
+  ST(aalloc(ctx, nv ? nv : 1, &d_vtiles));
+  ST(aalloc(ctx, (uint64_t)nv + 1, &d_vtp));
+  ST(aalloc(ctx, scan_tmp_words(nv), &d_tmp3));
+  launch_row_columns(w.d_bits, w.nwords, d_srow, (uint32_t)src.size(), WS, nv, d_S, d_vtiles, ctx->g.deg, ctx->s);
+  launch_scan(d_vtiles, SCAN_U32, nv, d_vtp, d_tmp3, ctx->s);
+  CU(cudaMemcpyAsync(d_stb + src.size() + 1, d_vtp + nv, 8, cudaMemcpyDeviceToDevice, ctx->s));
+  std::vector<uint64_t> stb(src.size() + 2);
   CU(d2h_sync(ctx, stb.data(), d_stb, 8 * stb.size()));
   CU(cudaGetLastError());
-  // edges, grouped by source so that one pass over a source's tiles serves
-  // all its tables
+  const uint64_t vtiles = stb[src.size() + 1];
+  // edges, grouped by source: a source's tables are one range of the edges
   struct EdgeReq {
     uint32_t s, qi, j, k;
   };
@@ -1043,6 +1059,8 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   // a table is keyed by its source row and filtered by its target row: queries
   // (or twin query vertices) that need the same pair share one table
   std::map<std::pair<uint32_t, uint32_t>, uint32_t> edge_by_rows;
+  std::vector<uint32_t> tgt_row;  // the target rows, one membership column bit each
+  std::vector<int> row_tcol(w.nrows, -1);
   for (const EdgeReq &rq : reqs) {
     const Plan &p = w.plan[rq.qi];
     const uint32_t tgt = w.row_of[rq.qi][p.order[rq.k]];
@@ -1058,8 +1076,12 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
     TabEdge e;
     e.src = rq.s;
     e.flags = flags;
-    e.rb_w = w.d_rb + (uint64_t)tgt * w.nwords;
-    e.bits_w = w.d_bits + (uint64_t)tgt * w.nwords;
+    if (row_tcol[tgt] < 0) {
+      row_tcol[tgt] = (int)tgt_row.size();
+      tgt_row.push_back(tgt);
+    }
+    e.tcol = (uint32_t)row_tcol[tgt];
+    e.pad = 0;
     e.tile_base = tiles;
     e.ntiles = stb[rq.s + 1] - stb[rq.s];
     e.off_base = offs;
@@ -1072,12 +1094,6 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
     edge.push_back(e);
   }
   const uint64_t src_tiles = stb[src.size()];
-  uint32_t *d_sedge, *d_tkey, *d_tsrc;
-  ST(aalloc(ctx, sedge.size(), &d_sedge));
-  CU(h2d(ctx, d_sedge, sedge.data(), sedge.size() * 4));
-  ST(aalloc(ctx, src_tiles ? src_tiles : 1, &d_tkey));
-  ST(aalloc(ctx, src_tiles ? src_tiles : 1, &d_tsrc));
-  launch_tile_keys(d_src, (uint32_t)src.size(), nkeys, d_tp, d_tkey, d_tsrc, ctx->s);
   uint64_t *d_offs;
   ST(aalloc(ctx, offs, &d_offs));
   for (auto &e : edge) e.offsets = d_offs + e.off_base;
@@ -1089,54 +1105,76 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   ST(aalloc(ctx, tiles ? tiles : 1, &d_mask));
   ST(aalloc(ctx, tiles + 1, &d_vp));
   ST(aalloc(ctx, scan_tmp_words(tiles), &d_tmp2));
-  // Out-of-core: group the tiles by adjacency partition; stream the
-  // partitions they touch when those are filled enough (their bytes at most
-  // twice what the tiles would read from the mapped adjacency), else read in
-  // place.
+  // the target membership columns, the tile -> vertex map, and the sources
+  // and tables as the passes read them
+  const uint32_t WT = (uint32_t)((tgt_row.size() + 31) / 32);
+  if (!table_vtx_fits(WT)) {
+    ctx->err = "too many edge-table target rows in one wave";
+    return GEM_ERR_LIMIT;
+  }
+  uint32_t *d_trow, *d_B, *d_vt;
+  ST(aalloc(ctx, tgt_row.size(), &d_trow));
+  CU(h2d(ctx, d_trow, tgt_row.data(), 4 * tgt_row.size()));
+  ST(aalloc(ctx, (uint64_t)nv * WT, &d_B));
+  launch_row_columns(w.d_bits, w.nwords, d_trow, (uint32_t)tgt_row.size(), WT, nv, d_B, nullptr, nullptr, ctx->s);
+  ST(aalloc(ctx, vtiles ? vtiles : 1, &d_vt));
+  launch_vertex_tile_map(d_vtp, nv, d_vt, ctx->s);
+  std::vector<VSrc> vs(src.size());
+  for (size_t i = 0; i < src.size(); ++i)
+    vs[i] = VSrc{w.d_rb + (uint64_t)src_row[i] * w.nwords, src[i].key_base, stb[i], sedge[2 * i], sedge[2 * i + 1]};
+  std::vector<VEdge> ve(edge.size());
+  for (size_t i = 0; i < edge.size(); ++i) ve[i] = VEdge{edge[i].tile_base, edge[i].tcol, edge[i].flags};
+  VSrc *d_vs;
+  VEdge *d_ve;
+  ST(aalloc(ctx, vs.size(), &d_vs));
+  CU(h2d(ctx, d_vs, vs.data(), vs.size() * sizeof(VSrc)));
+  ST(aalloc(ctx, ve.size(), &d_ve));
+  CU(h2d(ctx, d_ve, ve.data(), ve.size() * sizeof(VEdge)));
+  // Out-of-core: the vertex tiles of a partition (a vertex range) are one
+  // range of the tile order.  Stream the partitions that hold tiles when
+  // they are filled enough (their bytes at most twice what the tiles would
+  // read from the mapped adjacency), else read in place.
   const uint32_t nparts = ctx->part_v.empty() ? 0u : (uint32_t)ctx->part_v.size() - 1;
   std::vector<uint64_t> pstart;
-  uint32_t *d_tord = nullptr;
   bool streamed = false;
-  if (ctx->opts.ooc && nparts && ctx->opts.ooc_stream != 2 && src_tiles && src_tiles < (1ull << 32)) {
-    uint32_t *d_tpart, *d_hist;
-    ST(aalloc(ctx, src_tiles, &d_tpart));
-    ST(aalloc(ctx, nparts, &d_hist));
-    CU(cudaMemsetAsync(d_hist, 0, 4ull * nparts, ctx->s));
-    launch_tile_partition(d_src, d_tkey, d_tsrc, src_tiles, ctx->d_part_v, nparts, d_tpart, d_hist, ctx->s);
-    std::vector<uint32_t> hist(nparts);
-    CU(d2h_sync(ctx, hist.data(), d_hist, 4ull * nparts));
+  if (ctx->opts.ooc && nparts && ctx->opts.ooc_stream != 2 && vtiles) {
+    uint64_t *d_pb;
+    ST(aalloc(ctx, nparts + 1, &d_pb));
+    launch_gather_u64(d_vtp, ctx->d_part_v, nparts + 1, d_pb, ctx->s);
+    pstart.assign(nparts + 1, 0);
+    CU(d2h_sync(ctx, pstart.data(), d_pb, 8ull * (nparts + 1)));
     uint64_t need = 0;
     for (uint32_t p = 0; p < nparts; ++p)
-      if (hist[p]) need += 4 * (ctx->part_a[p + 1] - ctx->part_a[p]);
-    streamed = ctx->opts.ooc_stream == 1 || need <= 2 * 128 * src_tiles;
-    if (streamed) {
-      pstart.assign(nparts + 1, 0);
-      for (uint32_t p = 0; p < nparts; ++p) pstart[p + 1] = pstart[p] + hist[p];
-      std::vector<uint32_t> cursor(nparts);
-      for (uint32_t p = 0; p < nparts; ++p) cursor[p] = (uint32_t)pstart[p];
-      CU(h2d(ctx, d_hist, cursor.data(), 4ull * nparts));
-      ST(aalloc(ctx, src_tiles, &d_tord));
-      launch_tile_scatter(d_tpart, src_tiles, nparts, d_hist, d_tord, ctx->s);
-    }
+      if (pstart[p + 1] > pstart[p]) need += 4 * (ctx->part_a[p + 1] - ctx->part_a[p]);
+    streamed = ctx->opts.ooc_stream == 1 || need <= 2 * 128 * vtiles;
   }
   if (ctx->opts.ooc) ++(streamed ? ctx->ooc.waves_streamed : ctx->ooc.waves_in_place);
-  // One table pass (count or write) over every tile: in place, or partition
-  // by partition with the copy of the next partition (side stream, the other
-  // staging buffer) overlapping the kernel of the current one.
+  // One table pass (count or write) over every vertex tile: in place, or
+  // partition by partition with the copy of the next partition (side
+  // stream, the other staging buffer) overlapping the kernel of the current one.
   auto table_pass = [&](bool write) -> gem_status {
-    TabPass P;
+    VPass P;
+    std::memset(&P, 0, sizeof P);
     P.off = ctx->g.off;
     P.nbr = ctx->g.nbr;
     P.arc_shift = 0;
-    P.tord = nullptr;
     P.t0 = 0;
-    P.t1 = src_tiles;
+    P.t1 = vtiles;
+    P.vt = d_vt;
+    P.vtp = d_vtp;
+    P.S = d_S;
+    P.WS = WS;
+    P.WT = WT;
+    P.B = d_B;
+    P.vsrc = d_vs;
+    P.vedge = d_ve;
+    P.tp = d_tp;
+    P.mask = d_mask;
+    P.vp = d_vp;
+    P.values = w.d_values;
+    P.vkey = w.d_vkey;
     if (!streamed) {
-      if (write)
-        launch_table_write(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, d_vp, w.d_values, w.d_vkey,
-                           ctx->s);
-      else
-        launch_table_count(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, ctx->s);
+      launch_table_vtx(P, write, ctx->s);
       return GEM_OK;
     }
     // a staging buffer is free once the main stream has passed what used it
@@ -1154,14 +1192,9 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
       CU(cudaStreamWaitEvent(ctx->s, ctx->ev_ready[b], 0));
       P.nbr = ctx->d_stage[b];
       P.arc_shift = a0;
-      P.tord = d_tord;
       P.t0 = pstart[p];
       P.t1 = pstart[p + 1];
-      if (write)
-        launch_table_write(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, d_vp, w.d_values, w.d_vkey,
-                           ctx->s);
-      else
-        launch_table_count(P, d_src, d_sedge, d_edge, d_tp, d_tkey, d_tsrc, d_mask, ctx->s);
+      launch_table_vtx(P, write, ctx->s);
       CU(cudaEventRecord(ctx->ev_free[b], ctx->s));
       ctx->ooc.parts_streamed += 1;
       ctx->ooc.bytes_streamed += bytes;
@@ -1211,10 +1244,14 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   w.edges = edge;
   w.table_values = nvals;
   w.table_tiles = tiles;
-  // algorithmic bytes: per tile the 32 neighbour ids (count pass) plus the
-  // membership words, the mask word written and read, the position word,
-  // values written with their ids re-read, and the offsets.
-  w.bytes_tables = tiles * (32ull * 4 + 32ull * 8 + 4 + 4 + 8) + nvals * (4 + 4) + offs * 8 + nkeys * (4 + 8 + 4);
+  // algorithmic bytes of the two passes: per vertex tile (each pass) its
+  // offsets, 32 neighbour ids and source column, and (count) the 32 target
+  // columns; per tile of a source (each pass) the rank word and tile base;
+  // per table tile the mask written and read and the value position; per
+  // value its id (and key position); the offsets; per key its tile count
+  // and scan.
+  w.bytes_tables = 2 * vtiles * (16 + 32ull * 4 + 4ull * WS) + vtiles * 32ull * 4 * WT + 2 * src_tiles * 16 +
+                   tiles * (4 + 4 + 8) + nvals * (key_map ? 8 : 4) + offs * 8 + nkeys * (4 + 8 + 4);
   return GEM_OK;
 }
 

@@ -5,10 +5,15 @@
 // kernels of construct_kernel.cu:1183-1340) runs, per directed query edge, a
 // count kernel over 32-neighbour tiles, a CUB scan over the tiles of the
 // *whole* data graph, a max kernel and a write kernel, with host syncs in
-// between.  Here the tile space is compacted to the arcs of C(u) only, all
-// edges of a wave share each launch, every warp owns a fixed run of tiles (so
-// hub vertices do not serialise on one warp), and membership in C(w) is one
-// bit of w's rank bitmap.
+// between.  Here all tables of a wave share each launch, and the passes walk
+// the data graph's vertex tiles (32 arcs of one vertex) once: each tile
+// serves every source row whose candidates hold its vertex (in a batch of
+// queries a vertex is a candidate of many rows), and membership of an arc's
+// target in every target row is one word of that target's membership
+// column, staged in shared memory.  The tables keep the per-source layout
+// (a key's values at the key's tiles of its source), so the offsets, the
+// scans and the join see the same tables as a pass over each source would
+// write.
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -64,128 +69,216 @@ void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nk
   source_tile_bases_kernel<<<(nsrc + 256) / 256, 256, 0, s>>>(d_src, nsrc, nkeys, tp, out);
 }
 
-// Tile t of the flattened source-tile space (the 32-arc tiles of every key of
-// every source): the key it belongs to and its source.
-__global__ void tile_keys_kernel(const TabSource *__restrict__ src, uint32_t nsrc, uint64_t nkeys,
-                                 const uint64_t *__restrict__ tp, uint32_t *__restrict__ tkey,
-                                 uint32_t *__restrict__ tsrc) {
-  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nkeys; k += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t s = find_src(src, nsrc, k);
-    for (uint64_t t = tp[k], e = tp[k + 1]; t < e; ++t) {
-      tkey[t] = (uint32_t)k;
-      tsrc[t] = s;
+// Membership columns: out[v * W + c] holds, in bit b, whether vertex v is in
+// row rows[32c + b] (bits: the wave's membership bit rows, 32 vertices per
+// word).  One block per 32-vertex word j: each warp transposes 32 rows x 32
+// vertices with 32 ballots.  With vtiles, vtiles[v] = ceil(deg(v) / 32) for a
+// vertex in at least one of the rows, else 0.
+__global__ void __launch_bounds__(256) row_columns_kernel(const uint32_t *__restrict__ bits, uint32_t nwords,
+                                                          const uint32_t *__restrict__ rows, uint32_t nrows,
+                                                          uint32_t W, uint32_t nv, uint32_t *__restrict__ out,
+                                                          uint32_t *__restrict__ vtiles,
+                                                          const uint32_t *__restrict__ deg) {
+  __shared__ uint32_t any[32];
+  const uint32_t lane = dev::lane_id(), warp = threadIdx.x >> 5;
+  for (uint32_t j = blockIdx.x; j < nwords; j += gridDim.x) {
+    if (threadIdx.x < 32) any[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t v = j * 32u + lane;
+    uint32_t seen = 0;
+    for (uint32_t c = warp; c < W; c += blockDim.x >> 5) {
+      const uint32_t r = c * 32u + lane;
+      const uint32_t word = r < nrows ? __ldg(bits + (uint64_t)__ldg(rows + r) * nwords + j) : 0u;
+      uint32_t col = 0;
+#pragma unroll
+      for (uint32_t b = 0; b < 32; ++b) {
+        const uint32_t m = __ballot_sync(dev::FULL, (word >> b) & 1u);
+        if (lane == b) col = m;
+      }
+      if (v < nv) out[(uint64_t)v * W + c] = col;
+      seen |= col;
     }
+    if (vtiles) {
+      if (seen) atomicOr(any + lane, 1u);
+      __syncthreads();
+      if (warp == 0 && v < nv) vtiles[v] = any[lane] ? (__ldg(deg + v) + 31u) >> 5 : 0u;
+    }
+    __syncthreads();  // any[] is reset by the next word
   }
 }
 
-void launch_tile_keys(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp, uint32_t *tkey,
-                      uint32_t *tsrc, cudaStream_t s) {
-  if (nkeys == 0) return;
-  uint64_t blocks = (nkeys + 255) / 256;
-  if (blocks > 148ull * 32) blocks = 148ull * 32;
+void launch_row_columns(const uint32_t *bits, uint32_t nwords, const uint32_t *rows, uint32_t nrows, uint32_t W,
+                        uint32_t nv, uint32_t *out, uint32_t *vtiles, const uint32_t *deg, cudaStream_t s) {
+  if (nwords == 0) return;
+  uint32_t blocks = nwords < 148u * 16 ? nwords : 148u * 16;
   count_launch();
-  tile_keys_kernel<<<(uint32_t)blocks, 256, 0, s>>>(d_src, nsrc, nkeys, tp, tkey, tsrc);
+  row_columns_kernel<<<blocks, 256, 0, s>>>(bits, nwords, rows, nrows, W, nv, out, vtiles, deg);
 }
 
-// One warp per TILE_UNROLL consecutive source tiles: the tiles' key, vertex,
-// offsets and neighbour loads are independent and overlap; each tile is then
-// tested against (count) or copied for (write) every edge of its source, so
-// a source's adjacency is read once however many tables it keys.  The warps
-// cover positions [t0, t1) of the tile order `tord` (identity when null), and
-// a key's arcs are read at nbr[arc - arc_shift]: the resident (or mapped)
-// adjacency with shift 0, or a streamed partition that starts at arc_shift.
-constexpr int TILE_UNROLL = 4;
+// vt[t] = v for every tile t in [vtp[v], vtp[v + 1]).
+__global__ void vertex_tile_map_kernel(const uint64_t *__restrict__ vtp, uint32_t nv, uint32_t *__restrict__ vt) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    for (uint64_t t = __ldg(vtp + v), e = __ldg(vtp + v + 1); t < e; ++t) vt[t] = v;
+}
+
+void launch_vertex_tile_map(const uint64_t *vtp, uint32_t nv, uint32_t *vt, cudaStream_t s) {
+  if (nv == 0) return;
+  uint32_t blocks = (nv + 255) / 256;
+  if (blocks > 148u * 16) blocks = 148u * 16;
+  count_launch();
+  vertex_tile_map_kernel<<<blocks, 256, 0, s>>>(vtp, nv, vt);
+}
+
+__global__ void gather_u64_kernel(const uint64_t *__restrict__ a, const uint32_t *__restrict__ idx, uint32_t n,
+                                  uint64_t *__restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = __ldg(a + __ldg(idx + i));
+}
+
+void launch_gather_u64(const uint64_t *a, const uint32_t *idx, uint32_t n, uint64_t *out, cudaStream_t s) {
+  if (n == 0) return;
+  count_launch();
+  gather_u64_kernel<<<(n + 255) / 256, 256, 0, s>>>(a, idx, n, out);
+}
+
+// Position of the (r + 1)-th set bit of m (r < popc(m)).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t r) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t w = 16; w >= 1; w >>= 1) {
+    const uint32_t low = __popc(m & ((1u << w) - 1u));
+    if (r >= low) {
+      r -= low;
+      m >>= w;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
+// The table passes over vertex tiles.  One warp per tile (32 arcs of one
+// vertex v): the arcs are read once for every source whose candidates hold
+// v.  Those sources are the set bits of v's source column; the warp takes
+// them 32 at a time, one per lane, and each lane computes its source's key
+// position of v (rank bitmap) and tile index (tp).  The tables of those
+// sources are then flattened into (source, table) pairs, again one per
+// lane, 32 at a time:
+//   count: each lane tests its table's target column bit (tcol) for the 32
+//          arcs of the tile (the warp stages the arcs' target columns in
+//          shared memory, one column per arc) and writes the tile's mask;
+//   write: each lane reads its pair's mask and value position into a
+//          per-warp record; then for each record the lanes, one per arc,
+//          write the arcs whose bit is set (and the key position) at the
+//          value position plus their rank in the mask.
+// The mask and value positions are those of the source's own tile order
+// (mask[tile_base + lt], lt = the tile's index among the source's tiles), so
+// both passes lay out every table exactly as a pass over the sources would.
+struct VRec {
+  uint64_t vb;  // first value position of the pair's tile
+  uint32_t m;   // the tile's mask
+  uint32_t kf;  // key position to record, or 0xFFFFFFFF (no key map)
+};
 
 template <bool WRITE>
-__global__ void __launch_bounds__(256) table_src_kernel(TabPass P, const TabSource *__restrict__ srcs,
-                                                        const uint32_t *__restrict__ sedge,
-                                                        const TabEdge *__restrict__ edges,
-                                                        const uint64_t *__restrict__ tp,
-                                                        const uint32_t *__restrict__ tkey,
-                                                        const uint32_t *__restrict__ tsrc,
-                                                        uint32_t *__restrict__ mask, const uint64_t *__restrict__ vp,
-                                                        uint32_t *__restrict__ values, uint32_t *__restrict__ vkey) {
-  const uint32_t lane = dev::lane_id();
+__global__ void __launch_bounds__(256) table_vtx_kernel(VPass P) {
+  extern __shared__ uint32_t stage[];  // count: 32 target columns per warp
+  __shared__ VRec rec[8][32];          // write: the pairs of one round
+  const uint32_t lane = dev::lane_id(), warp = threadIdx.x >> 5;
   const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t base = P.t0 + (blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * TILE_UNROLL;
-       base < P.t1; base += nwarps * TILE_UNROLL) {
-    uint32_t x[TILE_UNROLL], sx[TILE_UNROLL], kx[TILE_UNROLL];
-    uint64_t lt[TILE_UNROLL];
-    bool xv[TILE_UNROLL];
-#pragma unroll
-    for (int i = 0; i < TILE_UNROLL; ++i) {
-      const bool tv = base + i < P.t1;
-      const uint64_t t = !tv ? 0ull : P.tord ? (uint64_t)__ldg(P.tord + base + i) : base + i;
-      const uint32_t k = tv ? __ldg(tkey + t) : 0u, sidx = tv ? __ldg(tsrc + t) : 0u;
-      const uint64_t kb = srcs[sidx].key_base;
-      const uint32_t *keys = srcs[sidx].keys;
-      const uint32_t v = tv ? __ldg(keys + (k - kb)) : 0u;
-      const uint64_t tk = tv ? __ldg(tp + k) : 0ull, stb = tv ? __ldg(tp + kb) : 0ull;
-      const uint64_t a0 = tv ? __ldg(P.off + v) : 0ull, a1 = tv ? __ldg(P.off + v + 1) : 0ull;
-      const uint64_t arc = a0 + (t - tk) * 32 + lane;
-      sx[i] = sidx;
-      kx[i] = (uint32_t)(k - kb);  // the key's position in its source's candidate list
-      lt[i] = t - stb;  // the tile's index among its source's tiles
-      xv[i] = tv && arc < a1;
-      x[i] = xv[i] ? __ldg(P.nbr + (arc - P.arc_shift)) : 0u;
+  for (uint64_t t = P.t0 + blockIdx.x * (uint64_t)(blockDim.x >> 5) + warp; t < P.t1; t += nwarps) {
+    const uint32_t v = __ldg(P.vt + t);
+    const uint64_t c = t - __ldg(P.vtp + v);
+    const uint64_t a0 = __ldg(P.off + v), arc = a0 + c * 32u + lane;
+    const uint64_t a1 = __ldg(P.off + v + 1);
+    const bool valid = arc < a1;
+    const uint32_t nvalid = a1 - a0 - c * 32u < 32u ? (uint32_t)(a1 - a0 - c * 32u) : 32u;  // valid lanes: a prefix
+    const uint32_t x = valid ? __ldg(P.nbr + (arc - P.arc_shift)) : 0u;
+    if (!WRITE) {
+      __syncwarp();  // the previous tile's reads of the stage are done
+      for (uint32_t l = 0; l < nvalid; ++l) {
+        const uint32_t xl = __shfl_sync(dev::FULL, x, l);
+        uint32_t *dst = stage + ((uint64_t)warp * 32u + l) * P.WTp;
+        for (uint32_t i = lane; i < P.WT; i += 32) dst[i] = __ldg(P.B + (uint64_t)xl * P.WT + i);
+      }
+      __syncwarp();
     }
-    // Common case: the warp's tiles all belong to one source (a source has
-    // many tiles).  Then each table of the source is read once for all of
-    // them, and its TILE_UNROLL membership probes (count) or mask / position
-    // loads (write) are issued together.
-    bool same = base + TILE_UNROLL <= P.t1;
+    const uint32_t *sv = P.S + (uint64_t)v * P.WS;
+    for (uint32_t wb = 0; wb < P.WS; wb += 32) {
+      const uint32_t word = wb + lane < P.WS ? __ldg(sv + wb + lane) : 0u;
+      const uint32_t cnt = __popc(word);
+      uint32_t incl = cnt;
 #pragma unroll
-    for (int i = 1; i < TILE_UNROLL; ++i) same = same && sx[i] == sx[0];
-    if (same) {
-      const uint32_t e0 = __ldg(sedge + 2 * sx[0]), ne = __ldg(sedge + 2 * sx[0] + 1);
-      for (uint32_t e = e0; e < e0 + ne; ++e) {
-        const uint64_t tb = edges[e].tile_base;
-        if (!WRITE) {
-          const uint32_t *bw = edges[e].bits_w;
-          bool hit[TILE_UNROLL];
+      for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(dev::FULL, incl, d);
+        if (lane >= d) incl += y;
+      }
+      const uint32_t total = __shfl_sync(dev::FULL, incl, 31);
+      for (uint32_t b = 0; b < total; b += 32) {
+        // lane i takes the (b + i)-th source of this word range: the first
+        // lane j whose inclusive count exceeds it holds it
+        const uint32_t q = b + lane;
+        uint32_t j = 0;
 #pragma unroll
-          for (int i = 0; i < TILE_UNROLL; ++i) hit[i] = xv[i] && ((__ldg(bw + (x[i] >> 5)) >> (x[i] & 31u)) & 1u);
+        for (uint32_t step = 16; step >= 1; step >>= 1)
+          if (__shfl_sync(dev::FULL, incl, j + step - 1) <= q) j += step;
+        const uint32_t wj = __shfl_sync(dev::FULL, word, j);
+        const uint32_t exj = __shfl_sync(dev::FULL, incl - cnt, j);
+        uint32_t k = 0, e0 = 0, ne = 0;
+        uint64_t lt = 0;
+        if (q < total) {
+          const VSrc &src = P.vsrc[(wb + j) * 32u + nth_set_bit(wj, q - exj)];
+          const uint64_t rw = __ldg(src.rb + (v >> 5));
+          k = (uint32_t)(rw >> 32) + __popc((uint32_t)rw & ((1u << (v & 31u)) - 1u));
+          lt = __ldg(P.tp + src.key_base + k) - src.stb + c;
+          e0 = src.e0;
+          ne = src.ne;
+        }
+        // the (source, table) pairs of these sources, one per lane
+        uint32_t pin = ne;
 #pragma unroll
-          for (int i = 0; i < TILE_UNROLL; ++i) {
-            const uint32_t m = __ballot_sync(dev::FULL, hit[i]);
-            if (lane == 0) mask[tb + lt[i]] = m;
-          }
-        } else {
-          uint32_t m[TILE_UNROLL];
-          uint64_t vb[TILE_UNROLL];
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+          const uint32_t y = __shfl_up_sync(dev::FULL, pin, d);
+          if (lane >= d) pin += y;
+        }
+        const uint32_t npairs = __shfl_sync(dev::FULL, pin, 31);
+        for (uint32_t pb = 0; pb < npairs; pb += 32) {
+          const uint32_t p = pb + lane;
+          uint32_t o = 0;  // the source lane of pair p
 #pragma unroll
-          for (int i = 0; i < TILE_UNROLL; ++i) {
-            m[i] = __ldg(mask + tb + lt[i]);
-            vb[i] = __ldg(vp + tb + lt[i]);
-          }
-          const bool km = (edges[e].flags & TAB_KEY_MAP) != 0;
-#pragma unroll
-          for (int i = 0; i < TILE_UNROLL; ++i)
-            if (m[i] & (1u << lane)) {
-              const uint64_t pos = vb[i] + __popc(m[i] & ((1u << lane) - 1u));
-              values[pos] = x[i];
-              if (km) vkey[pos] = kx[i];
+          for (uint32_t step = 16; step >= 1; step >>= 1)
+            if (__shfl_sync(dev::FULL, pin, o + step - 1) <= p) o += step;
+          const uint32_t u = p - (__shfl_sync(dev::FULL, pin, o) - __shfl_sync(dev::FULL, ne, o));
+          const uint32_t pe = __shfl_sync(dev::FULL, e0, o) + u;
+          const uint64_t plt = __shfl_sync(dev::FULL, lt, o);
+          const uint32_t pk = __shfl_sync(dev::FULL, k, o);
+          const bool have = p < npairs;
+          const VEdge E = have ? P.vedge[pe] : VEdge{0, 0, 0};
+          const uint64_t maddr = E.tile_base + plt;
+          if (!WRITE) {
+            const uint32_t *col = stage + (uint64_t)warp * 32u * P.WTp + (E.tcol >> 5);
+            const uint32_t sh = E.tcol & 31u;
+            uint32_t m = 0;
+            for (uint32_t l = 0; l < nvalid; ++l) m |= ((col[l * P.WTp] >> sh) & 1u) << l;
+            if (have) P.mask[maddr] = m;
+          } else {
+            VRec r{0, 0, 0xFFFFFFFFu};
+            if (have) {
+              r.m = __ldg(P.mask + maddr);
+              r.vb = __ldg(P.vp + maddr);
+              if (E.flags & TAB_KEY_MAP) r.kf = pk;
             }
-        }
-      }
-      continue;
-    }
-#pragma unroll
-    for (int i = 0; i < TILE_UNROLL; ++i) {
-      if (base + i >= P.t1) break;  // the same in every lane
-      const uint32_t e0 = __ldg(sedge + 2 * sx[i]), ne = __ldg(sedge + 2 * sx[i] + 1);
-      for (uint32_t e = e0; e < e0 + ne; ++e) {
-        const uint64_t et = edges[e].tile_base + lt[i];
-        if (!WRITE) {
-          const bool hit = xv[i] && ((__ldg(edges[e].bits_w + (x[i] >> 5)) >> (x[i] & 31u)) & 1u);
-          const uint32_t m = __ballot_sync(dev::FULL, hit);
-          if (lane == 0) mask[et] = m;
-        } else {
-          const uint32_t m = __ldg(mask + et);
-          if (m & (1u << lane)) {
-            const uint64_t pos = __ldg(vp + et) + __popc(m & ((1u << lane) - 1u));
-            values[pos] = x[i];
-            if (edges[e].flags & TAB_KEY_MAP) vkey[pos] = kx[i];
+            __syncwarp();  // the previous round's records are read
+            rec[warp][lane] = r;
+            __syncwarp();
+            const uint32_t nr = npairs - pb < 32u ? npairs - pb : 32u;
+            for (uint32_t i = 0; i < nr; ++i) {
+              const VRec ri = rec[warp][i];
+              if ((ri.m >> lane) & 1u) {
+                const uint64_t pos = ri.vb + __popc(ri.m & ((1u << lane) - 1u));
+                P.values[pos] = x;
+                if (ri.kf != 0xFFFFFFFFu) P.vkey[pos] = ri.kf;
+              }
+            }
           }
         }
       }
@@ -193,130 +286,30 @@ __global__ void __launch_bounds__(256) table_src_kernel(TabPass P, const TabSour
   }
 }
 
-static uint32_t src_tile_blocks(uint64_t ntile) {
-  uint64_t warps = (ntile + TILE_UNROLL - 1) / TILE_UNROLL;
-  uint64_t blocks = (warps + 7) / 8;
-  if (blocks > 148ull * 32) blocks = 148ull * 32;
-  if (blocks == 0) blocks = 1;
-  return (uint32_t)blocks;
+// Warps per block of the count pass: each warp stages 32 target columns of
+// WTp words; blocks stay within 96 KB of shared memory so that two fit an SM.
+static uint32_t count_warps(uint32_t WTp) {
+  const uint64_t per_warp = 32ull * WTp * 4;
+  const uint64_t w = (96ull << 10) / per_warp;
+  return w > 8 ? 8u : w < 1 ? 1u : (uint32_t)w;
 }
 
-void launch_table_count(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint32_t *mask,
-                        cudaStream_t s) {
-  if (P.t1 <= P.t0) return;
+bool table_vtx_fits(uint32_t WT) { return 32ull * (WT | 1u) * 4 <= (200ull << 10); }
+
+void launch_table_vtx(const VPass &P0, bool write, cudaStream_t s) {
+  if (P0.t1 <= P0.t0) return;
+  VPass P = P0;
+  P.WTp = P.WT | 1u;  // odd: the lanes' columns fall in distinct banks
+  const uint32_t warps = write ? 8u : count_warps(P.WTp);
+  uint64_t blocks = (P.t1 - P.t0 + warps - 1) / warps;
+  if (blocks > 148ull * 16) blocks = 148ull * 16;
   count_launch();
-  table_src_kernel<false><<<src_tile_blocks(P.t1 - P.t0), 256, 0, s>>>(P, d_src, sedge, d_edge, tp, tkey, tsrc, mask,
-                                                                        nullptr, nullptr, nullptr);
-}
-
-void launch_table_write(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, const uint32_t *mask,
-                        const uint64_t *vp, uint32_t *values, uint32_t *vkey, cudaStream_t s) {
-  if (P.t1 <= P.t0) return;
-  count_launch();
-  table_src_kernel<true><<<src_tile_blocks(P.t1 - P.t0), 256, 0, s>>>(P, d_src, sedge, d_edge, tp, tkey, tsrc,
-                                                                       const_cast<uint32_t *>(mask), vp, values, vkey);
-}
-
-// Partition of every source tile (by its key vertex: the partition whose
-// vertex range [part_v[p], part_v[p + 1]) holds it) and the tiles per
-// partition.  Partitions are few (adjacency bytes / partition size), so the
-// counts go through a shared-memory histogram when they fit one.
-__global__ void tile_partition_kernel(const TabSource *__restrict__ srcs, const uint32_t *__restrict__ tkey,
-                                      const uint32_t *__restrict__ tsrc, uint64_t ntile,
-                                      const uint32_t *__restrict__ part_v, uint32_t nparts,
-                                      uint32_t *__restrict__ tpart, uint32_t *__restrict__ hist) {
-  __shared__ uint32_t sh[TILE_PART_SMEM];
-  const bool local = nparts <= TILE_PART_SMEM;
-  if (local)
-    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) sh[i] = 0;
-  __syncthreads();
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ntile; t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t sidx = __ldg(tsrc + t);
-    const uint32_t v = __ldg(srcs[sidx].keys + (__ldg(tkey + t) - srcs[sidx].key_base));
-    uint32_t lo = 0, hi = nparts;  // last p with part_v[p] <= v
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (__ldg(part_v + mid) <= v) lo = mid; else hi = mid;
-    }
-    tpart[t] = lo;
-    if (local) atomicAdd(sh + lo, 1u); else atomicAdd(hist + lo, 1u);
-  }
-  __syncthreads();
-  if (local)
-    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x)
-      if (sh[i]) atomicAdd(hist + i, sh[i]);
-}
-
-// tord[cursor[p]++] = t for every tile t of partition p (cursor starts at the
-// partition's first position); the order within a partition is immaterial.
-// Partitions are few, so a per-tile global atomic would serialise on a
-// handful of cursors: each block counts a chunk of SCATTER_ITEMS tiles per
-// thread in shared memory (one atomic per warp and partition, lanes of the
-// same partition found with __match_any_sync), reserves each partition's
-// range with one global atomic, then writes.
-constexpr int SCATTER_ITEMS = 8;
-
-__global__ void __launch_bounds__(256) tile_scatter_kernel(const uint32_t *__restrict__ tpart, uint64_t ntile,
-                                                           uint32_t nparts, uint32_t *__restrict__ cursor,
-                                                           uint32_t *__restrict__ tord) {
-  __shared__ uint32_t cnt[TILE_PART_SMEM], base[TILE_PART_SMEM];
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint64_t chunk = (uint64_t)blockDim.x * SCATTER_ITEMS;
-  for (uint64_t c0 = blockIdx.x * chunk; c0 < ntile; c0 += (uint64_t)gridDim.x * chunk) {
-    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) cnt[i] = 0;
-    __syncthreads();
-    uint32_t pp[SCATTER_ITEMS], off[SCATTER_ITEMS];
-#pragma unroll
-    for (int it = 0; it < SCATTER_ITEMS; ++it) {
-      const uint64_t t = c0 + (uint64_t)it * blockDim.x + threadIdx.x;
-      const uint32_t p = t < ntile ? __ldg(tpart + t) : 0xFFFFFFFFu;
-      const uint32_t peers = __match_any_sync(dev::FULL, p);
-      const uint32_t leader = __ffs(peers) - 1;
-      uint32_t o = 0;
-      if (lane == leader && p != 0xFFFFFFFFu) o = atomicAdd(cnt + p, (uint32_t)__popc(peers));
-      pp[it] = p;
-      off[it] = __shfl_sync(dev::FULL, o, leader) + __popc(peers & ((1u << lane) - 1u));
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) base[i] = cnt[i] ? atomicAdd(cursor + i, cnt[i]) : 0u;
-    __syncthreads();
-#pragma unroll
-    for (int it = 0; it < SCATTER_ITEMS; ++it)
-      if (pp[it] != 0xFFFFFFFFu) tord[base[pp[it]] + off[it]] = (uint32_t)(c0 + (uint64_t)it * blockDim.x + threadIdx.x);
-    __syncthreads();  // cnt and base are reset by the next chunk
-  }
-}
-
-// Fallback for more partitions than the shared-memory tables hold.
-__global__ void tile_scatter_global_kernel(const uint32_t *__restrict__ tpart, uint64_t ntile,
-                                           uint32_t *__restrict__ cursor, uint32_t *__restrict__ tord) {
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ntile; t += (uint64_t)gridDim.x * blockDim.x)
-    tord[atomicAdd(cursor + __ldg(tpart + t), 1u)] = (uint32_t)t;
-}
-
-void launch_tile_partition(const TabSource *d_src, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                           const uint32_t *part_v, uint32_t nparts, uint32_t *tpart, uint32_t *hist, cudaStream_t s) {
-  if (ntile == 0) return;
-  uint64_t blocks = (ntile + 255) / 256;
-  if (blocks > 148ull * 8) blocks = 148ull * 8;
-  count_launch();
-  tile_partition_kernel<<<(uint32_t)blocks, 256, 0, s>>>(d_src, tkey, tsrc, ntile, part_v, nparts, tpart, hist);
-}
-
-void launch_tile_scatter(const uint32_t *tpart, uint64_t ntile, uint32_t nparts, uint32_t *cursor, uint32_t *tord,
-                         cudaStream_t s) {
-  if (ntile == 0) return;
-  count_launch();
-  if (nparts <= TILE_PART_SMEM) {
-    uint64_t blocks = (ntile + 256 * SCATTER_ITEMS - 1) / (256 * SCATTER_ITEMS);
-    if (blocks > 148ull * 8) blocks = 148ull * 8;
-    tile_scatter_kernel<<<(uint32_t)blocks, 256, 0, s>>>(tpart, ntile, nparts, cursor, tord);
+  if (write) {
+    table_vtx_kernel<true><<<(uint32_t)blocks, 256, 0, s>>>(P);
   } else {
-    uint64_t blocks = (ntile + 255) / 256;
-    if (blocks > 148ull * 32) blocks = 148ull * 32;
-    tile_scatter_global_kernel<<<(uint32_t)blocks, 256, 0, s>>>(tpart, ntile, cursor, tord);
+    const size_t smem = (size_t)warps * 32 * P.WTp * 4;
+    cudaFuncSetAttribute(table_vtx_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    table_vtx_kernel<false><<<(uint32_t)blocks, warps * 32, smem, s>>>(P);
   }
 }
 

@@ -103,8 +103,8 @@ struct TabSource {           // a (query, query vertex) whose candidates are tab
 struct TabEdge {             // a directed table T(u -> w)
   uint32_t src;              // index into TabSource
   uint32_t flags;            // TAB_KEY_MAP: the write pass also records each value's key position
-  const uint64_t *rb_w;      // rank bitmap row of the target w
-  const uint32_t *bits_w;    // membership bits of w alone (32 vertices per word)
+  uint32_t tcol;             // the target row's bit in the target membership columns
+  uint32_t pad;
   uint64_t tile_base;        // first tile of this edge in the flattened edge-tile space
   uint64_t ntiles;
   uint64_t off_base;         // first entry of this edge in the flattened offsets space
@@ -113,34 +113,57 @@ struct TabEdge {             // a directed table T(u -> w)
 // tiles[k] = ceil(deg(key k) / 32) over the flattened key space.
 void launch_key_tiles(const DevGraph &g, const TabSource *d_src, uint32_t nsrc, uint64_t nkeys,
                       uint32_t *tiles, cudaStream_t s);
-// tkey[t] / tsrc[t]: the key and the source of tile t of the flattened
-// source-tile space (tp: exclusive scan of the key tiles).
-void launch_tile_keys(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp, uint32_t *tkey,
-                      uint32_t *tsrc, cudaStream_t s);
-// One pass of the table kernels over positions [t0, t1) of a tile order
-// (tord; null = the tiles themselves): key arcs are read at
-// nbr[arc - arc_shift], with off the device offsets of the data graph.
-struct TabPass {
+// Membership columns of a list of rows: out[v * W + c] bit b = v is in row
+// rows[32c + b] (bits: membership bit rows, nwords u32 words per row).  With
+// vtiles, vtiles[v] = ceil(deg(v) / 32) for a vertex in any of the rows, else 0.
+void launch_row_columns(const uint32_t *bits, uint32_t nwords, const uint32_t *rows, uint32_t nrows, uint32_t W,
+                        uint32_t nv, uint32_t *out, uint32_t *vtiles, const uint32_t *deg, cudaStream_t s);
+// vt[t] = v for every vertex tile t in [vtp[v], vtp[v + 1]).
+void launch_vertex_tile_map(const uint64_t *vtp, uint32_t nv, uint32_t *vt, cudaStream_t s);
+// out[i] = a[idx[i]].
+void launch_gather_u64(const uint64_t *a, const uint32_t *idx, uint32_t n, uint64_t *out, cudaStream_t s);
+struct VSrc {                // a table source as the vertex-tile passes see it
+  const uint64_t *rb;        // rank bitmap row of its candidates
+  uint64_t key_base;         // first key in the flattened key space
+  uint64_t stb;              // tp[key_base]: its first tile
+  uint32_t e0, ne;           // its tables: edges [e0, e0 + ne)
+};
+struct VEdge {
+  uint64_t tile_base;
+  uint32_t tcol;
+  uint32_t flags;
+};
+// One table pass over vertex tiles [t0, t1) (vt: tile -> vertex, vtp: first
+// tile of each vertex).  Arcs are read at nbr[arc - arc_shift], with off the
+// device offsets of the data graph.  S: the source membership columns (WS
+// words per vertex), B: the target membership columns (WT words per vertex).
+// count: mask[edge.tile_base + lt] = the 32-bit membership mask of tile lt of
+// the edge's source; write: the values (and key positions) at vp.
+struct VPass {
   const uint64_t *off;
   const uint32_t *nbr;
   uint64_t arc_shift;
-  const uint32_t *tord;
   uint64_t t0, t1;
+  const uint32_t *vt;
+  const uint64_t *vtp;
+  const uint32_t *S;
+  uint32_t WS;
+  uint32_t WT;
+  uint32_t WTp;              // set by the launcher
+  uint32_t pad;
+  const uint32_t *B;
+  const VSrc *vsrc;
+  const VEdge *vedge;
+  const uint64_t *tp;
+  uint32_t *mask;
+  const uint64_t *vp;
+  uint32_t *values;
+  uint32_t *vkey;
 };
-// mask[edge.tile_base + i] = 32-bit membership mask of tile i of the edge's
-// source, for every edge of every source (sedge: {first edge, edges} per
-// source; a source's edges are consecutive).
-void launch_table_count(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, uint32_t *mask,
-                        cudaStream_t s);
-// Out-of-core partition streaming: tpart[t] = partition of tile t's key vertex
-// (part_v: nparts + 1 vertex bounds), hist[p] += tiles of partition p; then
-// the tiles grouped by partition into tord (cursor[p] = first position of p).
-constexpr uint32_t TILE_PART_SMEM = 4096;
-void launch_tile_partition(const TabSource *d_src, const uint32_t *tkey, const uint32_t *tsrc, uint64_t ntile,
-                           const uint32_t *part_v, uint32_t nparts, uint32_t *tpart, uint32_t *hist, cudaStream_t s);
-void launch_tile_scatter(const uint32_t *tpart, uint64_t ntile, uint32_t nparts, uint32_t *cursor, uint32_t *tord,
-                         cudaStream_t s);
+void launch_table_vtx(const VPass &P, bool write, cudaStream_t s);
+// Whether the count pass can stage WT-word target columns (one warp's 32
+// columns within 200 KB of shared memory).
+bool table_vtx_fits(uint32_t WT);
 // out[i] = tp[d_src[i].key_base] for i < nsrc, out[nsrc] = tp[nkeys].
 void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp,
                               uint64_t *out, cudaStream_t s);
@@ -153,9 +176,6 @@ void launch_table_offsets(const TabSource *d_src, const TabEdge *d_edge, uint32_
                           const uint64_t *tp, const uint64_t *vp, uint64_t total_offsets,
                           cudaStream_t s);
 constexpr uint32_t TAB_KEY_MAP = 1;
-void launch_table_write(const TabPass &P, const TabSource *d_src, const uint32_t *sedge, const TabEdge *d_edge,
-                        const uint64_t *tp, const uint32_t *tkey, const uint32_t *tsrc, const uint32_t *mask,
-                        const uint64_t *vp, uint32_t *values, uint32_t *vkey, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Cuckoo hash: vertex id -> position in C(u).  Two bucketised tables of

@@ -54,20 +54,22 @@ struct Server {
   }
   std::map<uint64_t, gem_result> done;
   uint64_t next_ticket = 1;
-  uint64_t in_flight = 0, budget = 0;
+  uint64_t in_flight = 0, budget = 0, per_wave = 0;
   uint64_t waves = 0;
 };
 
-// Upper bound of the device scratch one query's wave can take, from the
+// Upper bound of the device scratch one query adds to a wave, from the
 // graph's label statistics alone (the plan is not known at admission): per
 // query vertex its rank-bitmap row with the row scan, its candidate list
-// (at most the label's vertices) and, as an edge-table source, its keys'
-// tile bookkeeping (tiles <= vertices + arcs / 32 of the label) and an
-// index; per query edge the larger direction's table: per-tile masks and
-// positions, offsets per key, values and key positions (at most the arcs
-// between the two labels); per query the join's descriptors.
-static uint64_t estimate_bytes(const gem_ctx *ctx, const HostQuery &q) {
-  const uint64_t nwords = (ctx->g.nv + 31) / 32;
+// (at most the label's vertices), its bits in the wave's source and target
+// membership columns and, as an edge-table source, its keys' tile counts and
+// scan and an index; per query edge the larger direction's table: per-tile
+// masks and positions, offsets per key, values and key positions (at most
+// the arcs between the two labels); per query the join's descriptors.
+// *per_wave: what every wave takes once whatever its queries (the vertex
+// tiles, their scan and map, the columns' rounding word per vertex).
+static uint64_t estimate_bytes(const gem_ctx *ctx, const HostQuery &q, uint64_t *per_wave) {
+  const uint64_t nv = ctx->g.nv, nwords = (nv + 31) / 32;
   const size_t L = ctx->label_freq.size();
   auto freq = [&](uint32_t l) -> uint64_t { return l < L ? ctx->label_freq[l] : 0; };
   auto tiles = [&](uint32_t l) -> uint64_t { return l < L ? ctx->label_freq[l] + ctx->label_arcs[l] / 32 + 1 : 1; };
@@ -78,9 +80,10 @@ static uint64_t estimate_bytes(const gem_ctx *ctx, const HostQuery &q) {
   auto al = [](uint64_t b) -> uint64_t { return (b + 255) & ~(uint64_t)255; };
   uint64_t b = 0;
   for (uint32_t u = 0; u < q.nv; ++u) {
-    const uint64_t f = freq(q.lab[u]), t = tiles(q.lab[u]);
+    const uint64_t f = freq(q.lab[u]);
     b += al(8 * nwords) + al(8 * (nwords + 1)) + al(8 * (nwords / 2048 + 2)) + al(4 * f + 4);  // row, scan, list
-    b += al(4 * f) + al(8 * (f + 1)) + al(8 * (f / 2048 + 2)) + 2 * al(4 * t);  // source: key tiles, tile map
+    b += al(4 * nwords) + 2 * al(4 * nwords);                                  // bit row, both columns
+    b += al(4 * f) + al(8 * (f + 1)) + al(8 * (f / 2048 + 2));                 // source: key tiles and scan
     b += al(16 * f + 1024);                                                    // index
   }
   for (uint32_t e = 0; e < q.ne; ++e) {
@@ -93,6 +96,9 @@ static uint64_t estimate_bytes(const gem_ctx *ctx, const HostQuery &q) {
     }
     b += most;
   }
+  const uint64_t parts = ctx->part_v.empty() ? 0 : ctx->part_v.size();
+  *per_wave = 2 * al(4 * nv) + al(4 * nv + 4) + al(8 * (nv + 1)) + al(8 * (nv / 2048 + 2)) +
+              al(4 * (nv + ctx->g.narcs / 32 + 1)) + al(8 * parts + 8) + (1ull << 20);
   return b + (64ull << 10) * (q.nv + 1) + (1ull << 20);
 }
 
@@ -103,7 +109,8 @@ extern "C" gem_status gem_estimate_bytes(const gem_ctx *ctx, const gem_query *q,
   std::string err;
   const gem_status st = make_host_query(q, hq, err);
   if (st != GEM_OK) return st;
-  *bytes = estimate_bytes(ctx, hq);
+  uint64_t per_wave = 0;
+  *bytes = estimate_bytes(ctx, hq, &per_wave) + per_wave;
   return GEM_OK;
 }
 
@@ -223,8 +230,14 @@ extern "C" gem_status gem_submit(gem_ctx *ctx, const gem_query *q, int mode, uin
     if (ss != GEM_OK) return ss;
   }
   Server &S = *ctx->server;
-  const uint64_t est = estimate_bytes(ctx, hq);
+  uint64_t per_wave = 0;
+  const uint64_t est = estimate_bytes(ctx, hq, &per_wave);
   std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.per_wave) {  // every lane's wave takes this once, beside its queries'
+    S.per_wave = per_wave;
+    const uint64_t fixed = per_wave * S.lanes.size();
+    S.budget = S.budget > fixed ? S.budget - fixed : 0;
+  }
   if (S.in_flight + est > S.budget && S.in_flight > 0) return GEM_ERR_OOM;  // busy: retry later
   S.in_flight += est;
   *ticket = S.next_ticket++;

@@ -117,3 +117,39 @@ def test_out_of_core_two_lane_batch_matches_in_core():
     assert [(r["status"], r["count"]) for r in rb] == [(r["status"], r["count"]) for r in ra]
     waves = {r["wave"] for r in rb}
     assert st["waves_streamed"] == len(waves) and st["bytes_streamed"] > 0
+
+
+def _signatures(qs):
+    """Filter-row signatures (label, degree, sorted neighbour labels) of the
+    query vertices: a wave has one row per distinct signature."""
+    sigs = set()
+    for q in qs:
+        nb = [[] for _ in range(q.nv)]
+        for a, b in q.edges.tolist():
+            nb[a].append(int(q.labels[b]))
+            nb[b].append(int(q.labels[a]))
+        for u in range(q.nv):
+            sigs.add((int(q.labels[u]), len(nb[u]), tuple(sorted(nb[u]))))
+    return sigs
+
+
+def test_wave_with_many_sources_matches_oracle():
+    """A wave with well over 1,024 distinct filter rows: the table passes
+    find a vertex's sources in several 32-word chunks of its source column
+    and stage target columns of more than 32 words.  Every count the oracle
+    finishes equals the batch's."""
+    g = gem.HostGraph.rmat(10, 8, seed=0x47454D0A).set_labels(16, 1.0, seed=0x47454D0A ^ 0x4C)
+    pool = gem.gen_queries(g, 8, gem.SPARSE, 480, seed=0x5109)
+    assert sum(q.nv for q in pool) <= 4096  # one wave's rows
+    assert len(_signatures(pool)) >= 2000
+    with gem.Context(time_cap_ms=20000) as c:
+        c.load_graph(g)
+        st, rb = c.batch(pool)
+    assert len({r["wave"] for r in rb}) <= 2
+    checked = 0
+    for i, q in enumerate(pool):
+        cnt, _, ok = oracle.count(g, q, want_hash=False, work_cap=20_000_000)
+        if ok:
+            assert rb[i]["status"] == "OK" and rb[i]["count"] == cnt, (i, rb[i]["status"])
+            checked += 1
+    assert checked >= 300, checked
