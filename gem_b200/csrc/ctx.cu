@@ -86,6 +86,7 @@ gem_status Arena::alloc(gem_ctx *ctx, uint64_t bytes, void **out) {
       if (chunks[i].used == 0) {
         cudaFree(chunks[i].base);
         ctx->device_bytes -= chunks[i].size;
+        reserved = false;
       } else {
         chunks[k++] = chunks[i];
       }
@@ -96,6 +97,10 @@ gem_status Arena::alloc(gem_ctx *ctx, uint64_t bytes, void **out) {
     if (ctx->device_bytes + sz > ctx->budget) sz = bytes;
     if (ctx->device_bytes + sz > ctx->budget) {
       ctx->err = "device budget exceeded: need " + std::to_string(bytes) + " more bytes";
+      uint64_t held = 0;
+      for (const Chunk &c : chunks) held += c.size;
+      oom_need = in_use + bytes;
+      oom_room = ctx->budget > ctx->device_bytes - held ? ctx->budget - (ctx->device_bytes - held) : 0;
       return GEM_ERR_OOM;
     }
   }
@@ -104,6 +109,7 @@ gem_status Arena::alloc(gem_ctx *ctx, uint64_t bytes, void **out) {
   if (e != cudaSuccess) {
     cudaGetLastError();
     ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    oom_need = oom_room = 0;
     return GEM_ERR_OOM;
   }
   ctx->device_bytes += sz;
@@ -113,6 +119,19 @@ gem_status Arena::alloc(gem_ctx *ctx, uint64_t bytes, void **out) {
   in_use += bytes;
   peak = std::max(peak, in_use);
   return GEM_OK;
+}
+void Arena::reserve(gem_ctx *ctx, uint64_t bytes) {
+  release(ctx);
+  bytes &= ~((2ull << 20) - 1);
+  if (bytes == 0 || ctx->device_bytes + bytes > ctx->budget) return;
+  char *p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  ctx->device_bytes += bytes;
+  chunks.push_back({p, bytes, 0});
+  reserved = true;
 }
 void Arena::reset() {
   for (auto &c : chunks) c.used = 0;
@@ -125,6 +144,7 @@ void Arena::release(gem_ctx *ctx) {
     ctx->device_bytes -= c.size;
   }
   chunks.clear();
+  reserved = false;
   cur = 0;
   in_use = 0;
 }
@@ -305,6 +325,7 @@ void drop_batch_lane(gem_ctx *ctx) {
   if (!ctx->batch_lane) return;
   gem_ctx_destroy(ctx->batch_lane);
   ctx->batch_lane = nullptr;
+  if (ctx->arena.reserved) ctx->arena.release(ctx);  // it held the lane-split budget
   if (ctx->batch_saved_budget) ctx->budget = ctx->batch_saved_budget;
   ctx->batch_saved_budget = 0;
 }
@@ -1152,9 +1173,12 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   // One table pass (count or write) over every vertex tile: in place, or
   // partition by partition with the copy of the next partition (side
   // stream, the other staging buffer) overlapping the kernel of the current one.
+  unsigned long long *d_next;
+  ST(aalloc(ctx, 1, &d_next));
   auto table_pass = [&](bool write) -> gem_status {
     VPass P;
     std::memset(&P, 0, sizeof P);
+    P.next = d_next;
     P.off = ctx->g.off;
     P.nbr = ctx->g.nbr;
     P.arc_shift = 0;
@@ -1722,11 +1746,13 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
   }
   // Waves are packed as the batch runs: as many pending queries as the
   // lane's row limit allows.  A wave that does not fit the lane's device
-  // budget is split in halves and retried (down to single queries) with a
-  // released arena, and the lane's limit drops to half the rows that failed,
-  // so later waves (and later batches) are packed to a size that fits
-  // (the limit does not grow back: a retried wave costs its filter and
-  // table build).
+  // budget is retried with a released arena in smaller waves (down to single
+  // queries), and the lane's limit drops to the rows that would have fit:
+  // the failed wave's rows scaled by the bytes the budget left it over the
+  // bytes it asked for, with a tenth kept back (half when that is not
+  // known).  So later waves (and later batches) are packed to a size that
+  // fits; the limit does not grow back, since a retried wave costs its
+  // filter and table build.
   //
   // An in-core batch of more rows than one wave takes runs on two lanes: the
   // context and a lane context borrowing its graph (created once, kept), one
@@ -1781,11 +1807,31 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
         cudaGetLastError();
         std::lock_guard<std::mutex> lk(mu);
         if (st == GEM_ERR_OOM && ids.size() > 1) {
-          lane->wave_rows_cap = (uint32_t)std::max<uint64_t>(1, rows_of(ids) / 2);
-          lane->arena.release(lane);  // a fresh arena: chunks sized for the smaller waves
-          const size_t h = ids.size() / 2;
-          retry.push_front(std::vector<uint32_t>(ids.begin() + h, ids.end()));
-          retry.push_front(std::vector<uint32_t>(ids.begin(), ids.begin() + h));
+          // the rows that would have fit, by what the wave asked for against
+          // what the budget leaves it (a tenth kept back), else half
+          const Arena &a = lane->arena;
+          double f = a.oom_need ? 0.9 * (double)a.oom_room / (double)a.oom_need : 0.5;
+          f = std::min(0.9, std::max(0.25, f));
+          const uint64_t cap = std::max<uint64_t>(1, (uint64_t)(f * (double)rows_of(ids)));
+          lane->wave_rows_cap = (uint32_t)cap;
+          if (!lane->arena.reserved) lane->arena.release(lane);  // a fresh arena: chunks sized for the smaller waves
+          // the queries again in waves of at most cap rows (at least one query each)
+          std::vector<std::vector<uint32_t>> parts(1);
+          uint64_t rows = 0;
+          for (uint32_t id : ids) {
+            if (!parts.back().empty() && rows + all[id].nv > cap) {
+              parts.emplace_back();
+              rows = 0;
+            }
+            parts.back().push_back(id);
+            rows += all[id].nv;
+          }
+          if (parts.size() == 1) {  // one query over the cap: halve by count
+            const size_t h = ids.size() / 2;
+            parts.assign({std::vector<uint32_t>(ids.begin(), ids.begin() + h),
+                          std::vector<uint32_t>(ids.begin() + h, ids.end())});
+          }
+          for (size_t i = parts.size(); i-- > 0;) retry.push_front(std::move(parts[i]));
           continue;
         }
         for (uint32_t id : ids) res[id].status = st;
@@ -1822,6 +1868,11 @@ extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t 
     second = ctx->batch_lane;
   }
   if (second) {
+    // each lane's arena: one chunk of its whole budget, less room for the
+    // join's graph and other small allocations outside the arena
+    for (gem_ctx *l : {ctx, second})
+      if (!l->arena.reserved && l->budget > l->device_bytes + (1ull << 30))
+        l->arena.reserve(l, l->budget - l->device_bytes - (512ull << 20));
     for (int b = 0; b < 6; ++b) second->tune[b] = ctx->tune[b];
     ctx->join_grid_div = second->join_grid_div = 2;
     std::thread t(worker, second);

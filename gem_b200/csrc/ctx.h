@@ -25,7 +25,15 @@ struct Arena {
   std::vector<Chunk> chunks;
   size_t cur = 0;
   uint64_t in_use = 0, peak = 0;
+  // the last failed allocation: what the wave would have held with it, and
+  // what the budget leaves for the arena
+  uint64_t oom_need = 0, oom_room = 0;
+  bool reserved = false;  // one chunk holding the whole budget (batch lanes)
   gem_status alloc(gem_ctx *ctx, uint64_t bytes, void **out);
+  // Replaces the chunks by one chunk of `bytes` (kept until release): waves
+  // of any size then never call cudaMalloc or cudaFree, whose frees wait for
+  // the whole device.  Falls back to growing chunks when it cannot allocate.
+  void reserve(gem_ctx *ctx, uint64_t bytes);
   void reset();
   void release(gem_ctx *ctx);
 };
@@ -161,8 +169,8 @@ struct gem_ctx {
   uint32_t donate_max_level = 30;
   bool closed_form_suffix = true;
   uint32_t wave_max_rows = 4096;
-  // batch packing learnt from earlier waves: half the rows of the last wave
-  // that did not fit the device budget (0 = none yet)
+  // batch packing learnt from earlier waves: the rows that would have fit of
+  // the last wave that did not fit the device budget (0 = none yet)
   uint32_t wave_rows_cap = 0;
   uint32_t join_grid_div = 1;        // the join grid takes blocks_per_sm / this per SM (serving lanes: 2)
   // device timeline: waves report their first and last event against ev_ref

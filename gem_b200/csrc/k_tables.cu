@@ -173,6 +173,8 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t r) {
 // The mask and value positions are those of the source's own tile order
 // (mask[tile_base + lt], lt = the tile's index among the source's tiles), so
 // both passes lay out every table exactly as a pass over the sources would.
+constexpr uint32_t TAB_GRAB = 2;  // vertex tiles a warp takes from the counter at a time
+
 struct VRec {
   uint64_t vb;  // first value position of the pair's tile
   uint32_t m;   // the tile's mask
@@ -184,8 +186,15 @@ __global__ void __launch_bounds__(256) table_vtx_kernel(VPass P) {
   extern __shared__ uint32_t stage[];  // count: 32 target columns per warp
   __shared__ VRec rec[8][32];          // write: the pairs of one round
   const uint32_t lane = dev::lane_id(), warp = threadIdx.x >> 5;
-  const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t t = P.t0 + blockIdx.x * (uint64_t)(blockDim.x >> 5) + warp; t < P.t1; t += nwarps) {
+  for (;;) {
+    // tiles are taken in order from one counter, so the tiles in flight stay
+    // a narrow window of consecutive vertices
+    unsigned long long got = 0;
+    if (lane == 0) got = atomicAdd(P.next, (unsigned long long)TAB_GRAB);
+    const uint64_t t0 = P.t0 + __shfl_sync(dev::FULL, got, 0);
+    if (t0 >= P.t1) break;
+    const uint64_t t1 = t0 + TAB_GRAB < P.t1 ? t0 + TAB_GRAB : P.t1;
+    for (uint64_t t = t0; t < t1; ++t) {
     const uint32_t v = __ldg(P.vt + t);
     const uint64_t c = t - __ldg(P.vtp + v);
     const uint64_t a0 = __ldg(P.off + v), arc = a0 + c * 32u + lane;
@@ -283,6 +292,7 @@ __global__ void __launch_bounds__(256) table_vtx_kernel(VPass P) {
         }
       }
     }
+    }
   }
 }
 
@@ -296,20 +306,38 @@ static uint32_t count_warps(uint32_t WTp) {
 
 bool table_vtx_fits(uint32_t WT) { return 32ull * (WT | 1u) * 4 <= (200ull << 10); }
 
+// Persistent grid: what the SMs hold at once (blocks per SM by occupancy).
+// Its warps take tiles in order from the launch's counter, so the tiles in
+// flight are a window of consecutive vertices, and the rank words, tile
+// bases, masks and positions they read are the same few lines per source
+// and table, which stay in L2 while the window passes (a static stride lets
+// the warps drift apart until they touch the whole order at once).
+static uint32_t resident_blocks(const void *fn, int threads, size_t smem, uint64_t want) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+  uint64_t b = (uint64_t)(sms > 0 ? sms : 148) * (uint64_t)(per_sm > 0 ? per_sm : 1);
+  if (b > want) b = want;
+  return (uint32_t)(b ? b : 1);
+}
+
 void launch_table_vtx(const VPass &P0, bool write, cudaStream_t s) {
   if (P0.t1 <= P0.t0) return;
   VPass P = P0;
   P.WTp = P.WT | 1u;  // odd: the lanes' columns fall in distinct banks
   const uint32_t warps = write ? 8u : count_warps(P.WTp);
-  uint64_t blocks = (P.t1 - P.t0 + warps - 1) / warps;
-  if (blocks > 148ull * 16) blocks = 148ull * 16;
+  const uint64_t want = (P.t1 - P.t0 + warps - 1) / warps;
+  cudaMemsetAsync(P.next, 0, sizeof(unsigned long long), s);
   count_launch();
   if (write) {
-    table_vtx_kernel<true><<<(uint32_t)blocks, 256, 0, s>>>(P);
+    const uint32_t blocks = resident_blocks((const void *)table_vtx_kernel<true>, 256, 0, want);
+    table_vtx_kernel<true><<<blocks, 256, 0, s>>>(P);
   } else {
     const size_t smem = (size_t)warps * 32 * P.WTp * 4;
     cudaFuncSetAttribute(table_vtx_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    table_vtx_kernel<false><<<(uint32_t)blocks, warps * 32, smem, s>>>(P);
+    const uint32_t blocks = resident_blocks((const void *)table_vtx_kernel<false>, (int)warps * 32, smem, want);
+    table_vtx_kernel<false><<<blocks, warps * 32, smem, s>>>(P);
   }
 }
 

@@ -159,6 +159,7 @@ struct VPass {
   const uint64_t *vp;
   uint32_t *values;
   uint32_t *vkey;
+  unsigned long long *next;  // tile counter of the launch (zeroed by the launcher)
 };
 void launch_table_vtx(const VPass &P, bool write, cudaStream_t s);
 // Whether the count pass can stage WT-word target columns (one warp's 32
