@@ -1035,7 +1035,7 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   ST(aalloc(ctx, nkeys ? nkeys : 1, &d_tiles));
   ST(aalloc(ctx, nkeys + 1, &d_tp));
   ST(aalloc(ctx, scan_tmp_words(nkeys), &d_tmp));
-  ST(aalloc(ctx, src.size() + 2, &d_stb));
+  ST(aalloc(ctx, src.size() + 3, &d_stb));
   launch_key_tiles(ctx->g, d_src, (uint32_t)src.size(), nkeys, d_tiles, ctx->s);
   launch_scan(d_tiles, SCAN_U32, nkeys, d_tp, d_tmp, ctx->s);
   launch_source_tile_bases(d_src, (uint32_t)src.size(), nkeys, d_tp, d_stb, ctx->s);
@@ -1054,11 +1054,19 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   ST(aalloc(ctx, scan_tmp_words(nv), &d_tmp3));
   launch_row_columns(w.d_bits, w.nwords, d_srow, (uint32_t)src.size(), WS, nv, d_S, d_vtiles, ctx->g.deg, ctx->s);
   launch_scan(d_vtiles, SCAN_U32, nv, d_vtp, d_tmp3, ctx->s);
+  // the write pass's units: up to TAB_WGROUP consecutive tiles of one vertex
+  uint32_t *d_vunits;
+  uint64_t *d_vgp;
+  ST(aalloc(ctx, nv ? nv : 1, &d_vunits));
+  ST(aalloc(ctx, (uint64_t)nv + 1, &d_vgp));
+  launch_unit_counts(d_vtiles, nv, d_vunits, ctx->s);
+  launch_scan(d_vunits, SCAN_U32, nv, d_vgp, d_tmp3, ctx->s);
   CU(cudaMemcpyAsync(d_stb + src.size() + 1, d_vtp + nv, 8, cudaMemcpyDeviceToDevice, ctx->s));
-  std::vector<uint64_t> stb(src.size() + 2);
+  CU(cudaMemcpyAsync(d_stb + src.size() + 2, d_vgp + nv, 8, cudaMemcpyDeviceToDevice, ctx->s));
+  std::vector<uint64_t> stb(src.size() + 3);
   CU(d2h_sync(ctx, stb.data(), d_stb, 8 * stb.size()));
   CU(cudaGetLastError());
-  const uint64_t vtiles = stb[src.size() + 1];
+  const uint64_t vtiles = stb[src.size() + 1], vunits = stb[src.size() + 2];
   // edges, grouped by source: a source's tables are one range of the edges
   struct EdgeReq {
     uint32_t s, qi, j, k;
@@ -1138,8 +1146,11 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   CU(h2d(ctx, d_trow, tgt_row.data(), 4 * tgt_row.size()));
   ST(aalloc(ctx, (uint64_t)nv * WT, &d_B));
   launch_row_columns(w.d_bits, w.nwords, d_trow, (uint32_t)tgt_row.size(), WT, nv, d_B, nullptr, nullptr, ctx->s);
+  uint32_t *d_vg;
   ST(aalloc(ctx, vtiles ? vtiles : 1, &d_vt));
   launch_vertex_tile_map(d_vtp, nv, d_vt, ctx->s);
+  ST(aalloc(ctx, vunits ? vunits : 1, &d_vg));
+  launch_vertex_tile_map(d_vgp, nv, d_vg, ctx->s);
   std::vector<VSrc> vs(src.size());
   for (size_t i = 0; i < src.size(); ++i)
     vs[i] = VSrc{w.d_rb + (uint64_t)src_row[i] * w.nwords, src[i].key_base, stb[i], sedge[2 * i], sedge[2 * i + 1]};
@@ -1156,14 +1167,17 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   // they are filled enough (their bytes at most twice what the tiles would
   // read from the mapped adjacency), else read in place.
   const uint32_t nparts = ctx->part_v.empty() ? 0u : (uint32_t)ctx->part_v.size() - 1;
-  std::vector<uint64_t> pstart;
+  std::vector<uint64_t> pstart, pstart_w;  // each partition's first tile and first write unit
   bool streamed = false;
   if (ctx->opts.ooc && nparts && ctx->opts.ooc_stream != 2 && vtiles) {
     uint64_t *d_pb;
-    ST(aalloc(ctx, nparts + 1, &d_pb));
+    ST(aalloc(ctx, 2ull * (nparts + 1), &d_pb));
     launch_gather_u64(d_vtp, ctx->d_part_v, nparts + 1, d_pb, ctx->s);
-    pstart.assign(nparts + 1, 0);
-    CU(d2h_sync(ctx, pstart.data(), d_pb, 8ull * (nparts + 1)));
+    launch_gather_u64(d_vgp, ctx->d_part_v, nparts + 1, d_pb + nparts + 1, ctx->s);
+    std::vector<uint64_t> pb(2ull * (nparts + 1));
+    CU(d2h_sync(ctx, pb.data(), d_pb, 16ull * (nparts + 1)));
+    pstart.assign(pb.begin(), pb.begin() + nparts + 1);
+    pstart_w.assign(pb.begin() + nparts + 1, pb.end());
     uint64_t need = 0;
     for (uint32_t p = 0; p < nparts; ++p)
       if (pstart[p + 1] > pstart[p]) need += 4 * (ctx->part_a[p + 1] - ctx->part_a[p]);
@@ -1183,9 +1197,11 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
     P.nbr = ctx->g.nbr;
     P.arc_shift = 0;
     P.t0 = 0;
-    P.t1 = vtiles;
+    P.t1 = write ? vunits : vtiles;
     P.vt = d_vt;
     P.vtp = d_vtp;
+    P.vg = d_vg;
+    P.vgp = d_vgp;
     P.S = d_S;
     P.WS = WS;
     P.WT = WT;
@@ -1216,8 +1232,8 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
       CU(cudaStreamWaitEvent(ctx->s, ctx->ev_ready[b], 0));
       P.nbr = ctx->d_stage[b];
       P.arc_shift = a0;
-      P.t0 = pstart[p];
-      P.t1 = pstart[p + 1];
+      P.t0 = write ? pstart_w[p] : pstart[p];
+      P.t1 = write ? pstart_w[p + 1] : pstart[p + 1];
       launch_table_vtx(P, write, ctx->s);
       CU(cudaEventRecord(ctx->ev_free[b], ctx->s));
       ctx->ooc.parts_streamed += 1;

@@ -129,6 +129,19 @@ void launch_vertex_tile_map(const uint64_t *vtp, uint32_t nv, uint32_t *vt, cuda
   vertex_tile_map_kernel<<<blocks, 256, 0, s>>>(vtp, nv, vt);
 }
 
+__global__ void unit_counts_kernel(const uint32_t *__restrict__ vtiles, uint32_t nv, uint32_t *__restrict__ out) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    out[v] = (__ldg(vtiles + v) + TAB_WGROUP - 1) / TAB_WGROUP;
+}
+
+void launch_unit_counts(const uint32_t *vtiles, uint32_t nv, uint32_t *out, cudaStream_t s) {
+  if (nv == 0) return;
+  uint32_t blocks = (nv + 255) / 256;
+  if (blocks > 148u * 16) blocks = 148u * 16;
+  count_launch();
+  unit_counts_kernel<<<blocks, 256, 0, s>>>(vtiles, nv, out);
+}
+
 __global__ void gather_u64_kernel(const uint64_t *__restrict__ a, const uint32_t *__restrict__ idx, uint32_t n,
                                   uint64_t *__restrict__ out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -167,13 +180,14 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t r) {
 //          arcs of the tile (the warp stages the arcs' target columns in
 //          shared memory, one column per arc) and writes the tile's mask;
 //   write: each lane reads its pair's mask and value position into a
-//          per-warp record; then for each record the lanes, one per arc,
-//          write the arcs whose bit is set (and the key position) at the
-//          value position plus their rank in the mask.
+//          per-warp record (records of empty masks dropped); then for each
+//          record the lanes, one per arc, write the arcs whose bit is set
+//          (and the key position) at the value position plus their rank in
+//          the mask.
 // The mask and value positions are those of the source's own tile order
 // (mask[tile_base + lt], lt = the tile's index among the source's tiles), so
 // both passes lay out every table exactly as a pass over the sources would.
-constexpr uint32_t TAB_GRAB = 2;  // vertex tiles a warp takes from the counter at a time
+constexpr uint32_t TAB_GRAB = 2;  // units a warp takes from the counter at a time
 
 struct VRec {
   uint64_t vb;  // first value position of the pair's tile
@@ -183,25 +197,41 @@ struct VRec {
 
 template <bool WRITE>
 __global__ void __launch_bounds__(256) table_vtx_kernel(VPass P) {
+  constexpr uint32_t G = WRITE ? TAB_WGROUP : 1u;  // tiles of one vertex per unit
   extern __shared__ uint32_t stage[];  // count: 32 target columns per warp
-  __shared__ VRec rec[8][32];          // write: the pairs of one round
+  __shared__ VRec rec[WRITE ? 8 : 1][32 * G];  // write: the records of one round
   const uint32_t lane = dev::lane_id(), warp = threadIdx.x >> 5;
   for (;;) {
-    // tiles are taken in order from one counter, so the tiles in flight stay
-    // a narrow window of consecutive vertices
+    // units are taken in order from one counter, so the units in flight
+    // stay a narrow window of consecutive vertices
     unsigned long long got = 0;
     if (lane == 0) got = atomicAdd(P.next, (unsigned long long)TAB_GRAB);
     const uint64_t t0 = P.t0 + __shfl_sync(dev::FULL, got, 0);
     if (t0 >= P.t1) break;
     const uint64_t t1 = t0 + TAB_GRAB < P.t1 ? t0 + TAB_GRAB : P.t1;
     for (uint64_t t = t0; t < t1; ++t) {
-    const uint32_t v = __ldg(P.vt + t);
-    const uint64_t c = t - __ldg(P.vtp + v);
-    const uint64_t a0 = __ldg(P.off + v), arc = a0 + c * 32u + lane;
-    const uint64_t a1 = __ldg(P.off + v + 1);
-    const bool valid = arc < a1;
+    // the unit: tiles c .. c + nt - 1 of vertex v
+    uint32_t v, nt = 1;
+    uint64_t c;
+    if (WRITE) {
+      v = __ldg(P.vg + t);
+      c = (t - __ldg(P.vgp + v)) * G;
+      const uint64_t tv = __ldg(P.vtp + v + 1) - __ldg(P.vtp + v);
+      nt = tv - c < G ? (uint32_t)(tv - c) : G;
+    } else {
+      v = __ldg(P.vt + t);
+      c = t - __ldg(P.vtp + v);
+    }
+    const uint64_t a0 = __ldg(P.off + v), a1 = __ldg(P.off + v + 1);
+    uint32_t xs[G];
+#pragma unroll
+    for (uint32_t i = 0; i < G; ++i) {
+      const uint64_t arc = a0 + (c + i) * 32u + lane;
+      xs[i] = i < nt && arc < a1 ? __ldg(P.nbr + (arc - P.arc_shift)) : 0u;
+    }
+    const bool valid = a0 + c * 32u + lane < a1;  // lane's arc of the unit's first tile
     const uint32_t nvalid = a1 - a0 - c * 32u < 32u ? (uint32_t)(a1 - a0 - c * 32u) : 32u;  // valid lanes: a prefix
-    const uint32_t x = valid ? __ldg(P.nbr + (arc - P.arc_shift)) : 0u;
+    const uint32_t x = xs[0];
     if (!WRITE) {
       __syncwarp();  // the previous tile's reads of the stage are done
       for (uint32_t l = 0; l < nvalid; ++l) {
@@ -265,27 +295,48 @@ __global__ void __launch_bounds__(256) table_vtx_kernel(VPass P) {
           const uint64_t maddr = E.tile_base + plt;
           if (!WRITE) {
             const uint32_t *col = stage + (uint64_t)warp * 32u * P.WTp + (E.tcol >> 5);
-            const uint32_t sh = E.tcol & 31u;
-            uint32_t m = 0;
-            for (uint32_t l = 0; l < nvalid; ++l) m |= ((col[l * P.WTp] >> sh) & 1u) << l;
+            const uint32_t sh = E.tcol & 31u, st = P.WTp;
+            uint32_t m = 0, l = 0;
+            for (; l + 4 <= nvalid; l += 4) {
+              const uint32_t w0 = col[l * st], w1 = col[(l + 1) * st], w2 = col[(l + 2) * st], w3 = col[(l + 3) * st];
+              m |= (((w0 >> sh) & 1u) | (((w1 >> sh) & 1u) << 1) | (((w2 >> sh) & 1u) << 2) | (((w3 >> sh) & 1u) << 3)) << l;
+            }
+            for (; l < nvalid; ++l) m |= ((col[l * st] >> sh) & 1u) << l;
             if (have) P.mask[maddr] = m;
           } else {
-            VRec r{0, 0, 0xFFFFFFFFu};
-            if (have) {
-              r.m = __ldg(P.mask + maddr);
-              r.vb = __ldg(P.vp + maddr);
-              if (E.flags & TAB_KEY_MAP) r.kf = pk;
+            // records of the pair's tiles that have values, packed to the
+            // front; the tile's index in the unit rides in the top byte of
+            // the value position.  A key's tiles are consecutive in its
+            // source's tile order, so the unit's masks and positions are
+            // consecutive words.
+            const uint32_t kf = have && (E.flags & TAB_KEY_MAP) ? pk : 0xFFFFFFFFu;
+            const uint32_t below = (1u << lane) - 1u;
+            uint32_t m[G];
+            uint64_t vb[G];
+#pragma unroll
+            for (uint32_t i = 0; i < G; ++i) {
+              m[i] = have && i < nt ? __ldg(P.mask + maddr + i) : 0u;
+              vb[i] = have && i < nt ? __ldg(P.vp + maddr + i) : 0ull;
             }
             __syncwarp();  // the previous round's records are read
-            rec[warp][lane] = r;
+            uint32_t nr = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < G; ++i) {
+              const uint32_t nz = __ballot_sync(dev::FULL, m[i] != 0u);
+              if (m[i]) rec[warp][nr + __popc(nz & below)] = VRec{vb[i] | ((uint64_t)i << 56), m[i], kf};
+              nr += __popc(nz);
+            }
             __syncwarp();
-            const uint32_t nr = npairs - pb < 32u ? npairs - pb : 32u;
             for (uint32_t i = 0; i < nr; ++i) {
-              const VRec ri = rec[warp][i];
-              if ((ri.m >> lane) & 1u) {
-                const uint64_t pos = ri.vb + __popc(ri.m & ((1u << lane) - 1u));
-                P.values[pos] = x;
-                if (ri.kf != 0xFFFFFFFFu) P.vkey[pos] = ri.kf;
+              const VRec r0 = rec[warp][i];
+              if ((r0.m >> lane) & 1u) {
+                const uint32_t ti = (uint32_t)(r0.vb >> 56);
+                uint32_t xi = xs[0];
+#pragma unroll
+                for (uint32_t j = 1; j < G; ++j) xi = ti == j ? xs[j] : xi;
+                const uint64_t pos = (r0.vb & ((1ull << 56) - 1)) + __popc(r0.m & below);
+                P.values[pos] = xi;
+                if (r0.kf != 0xFFFFFFFFu) P.vkey[pos] = r0.kf;
               }
             }
           }

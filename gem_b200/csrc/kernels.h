@@ -120,6 +120,9 @@ void launch_row_columns(const uint32_t *bits, uint32_t nwords, const uint32_t *r
                         uint32_t nv, uint32_t *out, uint32_t *vtiles, const uint32_t *deg, cudaStream_t s);
 // vt[t] = v for every vertex tile t in [vtp[v], vtp[v + 1]).
 void launch_vertex_tile_map(const uint64_t *vtp, uint32_t nv, uint32_t *vt, cudaStream_t s);
+// Write-pass units: out[v] = ceil(vtiles[v] / TAB_WGROUP).
+constexpr uint32_t TAB_WGROUP = 4;
+void launch_unit_counts(const uint32_t *vtiles, uint32_t nv, uint32_t *out, cudaStream_t s);
 // out[i] = a[idx[i]].
 void launch_gather_u64(const uint64_t *a, const uint32_t *idx, uint32_t n, uint64_t *out, cudaStream_t s);
 struct VSrc {                // a table source as the vertex-tile passes see it
@@ -133,8 +136,9 @@ struct VEdge {
   uint32_t tcol;
   uint32_t flags;
 };
-// One table pass over vertex tiles [t0, t1) (vt: tile -> vertex, vtp: first
-// tile of each vertex).  Arcs are read at nbr[arc - arc_shift], with off the
+// One table pass over units [t0, t1): the count pass's units are vertex
+// tiles (vt: tile -> vertex, vtp: first tile of each vertex), the write
+// pass's up to TAB_WGROUP consecutive tiles of one vertex (vg, vgp).  Arcs are read at nbr[arc - arc_shift], with off the
 // device offsets of the data graph.  S: the source membership columns (WS
 // words per vertex), B: the target membership columns (WT words per vertex).
 // count: mask[edge.tile_base + lt] = the 32-bit membership mask of tile lt of
@@ -146,6 +150,8 @@ struct VPass {
   uint64_t t0, t1;
   const uint32_t *vt;
   const uint64_t *vtp;
+  const uint32_t *vg;        // write pass: unit -> vertex (units of up to 4 tiles of one vertex)
+  const uint64_t *vgp;       // first unit of each vertex
   const uint32_t *S;
   uint32_t WS;
   uint32_t WT;

@@ -3,8 +3,9 @@
 // No counterpart in the reference (one query per process).  gem_submit
 // admits a query when its estimated device bytes fit the admission budget.
 // Worker threads, one per serving lane, each turn everything admitted and
-// not yet taken into a wave (shared filter/table launches and one persistent
-// join launch) on their lane.  An in-core context serves on two lanes: the
+// not yet taken into a wave, up to the lane's row limit, into one wave
+// (shared filter/table launches and one persistent join launch) on their
+// lane.  An in-core context serves on two lanes: the
 // context itself and a lane context that borrows its resident graph (its own
 // stream, arena, control block and task queue).  While one lane's wave is on
 // the GPU the other lane takes the requests that arrived meanwhile, so their
@@ -42,16 +43,6 @@ struct Server {
     uint64_t est;
   };
   std::deque<Req> pending;
-  // tickets at which a wave that did not fit was halved: a wave ends before them
-  std::vector<uint64_t> split_at;
-  bool is_split_point(uint64_t t) {
-    for (size_t i = 0; i < split_at.size(); ++i)
-      if (split_at[i] == t) {
-        split_at.erase(split_at.begin() + (long)i);
-        return true;
-      }
-    return false;
-  }
   std::map<uint64_t, gem_result> done;
   uint64_t next_ticket = 1;
   uint64_t in_flight = 0, budget = 0, per_wave = 0;
@@ -67,7 +58,8 @@ struct Server {
 // masks and positions, offsets per key, values and key positions (at most
 // the arcs between the two labels); per query the join's descriptors.
 // *per_wave: what every wave takes once whatever its queries (the vertex
-// tiles, their scan and map, the columns' rounding word per vertex).
+// tiles and the write pass's units, their scans and maps, the columns'
+// rounding word per vertex).
 static uint64_t estimate_bytes(const gem_ctx *ctx, const HostQuery &q, uint64_t *per_wave) {
   const uint64_t nv = ctx->g.nv, nwords = (nv + 31) / 32;
   const size_t L = ctx->label_freq.size();
@@ -97,8 +89,8 @@ static uint64_t estimate_bytes(const gem_ctx *ctx, const HostQuery &q, uint64_t 
     b += most;
   }
   const uint64_t parts = ctx->part_v.empty() ? 0 : ctx->part_v.size();
-  *per_wave = 2 * al(4 * nv) + al(4 * nv + 4) + al(8 * (nv + 1)) + al(8 * (nv / 2048 + 2)) +
-              al(4 * (nv + ctx->g.narcs / 32 + 1)) + al(8 * parts + 8) + (1ull << 20);
+  *per_wave = 2 * al(4 * nv) + 2 * (al(4 * nv + 4) + al(8 * (nv + 1)) + al(4 * (nv + ctx->g.narcs / 32 + 1))) +
+              al(8 * (nv / 2048 + 2)) + al(16 * parts + 16) + (1ull << 20);
   return b + (64ull << 10) * (q.nv + 1) + (1ull << 20);
 }
 
@@ -125,11 +117,11 @@ static void server_loop(gem_ctx *root, gem_ctx *lane) {
       std::unique_lock<std::mutex> lk(S.mu);
       S.cv.wait(lk, [&] { return S.stop || !S.pending.empty(); });
       if (S.stop && S.pending.empty()) return;
-      uint32_t rows = 0;
+      uint32_t rows = 0, cap = lane->wave_max_rows;
+      if (lane->wave_rows_cap) cap = std::min(cap, lane->wave_rows_cap);
       const int mode = S.pending.front().mode;
       while (!S.pending.empty() && S.pending.front().mode == mode &&
-             (batch.empty() || rows + S.pending.front().q.nv <= lane->wave_max_rows) &&
-             (batch.empty() || !S.is_split_point(S.pending.front().ticket))) {
+             (batch.empty() || rows + S.pending.front().q.nv <= cap)) {
         rows += S.pending.front().q.nv;
         batch.push_back(std::move(S.pending.front()));
         S.pending.pop_front();
@@ -146,11 +138,18 @@ static void server_loop(gem_ctx *root, gem_ctx *lane) {
     }
     if (st == GEM_ERR_OOM && batch.size() > 1) {
       // the wave's tables do not fit the lane's budget: its requests go back
-      // to the front of the queue in halves, with a fresh arena
-      lane->arena.release(lane);
+      // to the front of the queue, and the lane's waves are limited to the
+      // rows that would have fit (the wave's rows scaled by the bytes the
+      // budget left it over the bytes it asked for, a tenth kept back; half
+      // when that is not known)
+      const Arena &a = lane->arena;
+      double f = a.oom_need ? 0.9 * (double)a.oom_room / (double)a.oom_need : 0.5;
+      f = std::min(0.9, std::max(0.25, f));
+      uint64_t rows = 0;
+      for (const auto &r : batch) rows += r.q.nv;
+      lane->wave_rows_cap = (uint32_t)std::max<uint64_t>(1, (uint64_t)(f * (double)rows));
+      if (!lane->arena.reserved) lane->arena.release(lane);
       std::lock_guard<std::mutex> lk(S.mu);
-      const size_t h = batch.size() / 2;
-      S.split_at.push_back(batch[h].ticket);
       for (size_t i = batch.size(); i-- > 0;) S.pending.push_front(std::move(batch[i]));
       S.cv.notify_all();
       continue;
@@ -187,6 +186,7 @@ void server_shutdown(gem_ctx *ctx) {
   }
   ctx->join_grid_div = 1;
   if (S->saved_budget) ctx->budget = S->saved_budget;
+  if (ctx->arena.reserved) ctx->arena.release(ctx);  // it held the lane-split budget
   delete S;
   ctx->server = nullptr;
 }
@@ -213,6 +213,10 @@ static gem_status server_start(gem_ctx *ctx) {
       cudaGetLastError();
     }
   }
+  // each lane's arena: one chunk of its whole budget (no cudaMalloc or
+  // cudaFree between waves), less room for the join's graph
+  for (gem_ctx *l : S->lanes)
+    if (l->budget > l->device_bytes + (1ull << 30)) l->arena.reserve(l, l->budget - l->device_bytes - (512ull << 20));
   for (gem_ctx *lane : S->lanes) S->th.emplace_back(server_loop, ctx, lane);
   return GEM_OK;
 }
