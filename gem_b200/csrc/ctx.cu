@@ -1136,7 +1136,9 @@ static gem_status wave_tables(gem_ctx *ctx, Wave &w) {
   ST(aalloc(ctx, scan_tmp_words(tiles), &d_tmp2));
   // the target membership columns, the tile -> vertex map, and the sources
   // and tables as the passes read them
-  const uint32_t WT = (uint32_t)((tgt_row.size() + 31) / 32);
+  // target columns: whole 16-byte chunks per vertex (the count pass stages
+  // them with 16-byte asynchronous copies)
+  const uint32_t WT = (uint32_t)((tgt_row.size() + 127) / 128 * 4);
   if (!table_vtx_fits(WT)) {
     ctx->err = "too many edge-table target rows in one wave";
     return GEM_ERR_LIMIT;

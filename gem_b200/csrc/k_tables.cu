@@ -154,6 +154,14 @@ void launch_gather_u64(const uint64_t *a, const uint32_t *idx, uint32_t n, uint6
   gather_u64_kernel<<<(n + 255) / 256, 256, 0, s>>>(a, idx, n, out);
 }
 
+// 16-byte asynchronous copy global -> shared (both 16-byte aligned),
+// bypassing L1; cp_async_wait_all waits for this thread's copies.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Position of the (r + 1)-th set bit of m (r < popc(m)).
 __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t r) {
   uint32_t pos = 0;
@@ -233,12 +241,18 @@ __global__ void __launch_bounds__(256) table_vtx_kernel(VPass P) {
     const uint32_t nvalid = a1 - a0 - c * 32u < 32u ? (uint32_t)(a1 - a0 - c * 32u) : 32u;  // valid lanes: a prefix
     const uint32_t x = xs[0];
     if (!WRITE) {
+      // stage the target columns of the tile's arcs with asynchronous 16-byte
+      // copies (all in flight at once): lane = (row in group, 16-byte chunk)
       __syncwarp();  // the previous tile's reads of the stage are done
-      for (uint32_t l = 0; l < nvalid; ++l) {
-        const uint32_t xl = __shfl_sync(dev::FULL, x, l);
-        uint32_t *dst = stage + ((uint64_t)warp * 32u + l) * P.WTp;
-        for (uint32_t i = lane; i < P.WT; i += 32) dst[i] = __ldg(P.B + (uint64_t)xl * P.WT + i);
+      const uint32_t ch = P.WT >> 2, rpi = 32u / ch;  // chunks per column, columns per round
+      const uint32_t r = lane / ch, q = lane - r * ch;
+      uint32_t *wst = stage + (uint64_t)warp * 32u * P.WTp;
+      for (uint32_t g = 0; g < nvalid; g += rpi) {
+        const uint32_t l = g + r;
+        const uint32_t xl = __shfl_sync(dev::FULL, x, l < 32u ? l : 0u);
+        if (r < rpi && l < nvalid) cp_async16(wst + l * P.WTp + q * 4u, P.B + (uint64_t)xl * P.WT + q * 4u);
       }
+      cp_async_wait_all();
       __syncwarp();
     }
     const uint32_t *sv = P.S + (uint64_t)v * P.WS;
@@ -355,7 +369,9 @@ static uint32_t count_warps(uint32_t WTp) {
   return w > 8 ? 8u : w < 1 ? 1u : (uint32_t)w;
 }
 
-bool table_vtx_fits(uint32_t WT) { return 32ull * (WT | 1u) * 4 <= (200ull << 10); }
+// Target columns are staged in 16-byte chunks, at most one per lane per
+// column: WT (a multiple of 4) words up to 128.
+bool table_vtx_fits(uint32_t WT) { return WT % 4 == 0 && WT >= 4 && WT <= 128; }
 
 // Persistent grid: what the SMs hold at once (blocks per SM by occupancy).
 // Its warps take tiles in order from the launch's counter, so the tiles in
@@ -376,7 +392,7 @@ static uint32_t resident_blocks(const void *fn, int threads, size_t smem, uint64
 void launch_table_vtx(const VPass &P0, bool write, cudaStream_t s) {
   if (P0.t1 <= P0.t0) return;
   VPass P = P0;
-  P.WTp = P.WT | 1u;  // odd: the lanes' columns fall in distinct banks
+  P.WTp = P.WT;  // the lanes of a pair round read one staged column each: no stride padding
   const uint32_t warps = write ? 8u : count_warps(P.WTp);
   const uint64_t want = (P.t1 - P.t0 + warps - 1) / warps;
   cudaMemsetAsync(P.next, 0, sizeof(unsigned long long), s);

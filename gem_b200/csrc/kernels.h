@@ -168,8 +168,8 @@ struct VPass {
   unsigned long long *next;  // tile counter of the launch (zeroed by the launcher)
 };
 void launch_table_vtx(const VPass &P, bool write, cudaStream_t s);
-// Whether the count pass can stage WT-word target columns (one warp's 32
-// columns within 200 KB of shared memory).
+// Whether the count pass can stage WT-word target columns (WT a multiple of
+// 4, at most 128: 4,096 target rows).
 bool table_vtx_fits(uint32_t WT);
 // out[i] = tp[d_src[i].key_base] for i < nsrc, out[nsrc] = tp[nkeys].
 void launch_source_tile_bases(const TabSource *d_src, uint32_t nsrc, uint64_t nkeys, const uint64_t *tp,
