@@ -136,13 +136,44 @@ __device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t x, uint64_t *t
   return r;
 }
 
+// A thread's SCAN_I consecutive items: 16-byte loads when they are whole
+// and the input is 16-byte aligned, else one by one.
+template <ScanInput K>
+__device__ __forceinline__ void scan_items(const void *in, uint64_t n, uint64_t base, uint32_t (&v)[SCAN_I]) {
+  if (base + SCAN_I <= n && ((uintptr_t)in & 15u) == 0) {
+    if (K == SCAN_POPC_U64LO) {
+      const uint4 *p = (const uint4 *)((const uint64_t *)in + base);
+#pragma unroll
+      for (uint32_t j = 0; j < SCAN_I / 2; ++j) {
+        const uint4 a = __ldg(p + j);
+        v[2 * j] = __popc(a.x);
+        v[2 * j + 1] = __popc(a.z);
+      }
+    } else {
+      const uint4 *p = (const uint4 *)((const uint32_t *)in + base);
+#pragma unroll
+      for (uint32_t j = 0; j < SCAN_I / 4; ++j) {
+        const uint4 a = __ldg(p + j);
+        v[4 * j] = K == SCAN_POPC_U32 ? __popc(a.x) : a.x;
+        v[4 * j + 1] = K == SCAN_POPC_U32 ? __popc(a.y) : a.y;
+        v[4 * j + 2] = K == SCAN_POPC_U32 ? __popc(a.z) : a.z;
+        v[4 * j + 3] = K == SCAN_POPC_U32 ? __popc(a.w) : a.w;
+      }
+    }
+    return;
+  }
+#pragma unroll
+  for (uint32_t j = 0; j < SCAN_I; ++j) v[j] = base + j < n ? scan_item<K>(in, base + j) : 0u;
+}
+
 template <ScanInput K>
 __global__ void __launch_bounds__(SCAN_T) scan_partial_kernel(const void *in, uint64_t n, uint64_t *part) {
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_B + (uint64_t)threadIdx.x * SCAN_I;
+  uint32_t v[SCAN_I];
+  scan_items<K>(in, n, base, v);
   uint64_t s = 0;
 #pragma unroll
-  for (uint32_t j = 0; j < SCAN_I; ++j)
-    if (base + j < n) s += scan_item<K>(in, base + j);
+  for (uint32_t j = 0; j < SCAN_I; ++j) s += v[j];
   __shared__ uint64_t tot;
   (void)block_exclusive_scan(s, &tot);
   if (threadIdx.x == 0) part[blockIdx.x] = tot;
@@ -193,18 +224,26 @@ __global__ void __launch_bounds__(SCAN_T) scan_final_kernel(const void *in, uint
                                                             uint64_t *out) {
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_B + (uint64_t)threadIdx.x * SCAN_I;
   uint32_t v[SCAN_I];
+  scan_items<K>(in, n, base, v);
   uint64_t s = 0;
 #pragma unroll
-  for (uint32_t j = 0; j < SCAN_I; ++j) {
-    v[j] = base + j < n ? scan_item<K>(in, base + j) : 0u;
-    s += v[j];
-  }
+  for (uint32_t j = 0; j < SCAN_I; ++j) s += v[j];
   __shared__ uint64_t tot;
   uint64_t ex = block_exclusive_scan(s, &tot) + part[blockIdx.x];
+  uint64_t o[SCAN_I];
 #pragma unroll
   for (uint32_t j = 0; j < SCAN_I; ++j) {
-    if (base + j < n) out[base + j] = ex;
+    o[j] = ex;
     ex += v[j];
+  }
+  if (base + SCAN_I <= n && ((uintptr_t)(out + base) & 15u) == 0) {
+    ulonglong2 *q = (ulonglong2 *)(out + base);  // 16-byte stores
+#pragma unroll
+    for (uint32_t j = 0; j < SCAN_I / 2; ++j) q[j] = make_ulonglong2(o[2 * j], o[2 * j + 1]);
+  } else {
+#pragma unroll
+    for (uint32_t j = 0; j < SCAN_I; ++j)
+      if (base + j < n) out[base + j] = o[j];
   }
 }
 
