@@ -1,7 +1,8 @@
 // Serving: continuous batching with memory-based admission.
 //
 // No counterpart in the reference (one query per process).  gem_submit
-// admits a query when its estimated device bytes fit the admission budget.
+// admits a query when its estimated device bytes (its upper bound scaled by
+// what the waves so far took of theirs) fit the admission budget.
 // Worker threads, one per serving lane, each turn everything admitted and
 // not yet taken into a wave, up to the lane's row limit, into one wave
 // (shared filter/table launches and one persistent join launch) on their
@@ -40,8 +41,15 @@ struct Server {
     uint64_t ticket;
     HostQuery q;
     int mode;
-    uint64_t est;
+    uint64_t est;     // bytes charged to the admission budget
+    uint64_t bound;   // the estimate (an upper bound of the query's bytes)
   };
+  // Admission charges a query its upper bound times `scale`, learnt from the
+  // waves that ran: 1.5 times the largest recent ratio of a wave's bytes to
+  // its queries' bounds (at most 1).  The bound is loose (label statistics
+  // only), so charging it whole would admit a fraction of what fits; a wave
+  // that is admitted but does not fit is retried smaller.
+  double scale = 1.0;
   std::deque<Req> pending;
   std::map<uint64_t, gem_result> done;
   uint64_t next_ticket = 1;
@@ -155,6 +163,14 @@ static void server_loop(gem_ctx *root, gem_ctx *lane) {
       continue;
     }
     std::lock_guard<std::mutex> lk(S.mu);
+    if (st == GEM_OK) {
+      uint64_t bound = 0;
+      for (const auto &r : batch) bound += r.bound;
+      if (bound) {
+        const double target = std::min(1.0, 1.5 * (double)w.arena_bytes / (double)bound);
+        S.scale = target > S.scale ? target : 0.8 * S.scale + 0.2 * target;
+      }
+    }
     for (size_t i = 0; i < batch.size(); ++i) {
       gem_result r;
       if (st == GEM_OK) {
@@ -235,17 +251,18 @@ extern "C" gem_status gem_submit(gem_ctx *ctx, const gem_query *q, int mode, uin
   }
   Server &S = *ctx->server;
   uint64_t per_wave = 0;
-  const uint64_t est = estimate_bytes(ctx, hq, &per_wave);
+  const uint64_t bound = estimate_bytes(ctx, hq, &per_wave);
   std::lock_guard<std::mutex> lk(S.mu);
   if (!S.per_wave) {  // every lane's wave takes this once, beside its queries'
     S.per_wave = per_wave;
     const uint64_t fixed = per_wave * S.lanes.size();
     S.budget = S.budget > fixed ? S.budget - fixed : 0;
   }
+  const uint64_t est = std::max<uint64_t>(1, (uint64_t)(S.scale * (double)bound));
   if (S.in_flight + est > S.budget && S.in_flight > 0) return GEM_ERR_OOM;  // busy: retry later
   S.in_flight += est;
   *ticket = S.next_ticket++;
-  S.pending.push_back({*ticket, std::move(hq), mode, est});
+  S.pending.push_back({*ticket, std::move(hq), mode, est, bound});
   S.cv.notify_one();
   return GEM_OK;
 }

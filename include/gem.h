@@ -386,12 +386,14 @@ gem_status gem_filter_static(const uint64_t *d_offsets, const uint32_t *d_nbrs,
 /* until gem_ctx_destroy.  Admitted requests run in waves: everything        */
 /* admitted while a wave is on the GPU forms the next wave.                  */
 /* ------------------------------------------------------------------------ */
-/* Device scratch bytes gem_submit reserves for q under the admission budget
- * (host only, no counterpart in the reference): an upper bound of what a
- * wave of q alone takes, from the resident graph's label statistics. */
+/* An upper bound of the device scratch a wave of q alone takes, from the
+ * resident graph's label statistics (host only, no counterpart in the
+ * reference).  gem_submit charges the admission budget this bound times a
+ * factor (at most 1) learnt from the bytes its waves took of their
+ * queries' bounds. */
 gem_status gem_estimate_bytes(const gem_ctx *ctx, const gem_query *q, uint64_t *bytes);
-/* Submit a query; returns GEM_ERR_OOM when its estimated device bytes do not
- * fit the admission budget right now (caller retries later). */
+/* Submit a query; returns GEM_ERR_OOM when its charge does not fit the
+ * admission budget right now (caller retries later). */
 gem_status gem_submit(gem_ctx *ctx, const gem_query *q, int mode,
                       uint64_t *ticket);
 /* Advance the server (admit queued work, launch, retire finished queries)
