@@ -195,7 +195,7 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t r) {
 // The mask and value positions are those of the source's own tile order
 // (mask[tile_base + lt], lt = the tile's index among the source's tiles), so
 // both passes lay out every table exactly as a pass over the sources would.
-constexpr uint32_t TAB_GRAB = 2;  // units a warp takes from the counter at a time
+constexpr uint32_t TAB_GRAB = 1;  // units a warp takes from the counter at a time (1: the narrowest window)
 
 struct VRec {
   uint64_t vb;  // first value position of the pair's tile
