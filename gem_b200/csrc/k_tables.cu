@@ -19,15 +19,6 @@
 
 namespace gem {
 
-// Last index i in [lo, hi) with a[i] <= x (requires a[lo] <= x).
-__device__ __forceinline__ uint64_t last_le(const uint64_t *__restrict__ a, uint64_t lo, uint64_t hi, uint64_t x) {
-  while (hi - lo > 1) {
-    uint64_t mid = (lo + hi) >> 1;
-    if (__ldg(a + mid) <= x) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
 __device__ __forceinline__ uint32_t find_src(const TabSource *__restrict__ src, uint32_t nsrc, uint64_t k) {
   uint32_t lo = 0, hi = nsrc;
   while (hi - lo > 1) {
