@@ -878,7 +878,7 @@ static gem_status wave_filter(gem_ctx *ctx, Wave &w, uint32_t threshold) {
   std::vector<std::vector<uint32_t>> row_sig;
   w.row_of.assign(w.q.size(), std::vector<uint32_t>());
   for (size_t i = 0; i < w.q.size(); ++i) {
-    const HostQuery &q = w.q[i];
+    const HostQuery &q = w.sig_query ? *w.sig_query : w.q[i];
     w.row_of[i].resize(q.nv);
     for (uint32_t u = 0; u < q.nv; ++u) {
       std::vector<uint32_t> sig{q.lab[u], q.deg(u)};
@@ -1748,6 +1748,35 @@ extern "C" gem_status gem_query_run(gem_ctx *ctx, const gem_query *q, uint32_t t
   }
   res->ms[GEM_PH_HOST] = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return (gem_status)res->status;
+}
+
+// Relaxed queries of `orig` at `threshold` in one wave whose filter rows are
+// orig's own at that threshold (the reference's filter with slack T: a
+// relaxed query's vertex loses at most T neighbours, so orig's slack
+// candidates hold every relaxed query's).  All relaxed queries then share
+// orig's candidate lists and the tables of the edges they keep; each is
+// planned and counted exactly on its own.  GEM_ERR_OOM when the wave does
+// not fit (the caller then counts them as a plain batch).
+gem_status gem::relaxed_wave(gem_ctx *ctx, const HostQuery &orig, const std::vector<HostQuery> &rq,
+                             uint32_t threshold, int mode, gem_result *res) {
+  if (ctx->server) return GEM_ERR_STATE;
+  if (mode != GEM_MODE_COUNT && mode != GEM_MODE_HASH) return GEM_ERR_ARG;
+  if (rq.empty()) return GEM_OK;
+  Wave w;
+  w.q = rq;
+  w.sig_query = &orig;
+  ctx->arena.reset();
+  const gem_status st = run_wave(ctx, w, threshold, mode, nullptr, 0);
+  if (st != GEM_OK) {
+    cudaStreamSynchronize(ctx->s);
+    cudaGetLastError();
+    return st;
+  }
+  for (size_t i = 0; i < rq.size(); ++i) {
+    wave_result(ctx, w, i, &res[i]);
+    res[i].wave = 0;
+  }
+  return GEM_OK;
 }
 
 extern "C" gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n, int mode, gem_result *res) {

@@ -65,6 +65,10 @@ struct Wave {
   // wave's query vertices, which have the same candidates in every query.
   std::vector<std::vector<uint32_t>> row_of;  // per query, per query vertex: its row
   bool share_rows = true;           // false: one row per query vertex (the phase entry points)
+  // Relaxed matching: when set, every query's filter rows are this query's
+  // (the one the wave's queries relax), filtered at the wave's threshold, so
+  // the relaxed queries share their candidate lists and the tables they key.
+  const gem::HostQuery *sig_query = nullptr;
   std::vector<uint8_t> active;      // 0 = some C(u) empty (count 0)
   std::vector<Plan> plan;
   std::vector<std::vector<uint32_t>> idx_kind;  // per query, per level

@@ -52,5 +52,9 @@ struct HostQuery {
 // Validates q (sizes, ranges, no self loops or duplicate edges); connectivity
 // is required for nv > 1.
 gem_status make_host_query(const gem_query *q, HostQuery &out, std::string &err);
+// Relaxed queries rq of orig counted in one wave that shares orig's filter
+// rows at `threshold` (ctx.cu); GEM_ERR_OOM when that wave does not fit.
+gem_status relaxed_wave(gem_ctx *ctx, const HostQuery &orig, const std::vector<HostQuery> &rq, uint32_t threshold,
+                        int mode, gem_result *res);
 
 }  // namespace gem

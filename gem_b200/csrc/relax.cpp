@@ -10,9 +10,10 @@
 // subset with at most `threshold` edges removed is reached that way (remove
 // the missing edges in any order: every intermediate set contains the subset,
 // so it stays connected and is not yet a tree), so the relaxed queries are
-// exactly those subsets.  Here they are enumerated the same way and handed to
-// gem_batch_run as ordinary queries; the batch shares every launch between
-// them instead of sharing intermediate results.
+// exactly those subsets.  Here they are enumerated the same way and counted
+// in one wave whose filter rows are the original query's at the threshold
+// (the reference's slack filter), so the relaxed queries share candidate
+// lists and edge tables; the join counts each on its own.
 #include <algorithm>
 #include <cstring>
 #include <queue>
@@ -120,5 +121,14 @@ extern "C" gem_status gem_relaxed_run(gem_ctx *ctx, const gem_query *q, uint32_t
     rq[i] = gem_query{q->nv, (uint32_t)(edges[i].size() / 2), q->labels, edges[i].data()};
     ets[i] = sets[i];
   }
+  // one wave on q's filter rows at the threshold (shared candidate lists and
+  // tables); a plain batch when that wave does not fit the device budget
+  std::vector<HostQuery> hr(rq.size());
+  for (size_t i = 0; i < rq.size(); ++i) {
+    st = make_host_query(&rq[i], hr[i], err);
+    if (st != GEM_OK) return st;
+  }
+  st = relaxed_wave(ctx, hq, hr, threshold, mode, res);
+  if (st != GEM_ERR_OOM) return st;
   return gem_batch_run(ctx, rq.data(), (uint32_t)rq.size(), mode, res);
 }

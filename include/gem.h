@@ -250,7 +250,10 @@ gem_status gem_batch_run(gem_ctx *ctx, const gem_query *qs, uint32_t n,
  * q's vertices and labels.  gem_relaxed_sets lists them (host only): ets[i]
  * has bit j set when q's edge j (in q's order) is kept; fewest edges removed
  * first, then by mask descending.  gem_relaxed_run counts each exactly, as
- * its own query, in one gem_batch_run, with res[i] for ets[i].  At most cap
+ * its own query, with res[i] for ets[i]: in one wave whose candidate lists are
+ * q's own filtered with slack `threshold` (as the reference filters at -t T),
+ * so the relaxed queries share those lists and the edge tables of the edges
+ * they keep (as one gem_batch_run when that wave does not fit the budget).  At most cap
  * relaxed queries: with more, GEM_ERR_LIMIT and *n_out = cap + 1.  Queries
  * with more than 64 edges return GEM_ERR_LIMIT.  A query with one edge or
  * none has only itself (the reference lists none). */

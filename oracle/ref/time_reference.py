@@ -22,7 +22,8 @@ lines, sorted edge lines) and run with threshold 0 (its default is 2):
   Table time`, `initVertexTries time`, `construct time` and `Join Time`
   (in-core/src/main.cu:145-227), all GPU phases; again with `-t 1`
   (relaxed matching, one count per relaxed query), beside this library's
-  gem_relaxed_run on the same files (counts compared modulo 2^32).
+  gem_relaxed_run on the same files (counts compared modulo 2^32), and at
+  `-t 1` on 4-vertex queries with a cycle, which have relaxed queries.
 
 The printed counts are checked against the oracle modulo 2^32 (both
 binaries print them through a uint32_t).
@@ -132,12 +133,89 @@ def main():
         res["t1_counts_equal"] = sum(1 for a, b in zip(rel, ours) if sorted(a.get("counts", [])) == b["counts_mod_2_32"])
     except Exception as e:  # the library is optional here: the reference's figures stand alone
         res["gem_t1_error"] = str(e)[:200]
+    res["relaxed_dense"] = relaxed_dense(g, gpath, work, env, ic)
     ok = [q["counts"] == [e] for q, e in zip(res["out_of_core"]["queries"], expect)]
     res["out_of_core"]["counts_equal_oracle"] = sum(ok)
     res["in_core_counts_equal_oracle"] = sum(1 for q, e in zip(runs, expect) if q.get("counts") == [e])
     with open(out_path, "w") as f:
         json.dump(res, f, indent=1)
     print(json.dumps({k: v for k, v in res.items() if k not in ("in_core",)})[:3000])
+
+
+def relaxed_t1(q):
+    """Edge sets of q's relaxed queries at threshold 1 (bit j: q's edge j kept):
+    q itself and q without one edge, where the rest still connects q."""
+    e = [tuple(x) for x in q.edges.reshape(-1, 2).tolist()]
+    full = (1 << len(e)) - 1
+    out = [full]
+    if len(e) + 1 > q.nv:  # not a spanning tree: an edge can go
+        for j in range(len(e)):
+            keep = [e[i] for i in range(len(e)) if i != j]
+            seen, todo = {0}, [0]
+            while todo:
+                u = todo.pop()
+                for a, b in keep:
+                    for x, y in ((a, b), (b, a)):
+                        if x == u and y not in seen:
+                            seen.add(y)
+                            todo.append(y)
+            if len(seen) == q.nv:
+                out.append(full & ~(1 << j))
+    return out
+
+
+def relaxed_dense(g, gpath, work, env, ic, n=6):
+    """Relaxed matching (-t 1) on 4-vertex queries with a cycle, which have
+    relaxed queries (a tree has none): the in-core binary against
+    gem_relaxed_run, counts compared modulo 2^32.  Only queries whose relaxed
+    counts (by the oracle) stay at most 2e8 are run, the size of the
+    configuration-1 counts the reference handled here."""
+    picked = []
+    for q in oracle.gen_queries(g, 4, 2, 60, seed=0x51100):
+        ne = len(q.edges.reshape(-1, 2))
+        if ne < 4 or ne > 5:
+            continue
+        counts = []
+        for m in relaxed_t1(q):
+            ed = [x for j, x in enumerate(q.edges.reshape(-1, 2).tolist()) if (m >> j) & 1]
+            c, _, ok = oracle.count(g, oracle.Query(q.labels, ed), want_hash=False, work_cap=2_000_000_000)
+            if not ok or c > 200_000_000:
+                counts = None
+                break
+            counts.append(c % (1 << 32))
+        if counts:
+            picked.append((q, sorted(counts)))
+        if len(picked) == n:
+            break
+    out = {"queries": len(picked), "relaxed_per_query": [len(c) for _, c in picked], "reference": [], "gem": []}
+    for i, (q, _) in enumerate(picked):
+        qpath = os.path.join(work, "queries_relaxed", f"R_{i}.in")
+        os.makedirs(os.path.dirname(qpath), exist_ok=True)
+        write_query(q, qpath)
+        t0 = time.time()
+        r = subprocess.run([ic, "-q", qpath, "-d", gpath, "-t", "1", "-g", "0"], capture_output=True, text=True,
+                           env=env, timeout=600)
+        p = parse(r.stdout)
+        out["reference"].append({"exit": r.returncode, "wall_s": round(time.time() - t0, 1), **(p[0] if p else {})})
+    try:
+        import gem_b200 as gem
+        with gem.Context() as c:
+            c.load_graph(gem.HostGraph.read_text(gpath))
+            for i in range(len(picked)):
+                q = gem.Query.read_text(os.path.join(work, "queries_relaxed", f"R_{i}.in"))
+                c.relaxed(q, 1)
+                t0 = time.time()
+                res = c.relaxed(q, 1)
+                out["gem"].append({"wall_ms": round((time.time() - t0) * 1e3, 3),
+                                   "device_ms": round(sum({r["wave"]: r["ms"]["total"] for _, r in res}.values()), 3),
+                                   "counts_mod_2_32": sorted(r["count"] % (1 << 32) for _, r in res)})
+    except Exception as e:  # the library is optional here: the reference's figures stand alone
+        out["gem_error"] = str(e)[:200]
+    out["oracle_equal_reference"] = sum(1 for (_, c), r in zip(picked, out["reference"])
+                                        if sorted(r.get("counts", [])) == c)
+    out["gem_equal_reference"] = sum(1 for a, b in zip(out["reference"], out["gem"])
+                                     if sorted(a.get("counts", [])) == b["counts_mod_2_32"])
+    return out
 
 
 def write_graph(g, path):
